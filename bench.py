@@ -1,0 +1,305 @@
+"""Benchmark of the continental time step (node-steps/s) on B200.
+
+Default workload: the 2049x2049 multiple-flow grid (xl=yl=200 km, bc=1010,
+p=1.1, n=1.5 Newton, kf=2e-6, m=0.45, kd=5e-2, dt=500, h=U[0,10)+1e-3*j,
+interior uplift 5e-4), seeded synthetic input.  A step is one
+FastScape_Execute_Step of that grid; the timed steps follow W warm-up steps of
+the same trajectory.  The grid's working set (~4 GB) is far larger than the
+126 MB L2, so no explicit L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU runs are independent replicas (one instance per GPU, no collective):
+a single grid's routing tree, basin graph and implicit solves are global
+dependencies, so the path does not shard; value = nodes*steps of all ranks /
+max time over ranks ("scaling": "weak").
+
+--impl reference times the reference's CPU algorithm: the C++ restatement in
+oracle/ (the Fortran reference cannot be compiled here), one single-threaded
+instance per host core, each stepping the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "fastscapelib-fortran_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "node-steps/s at 2049^2 (continental step, MFD p=1.1, n=1.5, FP64)"
+UNIT = "node-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=2049)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    return ap.parse_args()
+
+
+def workload(size, seed=12345):
+    from fastscapelib_fortran import workloads as W
+    return W.mfd(size, seed=seed)
+
+
+def config(args, wl, ranks):
+    return {"workload": f"mfd_{wl.nx}x{wl.ny}_bc{wl.bc}_p{wl.p}_n{wl.n}", "nx": wl.nx, "ny": wl.ny,
+            "grids_per_gpu": 1, "parallelism": f"replicas{ranks}" if ranks > 1 else "single",
+            "l2": "working set >> 126 MB L2 (no flush needed)"}
+
+
+# ---------------------------------------------------------------------------
+# oracle (CPU) timing
+
+def _oracle_worker(args):
+    size, seed, warm, steps = args
+    import oracle as O
+    wl = workload(size, seed)
+    wl.apply(O)
+    for _ in range(warm):
+        O.fastscape_execute_step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        O.fastscape_execute_step()
+    return time.perf_counter() - t0, wl.nn * steps
+
+
+def cpu_baseline(size, steps):
+    t, nodes = _oracle_worker((size, 12345, 0, steps))
+    return {"value": nodes / t, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"first {steps} steps of the {size}x{size} workload, C++ restatement of the "
+                      f"reference (oracle/), 1 thread, {t:.1f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    procs = max(1, min(os.cpu_count() or 1, 16))
+    # bounded sample: the reference needs ~5 s per 2049^2 step on one core
+    with mp.get_context("spawn").Pool(procs) as pool:
+        t0 = time.perf_counter()
+        res = pool.map(_oracle_worker, [(args.size, 12345 + r, args.warmup, args.steps)
+                                        for r in range(procs)])
+        wall = time.perf_counter() - t0
+    tmax = max(t for t, _ in res)
+    nodes = sum(n for _, n in res)
+    value = nodes / tmax
+    wl = workload(args.size)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * tmax / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(args, wl, 1),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
+                             "sample": f"{procs} independent single-threaded instances x "
+                                       f"{args.steps} steps after {args.warmup} warm-up steps "
+                                       f"({wall:.0f} s wall)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    def __init__(self, index, path):
+        self.path = path
+        self.proc = None
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sms, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sms:
+            return None
+        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+# algorithmic bytes per node of each stage (FP64 values, int32 indices; rbar =
+# mean number of multiple-flow receivers, nconn = basin-graph edges)
+def stage_bytes(stage, rbar, nconn_per_node, sfd):
+    table = {
+        "uplift": 40.0,
+        "receivers": 20.0,
+        "stack": 16.0,
+        "local_minima": 52.0 + 48.0 * nconn_per_node,
+        "lake_fill": 32.0,
+        "mfd_receivers": 12.0 + 20.0 * rbar,
+        "drainage_area": 24.0 if sfd else 16.0 + 12.0 * rbar,
+        "stream_power": 88.0 if sfd else 88.0 + 20.0 * rbar,
+        "diffusion": 88.0,
+    }
+    return table[stage]
+
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import fastscapelib_fortran as fs
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.size, args.cpu_steps)
+
+    wl = workload(args.size, seed=12345 + rank)
+    g = fs.FastScape(local)
+    g.set_nx_ny(wl.nx, wl.ny)
+    g.setup()
+    g.set_xl_yl(wl.xl, wl.yl)
+    g.set_dt(wl.dt)
+    g.init_h(wl.h0)
+    g.set_erosional_parameters(wl.kf, wl.kfsed, wl.m, wl.n, wl.kd, wl.kdsed, wl.g1, wl.g2, wl.p)
+    g.set_u(wl.u)
+    g.set_bc(wl.bc)
+    stream = torch.cuda.current_stream(dev)
+
+    for _ in range(args.warmup):
+        g.execute_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    g.set_profile(True)
+    g.stage_times(reset=True)
+    clocks = ClockSampler(local, os.path.join(ROOT, "gpurun_out", f"clocks_r{rank}.csv")) \
+        if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ClockSampler(local, f"/tmp/clocks_r{rank}.csv")
+    launches0 = g.launch_count()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    g.execute_step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    launches = g.launch_count() - launches0
+    stages = g.stage_times(reset=True)
+    g.set_profile(False)
+
+    # e2e through the reference-facing API with host buffers: set_u from pinned
+    # host memory, execute_step, copy_h back into pinned host memory
+    u_host = torch.from_numpy(wl.u.copy()).pin_memory()
+    h_host = torch.empty(wl.nn, dtype=torch.float64).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        g.set_u(u_host)
+        g.execute_step()
+        g.copy("h", h_host)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max(f0.elapsed_time(f1), 1e3 * (time.perf_counter() - t0))
+
+    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max, e2e_max = float(t[0]), float(t[1])
+    nodes = wl.nn * args.steps * world
+    value = nodes / (ms_max / 1e3)
+    e2e_val = nodes / (e2e_max / 1e3)
+
+    if rank == 0:
+        mnrec = g.copy_int("mnrec")
+        rbar = float(mnrec.mean())
+        dbg_nconn = g.locmin_debug()["nconn"]
+        top = max(stages.items(), key=lambda kv: kv[1][0])
+        name, (tot_ms, calls) = top
+        per_launch_ms = tot_ms / max(calls, 1)
+        bpn = stage_bytes(name, rbar, dbg_nconn / wl.nn, wl.p < -1.5)
+        achieved = bpn * wl.nn / (per_launch_ms / 1e3) / 1e9
+        peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        peak, peak_src = 6650.0, "fallback"
+        if os.path.exists(peaks_path):
+            peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "dram_traffic.json")
+        if os.path.exists(tpath):
+            traffic = json.load(open(tpath)).get(name)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config(args, wl, world),
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 8 * wl.nn,
+                    "d2h_bytes_per_step": 8 * wl.nn},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
+                         "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "bytes_per_node": bpn},
+            "stages_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()},
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,50 @@
+// Shared definitions of the B200 continental-step library.
+//
+// Node numbering is 0-based: ij = i + j*nx with i in [0,nx), j in [0,ny)
+// (x fastest), i.e. the reference's ij = i + (j-1)*nx minus one.  Slot arrays
+// (donors, multiple receivers) are node-major with 8 slots per node, which is
+// the reference's column-major don(8,nn) / mrec(8,nn) layout.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+
+namespace fsb {
+
+// Boundary description decoded from the reference's 4-digit code
+// (src/FastScape_ctx.f90:565-593): digits are bottom, right, top, left.
+struct Bounds {
+  int nx, ny;
+  int i1, i2, j1, j2;   // 0-based inclusive loop bounds of find_receiver
+  int fix_bottom, fix_right, fix_top, fix_left;
+  int xcyc, ycyc;
+};
+
+__host__ __device__ inline bool is_bc_node(const Bounds& b, int i, int j) {
+  return (b.fix_left && i == 0) || (b.fix_right && i == b.nx - 1) || (b.fix_bottom && j == 0) ||
+         (b.fix_top && j == b.ny - 1);
+}
+
+// Neighbour index with the reference's wrap-then-clamp rule
+// (FlowRouting.f90:336-344).
+__host__ __device__ inline int wrap_clamp(int v, int n, int cyc) {
+  if (v < 0 && cyc) v += n;
+  v = v < 0 ? 0 : v;
+  if (v > n - 1 && cyc) v -= n;
+  v = v > n - 1 ? n - 1 : v;
+  return v;
+}
+
+// Error codes written by device code to the context's status word.
+enum DeviceError : int {
+  DEV_OK = 0,
+  DEV_SPIN_LIMIT = 1,       // a bounded wait gave up
+  DEV_STACK_ERROR = 2,      // a traversal did not cover every node
+  DEV_TRIDAG_ZERO = 3,      // zero pivot in the tridiagonal solve
+  DEV_OVERFLOW = 4,         // a data-dependent buffer bound was exceeded
+};
+
+constexpr int kSpinLimit = 1 << 21;  // polls (~1 s) before a bounded wait gives up
+
+}  // namespace fsb

@@ -1,0 +1,141 @@
+// Device-resident state of one continental-step instance and the launchers
+// that operate on it.  One Ctx mirrors the reference's FastScapeContext module
+// (src/FastScape_ctx.f90:9-36) for the arrays the continental step touches.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <utility>
+
+#include "fsb_common.cuh"
+
+namespace fsb {
+
+constexpr int kBlock = 256;
+
+inline unsigned grid1d(size_t n, int block = kBlock) {
+  size_t g = (n + block - 1) / block;
+  if (g > 148u * 64u) g = 148u * 64u;  // grid-stride loops beyond 64 blocks per SM
+  if (g == 0) g = 1;
+  return (unsigned)g;
+}
+
+struct Ctx {
+  // ---- configuration (setters of FastScape_ctx.f90) ----
+  int nx = 0, ny = 0, nn = 0;
+  int ibc = 1111;
+  Bounds bd{};
+  double xl = 0, yl = 0, dt = 0, kfsed = -1, m = 0, n = 1, kdsed = -1, g1 = 0, g2 = 0, p = 0;
+  double dx = 0, dy = 0;
+  bool sfd = false, runSPL = false, runDiffusion = false, runUplift = false;
+  bool setup_done = false;
+  bool capture = false;  // keep LocalMinima intermediates of the last step
+  int step = 0;
+  cudaStream_t stream = 0;
+  long long launches = 0;  // kernels launched by this instance
+  void count_launch(long long k = 1) { launches += k; }
+
+  // ---- device arena ----
+  char* arena = nullptr;
+  size_t arena_bytes = 0;
+  bool owns_arena = false;
+
+  // ---- persistent fields (nn each unless noted) ----
+  double *h = nullptr, *b = nullptr, *u = nullptr, *kf = nullptr, *kd = nullptr, *precip = nullptr;
+  double *etot = nullptr, *erate = nullptr, *a = nullptr, *length = nullptr, *lake_depth = nullptr;
+  double *hwater = nullptr, *sedflux = nullptr;
+  int *rec = nullptr, *ndon = nullptr, *don = nullptr /*8*nn*/, *stack = nullptr;
+  int *pos = nullptr, *size = nullptr;
+  int *mrec = nullptr /*8*nn*/, *mnrec = nullptr, *mstack = nullptr, *mdmask = nullptr;
+  double *mwrec = nullptr /*8*nn*/, *mlrec = nullptr /*8*nn*/;
+  double* ltab = nullptr;  // 9 neighbour lengths of find_receiver / find_mult_rec
+
+  // ---- captured intermediates (debug / parity) ----
+  int *rec_pre = nullptr, *stack_pre = nullptr, *basins = nullptr, *outlets = nullptr;
+  double* length_pre = nullptr;
+
+  // ---- scratch ----
+  int *s_flag = nullptr, *s_scan = nullptr, *s_roots = nullptr, *s_root_rank = nullptr;
+  unsigned long long *s_list_a = nullptr, *s_list_b = nullptr;  // 2*nn each
+  // LocalMinima
+  size_t conn_cap = 0;       // capacity of edge arrays
+  size_t hash_cap = 0;       // capacity (power of two) of the basin-pair hash
+  unsigned long long *ht_key = nullptr, *ht_wmin = nullptr;
+  unsigned *ht_first = nullptr, *ht_best = nullptr;
+  int *e_b1 = nullptr, *e_b2 = nullptr, *e_n1 = nullptr, *e_n2 = nullptr;
+  double* e_w = nullptr;
+  unsigned *e_key = nullptr, *e_key2 = nullptr;
+  int *e_idx = nullptr, *e_idx2 = nullptr;
+  int *o_b1 = nullptr, *o_b2 = nullptr, *o_n1 = nullptr, *o_n2 = nullptr;  // oriented copies
+  int *r_b1 = nullptr, *r_b2 = nullptr, *r_n1 = nullptr, *r_n2 = nullptr;  // unsorted edges
+  double* r_w = nullptr;
+  int *nr_idx = nullptr, *nr_idx2 = nullptr, *nr_lf = nullptr, *nr_rf = nullptr, *nr_ls = nullptr,
+      *nr_rs = nullptr, *nr_lpos = nullptr, *nr_rpos = nullptr, *nr_segof = nullptr;
+  int *nr_seg = nullptr, *nr_seg2 = nullptr;  // segments: pairs (l, ir), 1-based
+  int *nr_small = nullptr;                    // small segments (l, ir)
+  double* nr_piv = nullptr;
+  int* nr_segmeta = nullptr;  // per segment: pv, i, j, T
+  int *e_rank = nullptr, *e_inmst = nullptr, *tree = nullptr;
+  int *mst_comp = nullptr, *mst_min = nullptr, *mst_next = nullptr;
+  int *arc_deg = nullptr, *arc_start = nullptr, *arc_slot = nullptr, *arc_adj = nullptr;
+  // MFD order
+  unsigned long long *o_keys = nullptr, *o_keys2 = nullptr;
+  int *o_vals = nullptr, *o_vals2 = nullptr, *o_pos = nullptr;
+  // sweeps
+  unsigned *done = nullptr;  // epoch flags per node
+  unsigned epoch = 0;
+  unsigned* ticket = nullptr;
+  double* water = nullptr;
+  double* hnew = nullptr;  // elevation written by the stream-power sweep
+  // diffusion scratch: kdint, tridiagonal coefficients, forward factors, x-pass result
+  double *dK = nullptr, *dA = nullptr, *dB = nullptr, *dC = nullptr, *dF = nullptr, *dG = nullptr, *dZ = nullptr;
+  // counters on device and their pinned host mirror
+  int* d_err = nullptr;   // device error word
+  int* d_cnt = nullptr;   // small device counters
+  int* h_cnt = nullptr;   // pinned host mirror of d_cnt
+  void* cub_tmp = nullptr;
+  size_t cub_tmp_bytes = 0;
+
+  // last LocalMinima counts (host)
+  int nbasins = 0, basin0 = 0, nconn = 0, tree_size = 0, nlocmin_before = 0, nlocmin_after = 0;
+
+  // per-stage device timing (CUDA events on the instance's stream)
+  static constexpr int kStages = 9;  // uplift receivers stack locmin fill mfd accum spl diffusion
+  bool profile = false;
+  cudaEvent_t ev_begin[kStages] = {}, ev_end[kStages] = {};
+  bool ev_pending[kStages] = {};
+  double stage_ms[kStages] = {};
+  long long stage_calls[kStages] = {};
+
+  std::string err;
+};
+
+// routing (fsb_routing.cu)
+void launch_uplift(Ctx& c);
+void launch_find_receiver(Ctx& c, const double* h, int* rec, double* length);
+void launch_find_donors(Ctx& c, const int* rec, int* ndon, int* don);
+void build_stack(Ctx& c, const int* rec, int* ndon, int* don, int* stack, int* pos, int* size);
+unsigned long long* list_rank(Ctx& c, size_t n, unsigned long long* a, unsigned long long* b);
+
+// primitives (fsb_prims.cu)
+void exclusive_scan_int(Ctx& c, const int* in, int* out, size_t n);
+void inclusive_scan_int(Ctx& c, const int* in, int* out, size_t n);
+void sort_pairs_u32(Ctx& c, const unsigned* kin, unsigned* kout, const int* vin, int* vout, size_t n, int end_bit);
+void sort_pairs_u64(Ctx& c, const unsigned long long* kin, unsigned long long* kout, const int* vin,
+                    int* vout, size_t n);
+size_t cub_temp_bytes_needed(size_t nn, size_t nconn);
+void fetch_counters(Ctx& c, int n);  // d_cnt[0..n) -> h_cnt (synchronises the stream)
+
+// LocalMinima (fsb_locmin.cu); returns false and sets c.err on failure
+bool local_minima(Ctx& c);
+
+// flow (fsb_flow.cu)
+void fill_sweep(Ctx& c);            // hwater along the stack (SFD lake fill / MFD h0)
+void mfd_receivers(Ctx& c);         // find_mult_rec: mrec, mnrec, mlrec, mwrec, order
+void accumulate(Ctx& c);            // drainage area
+void stream_power(Ctx& c);          // implicit stream power law (g == 0)
+void diffusion(Ctx& c);             // ADI hillslope diffusion
+
+}  // namespace fsb

@@ -1,0 +1,747 @@
+// Depression routing (Cordonnier et al. 2019 as implemented in the reference's
+// src/LocalMinima.f90:1-132, continuous_flow_v2 branch).
+//
+//   compute_basins        LocalMinima.f90:136-169  -> k_basins (scan over the stack)
+//   connect_basins        LocalMinima.f90:173-329  -> k_conn_pass / k_conn_compact / sort
+//   loc_min_3_indexx      LocalMinima.f90:947-1046 -> exact segmented emulation (nr_*)
+//   mst_kruskal+UnionFind LocalMinima.f90:333-385,766-832 -> Boruvka on the sort ranks
+//   order_tree            LocalMinima.f90:389-533  -> Euler tour of the tree + ranking
+//   correct_receivers_v2  LocalMinima.f90:601-662  -> k_correct (one thread per edge)
+//
+// Exactness argument.  Kruskal accepts edges in the order of the NR index
+// sort; the accepted set is the unique minimum spanning tree under the total
+// order "position in that sorted permutation", which Boruvka computes in
+// parallel.  The sorted permutation itself is reproduced exactly: quicksort
+// segments are independent once created, and one Hoare partition of a
+// segment is determined by the positions of the left-scan stoppers
+// (arr >= pivot) and right-scan stoppers (arr <= pivot) of the segment, which
+// prefix sums give in parallel (see k_nr_cross for the crossing rule).  The
+// conn list is built in the reference's discovery order: edge (b,nb) sits at
+// the first (stack position, neighbour slot) where it is met and keeps the
+// earliest minimum-weight pass.  Receiver corrections touch disjoint child
+// basins, so they run in parallel in any order.
+#include <cfloat>
+#include <climits>
+
+#include "fsb_kernels.cuh"
+
+namespace fsb {
+
+namespace {
+
+enum {
+  C_NBASINS = 0, C_NLOCMIN = 1, C_BASIN0 = 2, C_NEDGE = 3, C_NSEG = 4, C_NSMALL = 5,
+  C_CHANGED = 6, C_NTREE = 7, C_NLOCMIN_AFTER = 8, C_OVERFLOW = 9, C_NOTFLAT = 10
+};
+
+__constant__ int c_ii[8] = {-1, 1, 0, 0, -1, 1, -1, 1};
+__constant__ int c_jj[8] = {0, 0, -1, 1, -1, -1, 1, 1};
+
+__device__ inline unsigned long long ordered_u64(double x) {
+  unsigned long long u = (unsigned long long)__double_as_longlong(x);
+  return (u & 0x8000000000000000ull) ? ~u : (u | 0x8000000000000000ull);
+}
+
+__device__ inline unsigned long long mix64(unsigned long long x) {
+  x ^= x >> 33; x *= 0xff51afd7ed558ccdull; x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ull; x ^= x >> 33;
+  return x;
+}
+
+// ---- basins --------------------------------------------------------------
+__global__ void k_pos_root_flags(int nn, const int* __restrict__ stack, const int* __restrict__ rec,
+                                 int* __restrict__ flag) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nn; p += gridDim.x * blockDim.x) {
+    const int k = stack[p];
+    flag[p] = rec[k] == k ? 1 : 0;
+  }
+}
+
+__global__ void k_basins(int nn, const int* __restrict__ stack, const int* __restrict__ incl,
+                         int* __restrict__ basins) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nn; p += gridDim.x * blockDim.x)
+    basins[stack[p]] = incl[p];
+}
+
+// active roots (local minima) and basin0 = first basin whose root is on a fixed boundary
+__global__ void k_roots_scan(Bounds bd, int nroots, const int* __restrict__ roots, int* __restrict__ cnt) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nroots; r += gridDim.x * blockDim.x) {
+    const int k = roots[r];
+    if (is_bc_node(bd, k % bd.nx, k / bd.nx)) atomicMin(&cnt[C_BASIN0], r + 1);
+    else atomicAdd(&cnt[C_NLOCMIN], 1);
+  }
+}
+
+// ---- connect_basins ------------------------------------------------------
+__device__ inline unsigned ht_insert(unsigned long long* keys, size_t cap, unsigned long long key) {
+  size_t s = mix64(key) & (cap - 1);
+  const size_t limit = cap < 4096 ? cap : 4096;  // load stays below 1/2: long probes mean overflow
+  for (size_t probe = 0; probe < limit; ++probe) {
+    const unsigned long long old = atomicCAS(&keys[s], ~0ull, key);
+    if (old == ~0ull || old == key) return (unsigned)s;
+    s = (s + 1) & (cap - 1);
+  }
+  return 0xffffffffu;
+}
+
+__device__ inline unsigned ht_find(const unsigned long long* keys, size_t cap, unsigned long long key) {
+  size_t s = mix64(key) & (cap - 1);
+  const size_t limit = cap < 4096 ? cap : 4096;
+  for (size_t probe = 0; probe < limit; ++probe) {
+    const unsigned long long k = keys[s];
+    if (k == key) return (unsigned)s;
+    if (k == ~0ull) return 0xffffffffu;
+    s = (s + 1) & (cap - 1);
+  }
+  return 0xffffffffu;
+}
+
+// pass 0: insert pairs, min weight, first discovery; pass 1: earliest
+// discovery among the minimum-weight candidates of each pair.
+template <int PASS>
+__global__ void k_conn_pass(Bounds bd, const int* __restrict__ basins, const int* __restrict__ roots,
+                            const int* __restrict__ pos, const double* __restrict__ h,
+                            unsigned long long* __restrict__ ht_key, unsigned long long* __restrict__ ht_wmin,
+                            unsigned* __restrict__ ht_first, unsigned* __restrict__ ht_best, size_t cap,
+                            int* __restrict__ cnt) {
+  const int nx = bd.nx, ny = bd.ny, nn = nx * ny;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nn; p += gridDim.x * blockDim.x) {
+    const int b = basins[p];
+    const int outlet = roots[b - 1];
+    if (is_bc_node(bd, outlet % nx, outlet / nx)) continue;  // inactive basin: not scanned
+    const int i = p % nx, j = p / nx;
+    const double hp = h[p];
+    const unsigned disc0 = (unsigned)pos[p] * 8u;
+    for (int k = 0; k < 8; ++k) {
+      const int ki = i + c_ii[k], kj = j + c_jj[k];
+      if (ki < 0 || ki >= nx || kj < 0 || kj >= ny) continue;
+      const int q = ki + kj * nx;
+      const int nb = basins[q];
+      const int nbo = roots[nb - 1];
+      if (b >= nb && !is_bc_node(bd, nbo % nx, nbo / nx)) continue;
+      const double w = fmax(hp, h[q]);
+      const unsigned long long key = ((unsigned long long)b << 32) | (unsigned)nb;
+      const unsigned disc = disc0 + (unsigned)k;
+      if (PASS == 0) {
+        const unsigned s = ht_insert(ht_key, cap, key);
+        if (s == 0xffffffffu) { atomicExch(&cnt[C_OVERFLOW], 1); continue; }
+        atomicMin(&ht_wmin[s], ordered_u64(w));
+        atomicMin(&ht_first[s], disc);
+      } else {
+        const unsigned s = ht_find(ht_key, cap, key);
+        if (s == 0xffffffffu) continue;
+        if (ordered_u64(w) == ht_wmin[s]) atomicMin(&ht_best[s], disc);
+      }
+    }
+  }
+}
+
+__global__ void k_conn_compact(Bounds bd, size_t cap, const unsigned long long* __restrict__ ht_key,
+                               const unsigned* __restrict__ ht_first, const unsigned* __restrict__ ht_best,
+                               const int* __restrict__ stack, const double* __restrict__ h, size_t conn_cap,
+                               unsigned* __restrict__ r_key, int* __restrict__ r_b1, int* __restrict__ r_b2,
+                               int* __restrict__ r_n1, int* __restrict__ r_n2, double* __restrict__ r_w,
+                               int* __restrict__ cnt) {
+  const int nx = bd.nx;
+  for (size_t s = blockIdx.x * (size_t)blockDim.x + threadIdx.x; s < cap; s += (size_t)gridDim.x * blockDim.x) {
+    const unsigned long long key = ht_key[s];
+    if (key == ~0ull) continue;
+    const int idx = atomicAdd(&cnt[C_NEDGE], 1);
+    if ((size_t)idx >= conn_cap) { atomicExch(&cnt[C_OVERFLOW], 1); continue; }
+    const unsigned best = ht_best[s];
+    if (best == 0xffffffffu) { atomicExch(&cnt[C_OVERFLOW], 1); continue; }
+    const int p = stack[best >> 3];
+    const int k = best & 7;
+    const int q = (p % nx + c_ii[k]) + (p / nx + c_jj[k]) * nx;
+    r_key[idx] = ht_first[s];
+    r_b1[idx] = (int)(key >> 32);
+    r_b2[idx] = (int)(key & 0xffffffffu);
+    r_n1[idx] = p;
+    r_n2[idx] = q;
+    r_w[idx] = fmax(h[p], h[q]);
+  }
+}
+
+// virtual edges basin0 <-> every other open basin, keyed at the open root's stack position
+__global__ void k_conn_virtual(Bounds bd, int nroots, const int* __restrict__ roots, const int* __restrict__ pos,
+                               size_t conn_cap, unsigned* __restrict__ r_key, int* __restrict__ r_b1,
+                               int* __restrict__ r_b2, int* __restrict__ r_n1, int* __restrict__ r_n2,
+                               double* __restrict__ r_w, int* __restrict__ cnt) {
+  const int basin0 = cnt[C_BASIN0];
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nroots; r += gridDim.x * blockDim.x) {
+    const int k = roots[r];
+    if (!is_bc_node(bd, k % bd.nx, k / bd.nx) || r + 1 == basin0) continue;
+    const int idx = atomicAdd(&cnt[C_NEDGE], 1);
+    if ((size_t)idx >= conn_cap) { atomicExch(&cnt[C_OVERFLOW], 1); continue; }
+    r_key[idx] = (unsigned)pos[k] * 8u;
+    r_b1[idx] = basin0;
+    r_b2[idx] = r + 1;
+    r_n1[idx] = -1;
+    r_n2[idx] = -1;
+    r_w[idx] = -1.0e10;
+  }
+}
+
+__global__ void k_iota(int n, int* __restrict__ v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
+}
+
+__global__ void k_conn_gather(int n, const int* __restrict__ perm, const int* __restrict__ r_b1,
+                              const int* __restrict__ r_b2, const int* __restrict__ r_n1,
+                              const int* __restrict__ r_n2, const double* __restrict__ r_w,
+                              int* __restrict__ b1, int* __restrict__ b2, int* __restrict__ n1,
+                              int* __restrict__ n2, double* __restrict__ w) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int e = perm[t];
+    b1[t] = r_b1[e]; b2[t] = r_b2[e]; n1[t] = r_n1[e]; n2[t] = r_n2[e]; w[t] = r_w[e];
+  }
+}
+
+// ---- loc_min_3_indexx emulation (1-based positions l..ir) -----------------
+// idx[1..n] holds 1-based edge ids, arr[1..n] the weights (arr = w - 1).
+__global__ void k_nr_init(int n, int* __restrict__ idx, int* __restrict__ segof, int* __restrict__ seg,
+                          int* __restrict__ small, int* __restrict__ cnt) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= n + 1; q += gridDim.x * blockDim.x) {
+    if (q >= 1 && q <= n) idx[q] = q;
+    segof[q] = (q >= 1 && q <= n && n - 1 >= 7) ? 0 : -1;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (n - 1 >= 7) { seg[0] = 1; seg[1] = n; cnt[C_NSEG] = 1; }
+    else if (n >= 2) { small[0] = 1; small[1] = n; cnt[C_NSMALL] = 1; cnt[C_NSEG] = 0; }
+    else cnt[C_NSEG] = 0;
+  }
+}
+
+__device__ inline void iswap(int* v, int a, int b) { const int t = v[a]; v[a] = v[b]; v[b] = t; }
+
+// median of three (LocalMinima.f90:985-1006)
+__global__ void k_nr_median(int nseg, const int* __restrict__ seg, const double* __restrict__ arr,
+                            int* __restrict__ idx, double* __restrict__ piv, int* __restrict__ meta) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
+    const int l = seg[2 * s], ir = seg[2 * s + 1];
+    const int k = (l + ir) / 2;
+    iswap(idx, k, l + 1);
+    if (arr[idx[l + 1]] > arr[idx[ir]]) iswap(idx, l + 1, ir);
+    if (arr[idx[l]] > arr[idx[ir]]) iswap(idx, l, ir);
+    if (arr[idx[l + 1]] > arr[idx[l]]) iswap(idx, l + 1, l);
+    piv[s] = arr[idx[l]];
+    meta[4 * s] = idx[l];
+  }
+}
+
+// stopper flags: left scan stops where arr >= a (positions l+2..ir),
+// right scan stops where arr <= a (positions l+1..ir-1)
+__global__ void k_nr_flags(int n, const int* __restrict__ segof, const int* __restrict__ seg,
+                           const double* __restrict__ piv, const double* __restrict__ arr,
+                           const int* __restrict__ idx, int* __restrict__ lf, int* __restrict__ rf) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= n + 1; q += gridDim.x * blockDim.x) {
+    int a = 0, b = 0;
+    const int s = segof[q];
+    if (s >= 0) {
+      const int l = seg[2 * s], ir = seg[2 * s + 1];
+      const double pv = piv[s];
+      const double v = arr[idx[q]];
+      a = (q >= l + 2 && q <= ir && v >= pv) ? 1 : 0;
+      b = (q >= l + 1 && q <= ir - 1 && v <= pv) ? 1 : 0;
+    }
+    lf[q] = a;
+    rf[q] = b;
+  }
+}
+
+__global__ void k_nr_scatter(int n, const int* __restrict__ lf, const int* __restrict__ rf,
+                             const int* __restrict__ ls, const int* __restrict__ rs, int* __restrict__ lpos,
+                             int* __restrict__ rpos) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= n + 1; q += gridDim.x * blockDim.x) {
+    if (lf[q]) lpos[ls[q]] = q;
+    if (rf[q]) rpos[rs[q]] = q;
+  }
+}
+
+// Crossing of the Hoare scans.  With L_t the t-th left stopper (ascending)
+// and R_t the t-th right stopper (descending) of the unmodified segment, the
+// partition swaps (L_t, R_t) for every t < T, T = min{t : L_t >= R_t}.  If
+// L_T == R_T = P the scans stop at i=P+1, j=P-1; otherwise at
+// i = min(L_T, R_{T-1}), j = max(R_T, L_{T-1}) (R_0 = +inf, L_0 = -inf).
+__global__ void k_nr_cross(int nseg, const int* __restrict__ seg, const int* __restrict__ ls,
+                           const int* __restrict__ rs, const int* __restrict__ lpos,
+                           const int* __restrict__ rpos, int* __restrict__ meta) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
+    const int l = seg[2 * s], ir = seg[2 * s + 1];
+    const int lb = ls[l + 2], nL = ls[ir + 1] - ls[l + 2];
+    const int rtop = rs[ir], nR = rs[ir] - rs[l + 1];
+    auto L = [&](int t) { return lpos[lb + t - 1]; };
+    auto R = [&](int t) { return rpos[rtop - t]; };
+    int lo = 1, hi = min(nL, nR);
+    while (lo < hi) {
+      const int mid = (lo + hi) / 2;
+      if (L(mid) >= R(mid)) hi = mid; else lo = mid + 1;
+    }
+    const int T = lo;
+    int i, j;
+    if (L(T) == R(T)) {
+      i = L(T) + 1;
+      j = L(T) - 1;
+    } else {
+      i = (T == 1) ? L(1) : min(L(T), R(T - 1));
+      j = (T == 1) ? R(1) : max(R(T), L(T - 1));
+    }
+    meta[4 * s + 1] = i;
+    meta[4 * s + 2] = j;
+    meta[4 * s + 3] = T;
+  }
+}
+
+__device__ inline int nr_newval(int x, int l, int ir, int T, const int* idx, const int* lf,
+                                const int* rf, const int* ls, const int* rs, const int* lpos,
+                                const int* rpos) {
+  if (lf[x]) {
+    const int t = ls[x] - ls[l + 2] + 1;
+    if (t < T) return idx[rpos[rs[ir] - t]];
+  }
+  if (rf[x]) {
+    const int t = rs[ir] - rs[x];
+    if (t < T) return idx[lpos[ls[l + 2] + t - 1]];
+  }
+  return idx[x];
+}
+
+__global__ void k_nr_apply(int n, const int* __restrict__ segof, const int* __restrict__ seg,
+                           const int* __restrict__ meta, const int* __restrict__ idx, const int* __restrict__ lf,
+                           const int* __restrict__ rf, const int* __restrict__ ls, const int* __restrict__ rs,
+                           const int* __restrict__ lpos, const int* __restrict__ rpos, int* __restrict__ out) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= n; q += gridDim.x * blockDim.x) {
+    if (q == 0) continue;
+    const int s = segof[q];
+    if (s < 0) { out[q] = idx[q]; continue; }
+    const int l = seg[2 * s], ir = seg[2 * s + 1];
+    const int pv = meta[4 * s], j = meta[4 * s + 2], T = meta[4 * s + 3];
+    if (q == l) out[q] = nr_newval(j, l, ir, T, idx, lf, rf, ls, rs, lpos, rpos);
+    else if (q == j) out[q] = pv;
+    else out[q] = nr_newval(q, l, ir, T, idx, lf, rf, ls, rs, lpos, rpos);
+  }
+}
+
+// children segments [l, j-1] and [i, ir]: partitioned further when they hold
+// at least M+1=8 elements, insertion-sorted otherwise
+__global__ void k_nr_newsegs(int nseg, const int* __restrict__ seg, int* __restrict__ meta,
+                             int* __restrict__ seg2, int* __restrict__ small, int* __restrict__ cnt,
+                             int small_cap) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
+    const int l = seg[2 * s], ir = seg[2 * s + 1];
+    const int i = meta[4 * s + 1], j = meta[4 * s + 2];
+    int ids[2] = {-1, -1};
+    const int lo[2] = {l, i}, hi[2] = {j - 1, ir};
+    for (int c = 0; c < 2; ++c) {
+      if (hi[c] - lo[c] >= 7) {
+        const int id = atomicAdd(&cnt[C_NSEG], 1);
+        seg2[2 * id] = lo[c];
+        seg2[2 * id + 1] = hi[c];
+        ids[c] = id;
+      } else if (hi[c] - lo[c] >= 1) {
+        const int id = atomicAdd(&cnt[C_NSMALL], 1);
+        if (id < small_cap) { small[2 * id] = lo[c]; small[2 * id + 1] = hi[c]; }
+        else atomicExch(&cnt[C_OVERFLOW], 1);
+      }
+    }
+    // reuse meta slots 1,2 for the children ids (i, j no longer needed after this)
+    meta[4 * s + 1] = ids[0];
+    meta[4 * s + 2] = ids[1];
+    meta[4 * s + 3] = j;  // boundary of the left child
+    meta[4 * s] = i;      // start of the right child
+  }
+}
+
+__global__ void k_nr_segof(int n, const int* __restrict__ seg, const int* __restrict__ meta,
+                           int* __restrict__ segof) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= n + 1; q += gridDim.x * blockDim.x) {
+    const int s = segof[q];
+    if (s < 0) continue;
+    const int l = seg[2 * s], ir = seg[2 * s + 1];
+    const int i = meta[4 * s], j = meta[4 * s + 3];
+    int ns = -1;
+    if (q >= l && q <= j - 1) ns = meta[4 * s + 1];
+    else if (q >= i && q <= ir) ns = meta[4 * s + 2];
+    segof[q] = ns;
+  }
+}
+
+// straight insertion of a small segment (LocalMinima.f90:967-976); the
+// reference's inner loop runs down to 1 but stops at position l-1 at the
+// latest because everything left of a segment is <= everything in it.
+__global__ void k_nr_insertion(int nsmall, const int* __restrict__ small, const double* __restrict__ arr,
+                               int* __restrict__ idx) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsmall; s += gridDim.x * blockDim.x) {
+    const int l = small[2 * s], ir = small[2 * s + 1];
+    for (int j = l + 1; j <= ir; ++j) {
+      const int indxt = idx[j];
+      const double a = arr[indxt];
+      int i = j - 1;
+      for (; i >= l; --i) {
+        if (arr[idx[i]] <= a) break;
+        idx[i + 1] = idx[i];
+      }
+      idx[i + 1] = indxt;
+    }
+  }
+}
+
+__global__ void k_rank_from_perm(int n, const int* __restrict__ idx1, int* __restrict__ rank) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    rank[idx1[t + 1] - 1] = t;
+}
+
+// ---- Boruvka under the rank order ------------------------------------------
+__global__ void k_mst_init(int nb, int* __restrict__ comp) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) comp[b] = b;
+}
+
+__global__ void k_mst_reset(int nb, int* __restrict__ mn) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) mn[b] = INT_MAX;
+}
+
+__global__ void k_mst_minedge(int ne, const int* __restrict__ b1, const int* __restrict__ b2,
+                              const int* __restrict__ rank, const int* __restrict__ comp, int* __restrict__ mn) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+    const int cu = comp[b1[e] - 1], cv = comp[b2[e] - 1];
+    if (cu == cv) continue;
+    atomicMin(&mn[cu], rank[e]);
+    atomicMin(&mn[cv], rank[e]);
+  }
+}
+
+__global__ void k_mst_hook(int nb, const int* __restrict__ idx1, const int* __restrict__ b1,
+                           const int* __restrict__ b2, const int* __restrict__ comp, const int* __restrict__ mn,
+                           int* __restrict__ next, int* __restrict__ inmst, int* __restrict__ cnt) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nb; c += gridDim.x * blockDim.x) {
+    next[c] = comp[c];
+    if (comp[c] != c) continue;
+    const int r = mn[c];
+    if (r == INT_MAX) continue;
+    const int e = idx1[r + 1] - 1;
+    const int cu = comp[b1[e] - 1], cv = comp[b2[e] - 1];
+    const int other = cu == c ? cv : cu;
+    inmst[e] = 1;
+    if (mn[other] == r && c < other) continue;  // mutual choice: the smaller id stays a root
+    next[c] = other;
+    cnt[C_CHANGED] = 1;
+  }
+}
+
+__global__ void k_mst_apply(int nb, const int* __restrict__ next, int* __restrict__ comp) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nb; c += gridDim.x * blockDim.x) comp[c] = next[c];
+}
+
+// one synchronous pointer-jumping round: out[c] = in[in[c]]
+__global__ void k_mst_jump(int nb, const int* __restrict__ in, int* __restrict__ out, int* __restrict__ cnt) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nb; c += gridDim.x * blockDim.x) {
+    const int r = in[c];
+    const int rr = in[r];
+    out[c] = rr;
+    if (rr != r) cnt[C_NOTFLAT] = 1;
+  }
+}
+
+// tree = accepted edges in rank order (Kruskal acceptance order)
+__global__ void k_tree_flags(int ne, const int* __restrict__ idx1, const int* __restrict__ inmst,
+                             int* __restrict__ flag) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t <= ne; t += gridDim.x * blockDim.x)
+    flag[t] = t < ne ? inmst[idx1[t + 1] - 1] : 0;
+}
+
+__global__ void k_tree_list(int ne, const int* __restrict__ idx1, const int* __restrict__ flag,
+                            const int* __restrict__ scan, int* __restrict__ tree) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ne; t += gridDim.x * blockDim.x)
+    if (flag[t]) tree[scan[t]] = idx1[t + 1] - 1;
+}
+
+// ---- order_tree: Euler tour over the tree arcs -------------------------------
+__global__ void k_arc_degree(int ntree, const int* __restrict__ tree, const int* __restrict__ b1,
+                             const int* __restrict__ b2, int* __restrict__ deg) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < ntree; x += gridDim.x * blockDim.x) {
+    const int e = tree[x];
+    atomicAdd(&deg[b1[e] - 1], 1);
+    atomicAdd(&deg[b2[e] - 1], 1);
+  }
+}
+
+__global__ void k_arc_fill(int ntree, const int* __restrict__ tree, const int* __restrict__ b1,
+                           const int* __restrict__ b2, const int* __restrict__ start, int* __restrict__ fill,
+                           int* __restrict__ adj, int* __restrict__ slot) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < ntree; x += gridDim.x * blockDim.x) {
+    const int e = tree[x];
+    const int u = b1[e] - 1, v = b2[e] - 1;
+    const int su = atomicAdd(&fill[u], 1);
+    adj[start[u] + su] = 2 * x;       // arc u -> v
+    slot[2 * x] = su;
+    const int sv = atomicAdd(&fill[v], 1);
+    adj[start[v] + sv] = 2 * x + 1;   // arc v -> u
+    slot[2 * x + 1] = sv;
+  }
+}
+
+__global__ void k_arc_tour(int ntree, int root, const int* __restrict__ tree, const int* __restrict__ b1,
+                           const int* __restrict__ b2, const int* __restrict__ start,
+                           const int* __restrict__ deg, const int* __restrict__ adj,
+                           const int* __restrict__ slot, unsigned long long* __restrict__ lst) {
+  const unsigned END = 0xffffffffu;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < 2 * ntree; a += gridDim.x * blockDim.x) {
+    const int e = tree[a >> 1];
+    const int y = (a & 1) ? b1[e] - 1 : b2[e] - 1;  // head of arc a
+    const int tw = a ^ 1;                           // twin arc y -> x
+    const int ns = (slot[tw] + 1) % deg[y];
+    unsigned succ = (unsigned)adj[start[y] + ns];
+    if (y == root && ns == 0) succ = END;
+    lst[a] = ((unsigned long long)succ << 32) | 1ull;
+  }
+}
+
+__global__ void k_copy_edges(int ne, const int* __restrict__ b1, const int* __restrict__ b2,
+                             const int* __restrict__ n1, const int* __restrict__ n2, int* __restrict__ ob1,
+                             int* __restrict__ ob2, int* __restrict__ on1, int* __restrict__ on2) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+    ob1[e] = b1[e]; ob2[e] = b2[e]; on1[e] = n1[e]; on2[e] = n2[e];
+  }
+}
+
+__global__ void k_orient_tree(int ntree, const int* __restrict__ tree, const unsigned long long* __restrict__ rk,
+                              const int* __restrict__ b1, const int* __restrict__ b2, const int* __restrict__ n1,
+                              const int* __restrict__ n2, int* __restrict__ ob1, int* __restrict__ ob2,
+                              int* __restrict__ on1, int* __restrict__ on2) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < ntree; x += gridDim.x * blockDim.x) {
+    const int e = tree[x];
+    const unsigned r_uv = (unsigned)rk[2 * x], r_vu = (unsigned)rk[2 * x + 1];
+    // the arc met first in the tour (larger distance to the end) leaves the parent
+    if (r_uv < r_vu) {
+      ob1[e] = b2[e]; ob2[e] = b1[e]; on1[e] = n2[e]; on2[e] = n1[e];
+    }
+  }
+}
+
+// correct_receivers_v2: redirect node_from to node_to and reverse the
+// receiver path from node_from down to the child basin's outlet
+__global__ void k_correct(int ntree, int nx, double dx, double dy, int nn, const int* __restrict__ tree,
+                          const int* __restrict__ ob2, const int* __restrict__ on1, const int* __restrict__ on2,
+                          const int* __restrict__ roots, int* rec, double* length, int* __restrict__ err) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < ntree; x += gridDim.x * blockDim.x) {
+    const int e = tree[x];
+    const int node_to = on1[e], node_from = on2[e];
+    if (node_from == -1) continue;
+    const int outlet_from = roots[ob2[e] - 1];
+    int next_node = rec[node_from];
+    int cur = node_from;
+    double prev = length[node_from];
+    rec[node_from] = node_to;
+    const double ddx = dx * (double)((node_from % nx) - (node_to % nx));
+    const double ddy = dy * (double)((node_from / nx) - (node_to / nx));
+    length[node_from] = sqrt(ddx * ddx + ddy * ddy);
+    int guard = 0;
+    while (cur != outlet_from) {
+      if (++guard > nn) { atomicExch(err, DEV_STACK_ERROR); break; }
+      const int rcv_next = rec[next_node];
+      rec[next_node] = cur;
+      const double tmp = prev;
+      prev = length[next_node];
+      length[next_node] = tmp;
+      cur = next_node;
+      next_node = rcv_next;
+    }
+  }
+}
+
+__global__ void k_count_active_roots(Bounds bd, const int* __restrict__ rec, int* __restrict__ cnt) {
+  const int nn = bd.nx * bd.ny;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x)
+    if (rec[k] == k && !is_bc_node(bd, k % bd.nx, k / bd.nx)) atomicAdd(&cnt[C_NLOCMIN_AFTER], 1);
+}
+
+__global__ void k_copy_nroots(const int* src, int* cnt) {
+  cnt[C_NBASINS] = *src;
+  cnt[C_NLOCMIN] = 0;
+  cnt[C_BASIN0] = INT_MAX;
+  for (int i = C_NEDGE; i <= C_OVERFLOW; ++i) cnt[i] = 0;
+}
+
+}  // namespace
+
+// Runs the exact NR index sort on w[0..n-1]; result: c.nr_idx[1..n] holds the
+// 1-based ids in sorted order.  Returns false on buffer overflow.
+static bool nr_indexx(Ctx& c, int n, const double* w) {
+  const double* arr = w - 1;  // 1-based
+  int* idx = c.nr_idx;
+  int* idx2 = c.nr_idx2;
+  int* seg = c.nr_seg;
+  int* seg2 = c.nr_seg2;
+  const int small_cap = (int)(c.conn_cap / 2 + 8);
+  k_nr_init<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, idx, c.nr_segof, seg, c.nr_small, c.d_cnt);
+  c.count_launch();
+  fetch_counters(c, 10);
+  int nseg = c.h_cnt[C_NSEG];
+  int levels = 0;
+  while (nseg > 0) {
+    if (++levels > 200) { c.err = "NR sort emulation: too many levels"; return false; }
+    k_nr_median<<<grid1d(nseg), kBlock, 0, c.stream>>>(nseg, seg, arr, idx, c.nr_piv, c.nr_segmeta);
+    k_nr_flags<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, c.nr_segof, seg, c.nr_piv, arr, idx, c.nr_lf, c.nr_rf);
+    exclusive_scan_int(c, c.nr_lf, c.nr_ls, n + 2);
+    exclusive_scan_int(c, c.nr_rf, c.nr_rs, n + 2);
+    k_nr_scatter<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, c.nr_lf, c.nr_rf, c.nr_ls, c.nr_rs, c.nr_lpos, c.nr_rpos);
+    k_nr_cross<<<grid1d(nseg), kBlock, 0, c.stream>>>(nseg, seg, c.nr_ls, c.nr_rs, c.nr_lpos, c.nr_rpos, c.nr_segmeta);
+    k_nr_apply<<<grid1d(n + 1), kBlock, 0, c.stream>>>(n, c.nr_segof, seg, c.nr_segmeta, idx, c.nr_lf, c.nr_rf,
+                                                        c.nr_ls, c.nr_rs, c.nr_lpos, c.nr_rpos, idx2);
+    std::swap(idx, idx2);
+    cudaMemsetAsync(c.d_cnt + C_NSEG, 0, sizeof(int), c.stream);
+    k_nr_newsegs<<<grid1d(nseg), kBlock, 0, c.stream>>>(nseg, seg, c.nr_segmeta, seg2, c.nr_small, c.d_cnt, small_cap);
+    k_nr_segof<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, seg, c.nr_segmeta, c.nr_segof);
+    c.count_launch(7);
+    std::swap(seg, seg2);
+    fetch_counters(c, 10);
+    nseg = c.h_cnt[C_NSEG];
+    if (c.h_cnt[C_OVERFLOW]) { c.err = "NR sort emulation: small-segment buffer overflow"; return false; }
+  }
+  const int nsmall = c.h_cnt[C_NSMALL];
+  if (nsmall > 0) {
+    k_nr_insertion<<<grid1d(nsmall), kBlock, 0, c.stream>>>(nsmall, c.nr_small, arr, idx);
+    c.count_launch();
+  }
+  if (idx != c.nr_idx)
+    cudaMemcpyAsync(c.nr_idx, idx, sizeof(int) * (n + 2), cudaMemcpyDeviceToDevice, c.stream);
+  return true;
+}
+
+bool local_minima(Ctx& c) {
+  const int nn = c.nn;
+  cudaStream_t st = c.stream;
+  if (c.capture) {
+    cudaMemcpyAsync(c.rec_pre, c.rec, sizeof(int) * nn, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(c.stack_pre, c.stack, sizeof(int) * nn, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(c.length_pre, c.length, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st);
+  }
+  // ---- compute_basins: basin id = number of roots met so far along the stack
+  k_copy_nroots<<<1, 1, 0, st>>>(c.s_scan + nn, c.d_cnt);
+  k_pos_root_flags<<<grid1d(nn), kBlock, 0, st>>>(nn, c.stack, c.rec, c.s_flag);
+  c.count_launch(2);
+  inclusive_scan_int(c, c.s_flag, c.s_scan, nn);
+  k_basins<<<grid1d(nn), kBlock, 0, st>>>(nn, c.stack, c.s_scan, c.basins);
+  c.count_launch();
+  fetch_counters(c, 10);
+  const int nroots = c.h_cnt[C_NBASINS];
+  k_roots_scan<<<grid1d(nroots), kBlock, 0, st>>>(c.bd, nroots, c.s_roots, c.d_cnt);
+  c.count_launch();
+  fetch_counters(c, 10);
+  c.nbasins = nroots;
+  c.nlocmin_before = c.h_cnt[C_NLOCMIN];
+  c.basin0 = c.h_cnt[C_BASIN0] == INT_MAX ? -1 : c.h_cnt[C_BASIN0];
+  c.nconn = 0;
+  c.tree_size = 0;
+  c.nlocmin_after = c.nlocmin_before;
+  if (c.nlocmin_before == 0 && !c.capture) return true;  // no pit: receivers unchanged
+  if (c.basin0 < 1) {
+    c.err = "LocalMinima: no basin drains to a fixed boundary (the reference indexes out of bounds here)";
+    return false;
+  }
+  // ---- connect_basins
+  size_t cap = 1024;
+  while (cap < 16 * (size_t)nroots && cap < c.hash_cap) cap <<= 1;
+  cudaMemsetAsync(c.ht_key, 0xff, sizeof(unsigned long long) * cap, st);
+  cudaMemsetAsync(c.ht_wmin, 0xff, sizeof(unsigned long long) * cap, st);
+  cudaMemsetAsync(c.ht_first, 0xff, sizeof(unsigned) * cap, st);
+  cudaMemsetAsync(c.ht_best, 0xff, sizeof(unsigned) * cap, st);
+  k_conn_pass<0><<<grid1d(nn), kBlock, 0, st>>>(c.bd, c.basins, c.s_roots, c.pos, c.h, c.ht_key, c.ht_wmin,
+                                                 c.ht_first, c.ht_best, cap, c.d_cnt);
+  k_conn_pass<1><<<grid1d(nn), kBlock, 0, st>>>(c.bd, c.basins, c.s_roots, c.pos, c.h, c.ht_key, c.ht_wmin,
+                                                 c.ht_first, c.ht_best, cap, c.d_cnt);
+  k_conn_compact<<<grid1d(cap), kBlock, 0, st>>>(c.bd, cap, c.ht_key, c.ht_first, c.ht_best, c.stack, c.h,
+                                                  c.conn_cap, c.e_key, c.r_b1, c.r_b2, c.r_n1, c.r_n2,
+                                                  c.r_w, c.d_cnt);
+  k_conn_virtual<<<grid1d(nroots), kBlock, 0, st>>>(c.bd, nroots, c.s_roots, c.pos, c.conn_cap, c.e_key, c.r_b1,
+                                                     c.r_b2, c.r_n1, c.r_n2, c.r_w, c.d_cnt);
+  c.count_launch(4);
+  fetch_counters(c, 10);
+  if (c.h_cnt[C_OVERFLOW]) { c.err = "connect_basins: edge buffer overflow"; return false; }
+  const int ne = c.h_cnt[C_NEDGE];
+  c.nconn = ne;
+  if (ne > 6 * nroots) {
+    c.err = "connect_basins: nconn exceeds nconn_max=6*nbasins (the reference overflows here)";
+    return false;
+  }
+  k_iota<<<grid1d(ne), kBlock, 0, st>>>(ne, c.e_idx);
+  c.count_launch();
+  int bits = 1;
+  while (bits < 32 && (1ull << bits) < 8ull * (unsigned long long)nn) ++bits;
+  sort_pairs_u32(c, c.e_key, c.e_key2, c.e_idx, c.e_idx2, ne, bits);
+  k_conn_gather<<<grid1d(ne), kBlock, 0, st>>>(ne, c.e_idx2, c.r_b1, c.r_b2, c.r_n1, c.r_n2, c.r_w, c.e_b1,
+                                                c.e_b2, c.e_n1, c.e_n2, c.e_w);
+  c.count_launch();
+  // ---- loc_min_3_indexx + Kruskal
+  if (!nr_indexx(c, ne, c.e_w)) return false;
+  k_rank_from_perm<<<grid1d(ne), kBlock, 0, st>>>(ne, c.nr_idx, c.e_rank);
+  cudaMemsetAsync(c.e_inmst, 0, sizeof(int) * ne, st);
+  k_mst_init<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_comp);
+  c.count_launch(2);
+  for (int round = 0; round < 64; ++round) {
+    k_mst_reset<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_min);
+    k_mst_minedge<<<grid1d(ne), kBlock, 0, st>>>(ne, c.e_b1, c.e_b2, c.e_rank, c.mst_comp, c.mst_min);
+    cudaMemsetAsync(c.d_cnt + C_CHANGED, 0, sizeof(int), st);
+    k_mst_hook<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.nr_idx, c.e_b1, c.e_b2, c.mst_comp, c.mst_min,
+                                                   c.mst_next, c.e_inmst, c.d_cnt);
+    k_mst_apply<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_next, c.mst_comp);
+    c.count_launch(4);
+    fetch_counters(c, 12);
+    if (!c.h_cnt[C_CHANGED]) break;
+    // flatten the hook forest: comp[c] <- root of c
+    for (int jr = 0; jr < 40; ++jr) {
+      cudaMemsetAsync(c.d_cnt + C_NOTFLAT, 0, sizeof(int), st);
+      k_mst_jump<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_comp, c.mst_next, c.d_cnt);
+      k_mst_jump<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_next, c.mst_comp, c.d_cnt);
+      c.count_launch(2);
+      fetch_counters(c, 12);
+      if (!c.h_cnt[C_NOTFLAT]) break;
+    }
+  }
+  k_tree_flags<<<grid1d(ne + 1), kBlock, 0, st>>>(ne, c.nr_idx, c.e_inmst, c.nr_lf);
+  c.count_launch();
+  exclusive_scan_int(c, c.nr_lf, c.nr_ls, ne + 1);
+  k_tree_list<<<grid1d(ne), kBlock, 0, st>>>(ne, c.nr_idx, c.nr_lf, c.nr_ls, c.tree);
+  cudaMemcpyAsync(c.d_cnt + C_NTREE, c.nr_ls + ne, sizeof(int), cudaMemcpyDeviceToDevice, st);
+  c.count_launch();
+  fetch_counters(c, 10);
+  const int ntree = c.h_cnt[C_NTREE];
+  c.tree_size = ntree;
+  if (ntree != nroots - 1) {
+    c.err = "LocalMinima: the basin graph is not connected";
+    return false;
+  }
+  // ---- order_tree
+  k_copy_edges<<<grid1d(ne), kBlock, 0, st>>>(ne, c.e_b1, c.e_b2, c.e_n1, c.e_n2, c.o_b1, c.o_b2, c.o_n1,
+                                              c.o_n2);
+  c.count_launch();
+  if (ntree > 0) {
+    cudaMemsetAsync(c.arc_deg, 0, sizeof(int) * (nroots + 1), st);
+    k_arc_degree<<<grid1d(ntree), kBlock, 0, st>>>(ntree, c.tree, c.e_b1, c.e_b2, c.arc_deg);
+    c.count_launch();
+    exclusive_scan_int(c, c.arc_deg, c.arc_start, nroots + 1);
+    cudaMemsetAsync(c.mst_min, 0, sizeof(int) * nroots, st);
+    k_arc_fill<<<grid1d(ntree), kBlock, 0, st>>>(ntree, c.tree, c.e_b1, c.e_b2, c.arc_start, c.mst_min,
+                                                  c.arc_adj, c.arc_slot);
+    k_arc_tour<<<grid1d(2 * ntree), kBlock, 0, st>>>(ntree, c.basin0 - 1, c.tree, c.e_b1, c.e_b2, c.arc_start,
+                                                      c.arc_deg, c.arc_adj, c.arc_slot, c.s_list_a);
+    c.count_launch(2);
+    unsigned long long* rk = list_rank(c, 2 * (size_t)ntree, c.s_list_a, c.s_list_b);
+    k_orient_tree<<<grid1d(ntree), kBlock, 0, st>>>(ntree, c.tree, rk, c.e_b1, c.e_b2, c.e_n1, c.e_n2, c.o_b1,
+                                                     c.o_b2, c.o_n1, c.o_n2);
+    // ---- correct_receivers_v2
+    k_correct<<<grid1d(ntree, 128), 128, 0, st>>>(ntree, c.nx, c.dx, c.dy, nn, c.tree, c.o_b2, c.o_n1, c.o_n2,
+                                                   c.s_roots, c.rec, c.length, c.d_err);
+    c.count_launch(2);
+  }
+  if (c.capture) {
+    k_count_active_roots<<<grid1d(nn), kBlock, 0, st>>>(c.bd, c.rec, c.d_cnt);
+    c.count_launch();
+    fetch_counters(c, 10);
+    c.nlocmin_after = c.h_cnt[C_NLOCMIN_AFTER];
+  }
+  // loc_min_3_find_donors + loc_min_3_find_stack
+  build_stack(c, c.rec, c.ndon, c.don, c.stack, c.pos, c.size);
+  return true;
+}
+
+}  // namespace fsb

@@ -1,0 +1,425 @@
+"""Drop-in ``fastscapelib_fortran`` for the continental time step on a B200.
+
+This package exposes the reference's Python API -- the f2py module built from
+src/FastScape_api.f90 -- with the same routine names and argument orders:
+
+    fastscape_init, fastscape_set_nx_ny, fastscape_setup, fastscape_set_xl_yl,
+    fastscape_set_dt, fastscape_set_erosional_parameters, fastscape_set_u,
+    fastscape_set_bc, fastscape_init_h, fastscape_execute_step,
+    fastscape_copy_h, fastscape_copy_drainage_area, fastscape_get_step, ...
+
+The model state lives in one device arena (a torch uint8 tensor) and every
+operation runs as hand-written sm_100a CUDA kernels in ``libfsgpu.so``,
+called through its C ABI (include/fastscape_b200.h) with ctypes.  There is no
+CPU fallback: importing this package fails if the library is missing and
+``fastscape_setup`` fails if no CUDA device is present.
+
+Differences from the reference, by design:
+  * errors raise ``RuntimeError`` where the Fortran executes ``stop``;
+  * array arguments may also be torch tensors; CUDA tensors are read/written
+    on the device without a host round trip;
+  * ``FastScape`` objects give independent instances (the reference keeps one
+    global model per process; the module-level functions drive a default one).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+try:
+    import torch
+except ImportError as exc:  # pragma: no cover - torch is part of the runtime
+    raise ImportError("fastscapelib_fortran (B200) needs torch for device memory") from exc
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfsgpu.so")
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing: build the CUDA library first (make -C {os.path.dirname(_HERE)})")
+
+_lib = ctypes.CDLL(LIB_PATH)
+
+FSB_HOST, FSB_DEVICE = 0, 1
+FIELDS = {"h": 0, "basement": 1, "total_erosion": 2, "drainage_area": 3, "erosion_rate": 4,
+          "lake_depth": 5, "length": 6, "hwater": 7, "sedflux": 8, "u": 10, "precip": 11,
+          "kf": 12, "kd": 13}
+INT_FIELDS = {"rec": 0, "ndon": 1, "stack": 2, "mnrec": 3, "mstack": 4, "basins": 5,
+              "rec_pre": 6, "stack_pre": 7}
+SLOT_FIELDS = {"don": 0, "mrec": 1, "mwrec": 2, "mlrec": 3}
+
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_d = ctypes.c_double
+
+
+def _sig(name, *args, res=ctypes.c_int):
+    f = getattr(_lib, name)
+    f.argtypes = list(args)
+    f.restype = res
+    return f
+
+
+_lib.fsb_last_error.restype = ctypes.c_char_p
+_sig("fsb_create", ctypes.POINTER(_vp))
+_sig("fsb_destroy", _vp)
+_sig("fsb_set_nx_ny", _vp, _i, _i)
+_sig("fsb_workspace_bytes", _vp, ctypes.POINTER(ctypes.c_size_t))
+_sig("fsb_setup", _vp, _vp, ctypes.c_size_t)
+_sig("fsb_set_stream", _vp, _vp)
+_sig("fsb_set_xl_yl", _vp, _d, _d)
+_sig("fsb_set_dt", _vp, _d)
+_sig("fsb_set_erosional_parameters", _vp, _vp, _d, _d, _d, _vp, _d, _d, _d, _d, _i)
+_sig("fsb_set_bc", _vp, _i)
+for _n in ("fsb_set_u", "fsb_init_h", "fsb_set_h", "fsb_set_basement", "fsb_set_precip"):
+    _sig(_n, _vp, _vp, _i)
+_sig("fsb_reset_cumulative_erosion", _vp)
+_sig("fsb_execute_step", _vp)
+_sig("fsb_execute_steps", _vp, _i)
+_sig("fsb_get_step", _vp, ctypes.POINTER(_i))
+_sig("fsb_get_sizes", _vp, ctypes.POINTER(_i), ctypes.POINTER(_i))
+_sig("fsb_copy_field", _vp, _i, _vp, _i)
+_sig("fsb_field_device_ptr", _vp, _i, ctypes.POINTER(_vp))
+_sig("fsb_copy_int_field", _vp, _i, _vp, _i)
+_sig("fsb_copy_slots", _vp, _i, _vp, _i)
+_sig("fsb_set_capture", _vp, _i)
+_sig("fsb_locmin_counts", _vp, _vp)
+_sig("fsb_copy_locmin", _vp, *([_vp] * 11))
+_sig("fsb_synchronize", _vp)
+_sig("fsb_launch_count", _vp, res=ctypes.c_longlong)
+_sig("fsb_set_profile", _vp, _i)
+_sig("fsb_stage_times", _vp, _vp, _vp, _i, _i)
+
+STAGES = ("uplift", "receivers", "stack", "local_minima", "lake_fill", "mfd_receivers",
+          "drainage_area", "stream_power", "diffusion")
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError(_lib.fsb_last_error().decode())
+
+
+class FastScape:
+    """One continental-step model instance resident on a CUDA device."""
+
+    def __init__(self, device: int | str | torch.device | None = None):
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else
+                                   torch.device(device).index or 0)
+        h = _vp()
+        _check(_lib.fsb_create(ctypes.byref(h)))
+        self._h = h
+        self._arena = None
+        self.nx = self.ny = 0
+
+    # -- lifecycle ---------------------------------------------------------
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                _lib.fsb_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    def _stream(self):
+        return torch.cuda.current_stream(self.device)
+
+    def set_nx_ny(self, nx: int, ny: int) -> None:
+        self.nx, self.ny = int(nx), int(ny)
+        _check(_lib.fsb_set_nx_ny(self._h, self.nx, self.ny))
+
+    @property
+    def nn(self) -> int:
+        return self.nx * self.ny
+
+    def workspace_bytes(self) -> int:
+        b = ctypes.c_size_t(0)
+        _check(_lib.fsb_workspace_bytes(self._h, ctypes.byref(b)))
+        return b.value
+
+    def setup(self) -> None:
+        if not torch.cuda.is_available():
+            raise RuntimeError("fastscape_setup: no CUDA device (this build has no CPU path)")
+        nbytes = self.workspace_bytes()
+        with torch.cuda.device(self.device):
+            self._arena = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            _check(_lib.fsb_set_stream(self._h, self._stream().cuda_stream))
+            _check(_lib.fsb_setup(self._h, self._arena.data_ptr(), nbytes))
+
+    def destroy(self) -> None:
+        if self._h:
+            _lib.fsb_destroy(self._h)
+            self._h = None
+        self._arena = None
+
+    # -- array marshalling -------------------------------------------------
+    def _in(self, a):
+        """(pointer, where, keepalive) for an intent(in) node array."""
+        if isinstance(a, torch.Tensor):
+            t = a.detach().reshape(-1)
+            if t.dtype != torch.float64:
+                t = t.to(torch.float64)
+            if t.is_cuda:
+                t = t.to(self.device).contiguous()
+                where = FSB_DEVICE
+            else:
+                t = t.contiguous()
+                where = FSB_HOST
+            if t.numel() < self.nn:
+                raise ValueError(f"array of size {t.numel()} is smaller than nx*ny={self.nn}")
+            return t.data_ptr(), where, t
+        arr = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+        if arr.size < self.nn:
+            raise ValueError(f"array of size {arr.size} is smaller than nx*ny={self.nn}")
+        return arr.ctypes.data, FSB_HOST, arr
+
+    def _out(self, buf, dtype=np.float64, per_node=1):
+        """(pointer, where) of an intent(inout) buffer filled in place."""
+        n = self.nn * per_node
+        if isinstance(buf, torch.Tensor):
+            tdt = {np.float64: torch.float64, np.int32: torch.int32}[dtype]
+            if buf.dtype != tdt or not buf.is_contiguous() or buf.numel() < n:
+                raise ValueError(f"output tensor must be contiguous {tdt} with >= {n} elements")
+            return buf.data_ptr(), FSB_DEVICE if buf.is_cuda else FSB_HOST
+        if not isinstance(buf, np.ndarray) or buf.dtype != dtype or not buf.flags.c_contiguous \
+                or buf.size < n:
+            raise ValueError(f"output array must be a C-contiguous {np.dtype(dtype).name} ndarray "
+                             f"with >= {n} elements (filled in place)")
+        return buf.ctypes.data, FSB_HOST
+
+    # -- setters (FastScape_api.f90) -----------------------------------------
+    def set_xl_yl(self, xl: float, yl: float) -> None:
+        _check(_lib.fsb_set_xl_yl(self._h, float(xl), float(yl)))
+
+    def set_dt(self, dt: float) -> None:
+        _check(_lib.fsb_set_dt(self._h, float(dt)))
+
+    def set_erosional_parameters(self, kf, kfsed, m, n, kd, kdsed, g1, g2, p) -> None:
+        pkf, wkf, k1 = self._in(kf)
+        pkd, wkd, k2 = self._in(kd)
+        if wkf != wkd:
+            k1 = self._in(torch.as_tensor(np.asarray(kf, dtype=np.float64)).to(self.device))[2]
+            k2 = self._in(torch.as_tensor(np.asarray(kd, dtype=np.float64)).to(self.device))[2]
+            pkf, pkd, wkf = k1.data_ptr(), k2.data_ptr(), FSB_DEVICE
+        _check(_lib.fsb_set_erosional_parameters(self._h, pkf, float(kfsed), float(m), float(n),
+                                                 pkd, float(kdsed), float(g1), float(g2),
+                                                 float(p), wkf))
+        self._sync_if_device(wkf)
+
+    def set_bc(self, bc: int) -> None:
+        _check(_lib.fsb_set_bc(self._h, int(bc)))
+
+    def _set(self, fn, a) -> None:
+        ptr, where, keep = self._in(a)
+        _check(fn(self._h, ptr, where))
+        self._sync_if_device(where)
+        del keep
+
+    def _sync_if_device(self, where):
+        if where == FSB_DEVICE:
+            self._stream().synchronize()
+
+    def set_u(self, u) -> None:
+        self._set(_lib.fsb_set_u, u)
+
+    def init_h(self, h) -> None:
+        self._set(_lib.fsb_init_h, h)
+
+    def set_h(self, h) -> None:
+        self._set(_lib.fsb_set_h, h)
+
+    def set_basement(self, b) -> None:
+        self._set(_lib.fsb_set_basement, b)
+
+    def set_precip(self, p) -> None:
+        self._set(_lib.fsb_set_precip, p)
+
+    def reset_cumulative_erosion(self) -> None:
+        _check(_lib.fsb_reset_cumulative_erosion(self._h))
+
+    # -- stepping ------------------------------------------------------------
+    def execute_step(self, nsteps: int = 1) -> None:
+        _check(_lib.fsb_execute_steps(self._h, int(nsteps)))
+
+    def get_step(self) -> int:
+        s = _i(0)
+        _check(_lib.fsb_get_step(self._h, ctypes.byref(s)))
+        return s.value
+
+    def get_sizes(self):
+        return self.nx, self.ny
+
+    def synchronize(self) -> None:
+        _check(_lib.fsb_synchronize(self._h))
+
+    def launch_count(self) -> int:
+        return int(_lib.fsb_launch_count(self._h))
+
+    def set_profile(self, on: bool = True) -> None:
+        """Time every stage with CUDA events on the instance's stream."""
+        _check(_lib.fsb_set_profile(self._h, 1 if on else 0))
+
+    def stage_times(self, reset: bool = False) -> dict:
+        """Accumulated device milliseconds and call counts per stage."""
+        ms = np.zeros(len(STAGES), np.float64)
+        calls = np.zeros(len(STAGES), np.int64)
+        _check(_lib.fsb_stage_times(self._h, ms.ctypes.data, calls.ctypes.data, len(STAGES),
+                                    1 if reset else 0))
+        return {s: (float(ms[i]), int(calls[i])) for i, s in enumerate(STAGES)}
+
+    # -- copy-outs -------------------------------------------------------------
+    def copy(self, name: str, buf) -> None:
+        ptr, where = self._out(buf)
+        _check(_lib.fsb_copy_field(self._h, FIELDS[name], ptr, where))
+        self._sync_if_device(where)
+
+    def field(self, name: str) -> torch.Tensor:
+        """Zero-copy float64 view of a device field (shape (ny, nx))."""
+        p = _vp()
+        _check(_lib.fsb_field_device_ptr(self._h, FIELDS[name], ctypes.byref(p)))
+        off = p.value - self._arena.data_ptr()
+        return self._arena[off:off + 8 * self.nn].view(torch.float64).view(self.ny, self.nx)
+
+    def copy_int(self, name: str) -> np.ndarray:
+        out = np.empty(self.nn, dtype=np.int32)
+        _check(_lib.fsb_copy_int_field(self._h, INT_FIELDS[name], out.ctypes.data, FSB_HOST))
+        return out
+
+    def copy_slots(self, name: str) -> np.ndarray:
+        fid = SLOT_FIELDS[name]
+        out = np.empty((self.nn, 8), dtype=np.int32 if fid < 2 else np.float64)
+        _check(_lib.fsb_copy_slots(self._h, fid, out.ctypes.data, FSB_HOST))
+        return out
+
+    def set_capture(self, on: bool = True) -> None:
+        _check(_lib.fsb_set_capture(self._h, 1 if on else 0))
+
+    def locmin_debug(self) -> dict:
+        cnt = np.zeros(6, dtype=np.int32)
+        _check(_lib.fsb_locmin_counts(self._h, cnt.ctypes.data))
+        nb, basin0, nconn, ntree, nbefore, nafter = (int(x) for x in cnt)
+        a = {k: np.zeros(max(nconn, 1), dtype=np.int32) for k in
+             ("b1", "b2", "n1", "n2", "sort_id", "ob1", "ob2", "on1", "on2")}
+        a["w"] = np.zeros(max(nconn, 1), dtype=np.float64)
+        a["tree"] = np.zeros(max(ntree, 1), dtype=np.int32)
+        _check(_lib.fsb_copy_locmin(self._h, *(a[k].ctypes.data for k in
+                                               ("b1", "b2", "n1", "n2", "w", "sort_id", "tree",
+                                                "ob1", "ob2", "on1", "on2"))))
+        out = {k: v[:nconn] for k, v in a.items() if k != "tree"}
+        out["tree"] = a["tree"][:ntree]
+        out.update(nbasins=nb, basin0=basin0, nconn=nconn, tree_size=ntree,
+                   nlocmin_before=nbefore, nlocmin_after=nafter)
+        return out
+
+
+# ---------------------------------------------------------------------------
+# Module-level API of the reference (one default instance per process)
+_default: FastScape | None = None
+
+
+def _inst() -> FastScape:
+    if _default is None:
+        raise RuntimeError("fastscape_init has not been called")
+    return _default
+
+
+def fastscape_init():
+    """FastScape_Init (api:146)."""
+    global _default
+    if _default is not None:
+        _default.destroy()
+    _default = FastScape()
+
+
+def fastscape_set_nx_ny(nnx, nny):
+    _inst().set_nx_ny(nnx, nny)
+
+
+def fastscape_setup():
+    _inst().setup()
+
+
+def fastscape_destroy():
+    global _default
+    if _default is not None:
+        _default.destroy()
+    _default = None
+
+
+def fastscape_set_xl_yl(xxl, yyl):
+    _inst().set_xl_yl(xxl, yyl)
+
+
+def fastscape_set_dt(dtt):
+    _inst().set_dt(dtt)
+
+
+def fastscape_set_erosional_parameters(kkf, kkfsed, mm, nnn, kkd, kkdsed, gg1, gg2, pp):
+    _inst().set_erosional_parameters(kkf, kkfsed, mm, nnn, kkd, kkdsed, gg1, gg2, pp)
+
+
+def fastscape_set_bc(jbc):
+    _inst().set_bc(jbc)
+
+
+def fastscape_set_u(up):
+    _inst().set_u(up)
+
+
+def fastscape_init_h(hp):
+    _inst().init_h(hp)
+
+
+def fastscape_set_h(hp):
+    _inst().set_h(hp)
+
+
+def fastscape_set_basement(bp):
+    _inst().set_basement(bp)
+
+
+def fastscape_set_precip(precipp):
+    _inst().set_precip(precipp)
+
+
+def fastscape_reset_cumulative_erosion():
+    _inst().reset_cumulative_erosion()
+
+
+def fastscape_execute_step():
+    _inst().execute_step()
+
+
+def fastscape_get_step():
+    return _inst().get_step()
+
+
+def fastscape_get_sizes():
+    return _inst().get_sizes()
+
+
+def fastscape_copy_h(hp):
+    _inst().copy("h", hp)
+
+
+def fastscape_copy_drainage_area(ap):
+    _inst().copy("drainage_area", ap)
+
+
+def fastscape_copy_basement(bp):
+    _inst().copy("basement", bp)
+
+
+def fastscape_copy_total_erosion(etotp):
+    _inst().copy("total_erosion", etotp)
+
+
+def fastscape_copy_erosion_rate(eratep):
+    _inst().copy("erosion_rate", eratep)
+
+
+def fastscape_copy_lake_depth(lp):
+    _inst().copy("lake_depth", lp)
+
+
+__all__ = [n for n in dir() if n.startswith("fastscape_")] + ["FastScape", "LIB_PATH"]

@@ -1,0 +1,157 @@
+"""GPU parity: the CUDA library (through its C ABI) against the oracle.
+
+Tolerances (stated here, checked below):
+  * single flow direction (p < -1.5): every integer artefact (receivers,
+    donors, stack, basins, conn list, sort permutation, MST, orientation) is
+    bit-exact and every float64 field is bit-exact, step after step;
+  * multiple flow direction: receivers, donors, stack, basins, conn list,
+    MST and mrec/mnrec are bit-exact; float64 fields agree to 1e-9 relative per
+    step (the accumulation sums donors in a different, equally valid order);
+    the multiple-flow stack is a topological order but not the reference's
+    LIFO order.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from fastscapelib_fortran import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+FLOAT_FIELDS = ("h", "drainage_area", "total_erosion", "erosion_rate", "basement", "lake_depth")
+
+
+def make_gpu(wl):
+    import fastscapelib_fortran as fs
+    g = fs.FastScape()
+    g.set_nx_ny(wl.nx, wl.ny)
+    g.setup()
+    g.set_xl_yl(wl.xl, wl.yl)
+    g.set_dt(wl.dt)
+    g.init_h(wl.h0.copy())
+    g.set_erosional_parameters(wl.kf, wl.kfsed, wl.m, wl.n, wl.kd, wl.kdsed, wl.g1, wl.g2, wl.p)
+    g.set_u(wl.u)
+    g.set_bc(wl.bc)
+    g.set_capture(True)
+    return g
+
+
+def gpu_float(g, name):
+    out = np.empty(g.nn, np.float64)
+    g.copy(name, out)
+    return out
+
+
+def compare_locmin(g, exact=True):
+    dg, do = g.locmin_debug(), O.locmin_debug()
+    for k in ("nbasins", "basin0", "nconn", "tree_size", "nlocmin_before", "nlocmin_after"):
+        assert dg[k] == do[k], (k, dg[k], do[k])
+    assert np.array_equal(g.copy_int("basins"), O.copy_int("basins"))
+    for k in ("b1", "b2", "n1", "n2", "w", "sort_id", "tree", "ob1", "ob2", "on1", "on2"):
+        assert np.array_equal(dg[k], do[k]), k
+
+
+def compare_routing(g):
+    assert np.array_equal(g.copy_int("rec_pre"), O.copy_int("rec_pre"))
+    assert np.array_equal(g.copy_int("stack_pre"), O.copy_int("stack_pre"))
+    compare_locmin(g)
+    assert np.array_equal(g.copy_int("rec"), O.copy_int("rec"))
+    assert np.array_equal(g.copy_int("stack"), O.copy_int("stack"))
+    nd = g.copy_int("ndon")
+    assert np.array_equal(nd, O.copy_int("ndon"))
+    dg, do = g.copy_slots("don"), O.copy_slots("don")
+    mask = np.arange(8)[None, :] < nd[:, None]
+    assert np.array_equal(dg[mask], do[mask])
+
+
+def rel_err(a, b):
+    scale = np.maximum(np.abs(b), 1.0)
+    return float(np.max(np.abs(a - b) / scale))
+
+
+@pytest.mark.parametrize("nx,ny,bc", [(101, 101, 1111), (64, 48, 1010), (57, 71, 101), (40, 40, 1000)])
+def test_sfd_bit_exact(nx, ny, bc):
+    wl = W.plain_d8(nx, ny, seed=nx + ny)
+    wl.bc = bc
+    wl.apply(O)
+    g = make_gpu(wl)
+    for step in range(12):
+        O.fastscape_execute_step()
+        g.execute_step()
+        compare_routing(g)
+        for f in FLOAT_FIELDS + ("length",):
+            a, b = gpu_float(g, f), O.copy_double(f)
+            assert np.array_equal(a, b), (step, f, rel_err(a, b))
+    assert g.get_step() == O.fastscape_get_step() == 12
+
+
+@pytest.mark.parametrize("n", [1.0, 1.5])
+def test_sfd_newton_bit_exact(n):
+    wl = W.plain_d8(61, 53, seed=5)
+    wl.n = n
+    wl.apply(O)
+    g = make_gpu(wl)
+    for _ in range(6):
+        O.fastscape_execute_step()
+        g.execute_step()
+        compare_routing(g)
+        for f in FLOAT_FIELDS:
+            a, b = gpu_float(g, f), O.copy_double(f)
+            assert rel_err(a, b) <= 1e-12, (f, rel_err(a, b))
+
+
+@pytest.mark.parametrize("nx,ny,bc,n,p", [(65, 65, 1010, 1.5, 1.1), (48, 56, 1111, 1.0, 1.0),
+                                           (50, 44, 101, 1.0, -1.0)])
+def test_mfd_per_step(nx, ny, bc, n, p):
+    wl = W.mfd(nx, ny, seed=nx, n=n, p=p, bc=bc)
+    wl.apply(O)
+    g = make_gpu(wl)
+    for step in range(6):
+        # start both from the oracle's state so each step is compared on its own
+        h = O.copy_double("h")
+        g.set_h(h)
+        g.set_basement(O.copy_double("basement"))
+        O.fastscape_execute_step()
+        g.execute_step()
+        compare_routing(g)
+        mn = g.copy_int("mnrec")
+        assert np.array_equal(mn, O.copy_int("mnrec"))
+        mg, mo = g.copy_slots("mrec"), O.copy_slots("mrec")
+        mask = np.arange(8)[None, :] < mn[:, None]
+        assert np.array_equal(mg[mask], mo[mask])
+        wg, wo = g.copy_slots("mwrec"), O.copy_slots("mwrec")
+        assert np.max(np.abs(wg[mask] - wo[mask])) <= 1e-12
+        for f in ("h", "drainage_area", "erosion_rate", "lake_depth"):
+            a, b = gpu_float(g, f), O.copy_double(f)
+            assert rel_err(a, b) <= 1e-9, (step, f, rel_err(a, b))
+        # the GPU multiple-flow stack is a topological order of mrec
+        ms = g.copy_int("mstack")
+        pos = np.empty(g.nn, np.int64)
+        pos[ms] = np.arange(g.nn)
+        rows, cols = np.nonzero(mask)
+        assert np.all(pos[mg[rows, cols]] > pos[rows])
+
+
+def test_reference_api_drop_in():
+    """The module-level fastscape_* functions behave like the reference's."""
+    import fastscapelib_fortran as fs
+    wl = W.plain_d8(51, 45, seed=3)
+    wl.apply(fs)
+    wl.apply(O)
+    for _ in range(3):
+        fs.fastscape_execute_step()
+        O.fastscape_execute_step()
+    hg = np.empty(wl.nn)
+    fs.fastscape_copy_h(hg)
+    ag = np.zeros((wl.ny, wl.nx))
+    fs.fastscape_copy_drainage_area(ag)
+    assert np.array_equal(hg, O.copy_double("h"))
+    assert np.array_equal(ag.ravel(), O.copy_double("drainage_area"))
+    assert fs.fastscape_get_step() == 3
+    with pytest.raises(ValueError):
+        fs.fastscape_copy_h(np.empty(wl.nn, np.float32))
+    import torch
+    ht = torch.empty(wl.nn, dtype=torch.float64, device="cuda")
+    fs.fastscape_copy_h(ht)
+    assert np.array_equal(ht.cpu().numpy(), hg)
+    fs.fastscape_destroy()
