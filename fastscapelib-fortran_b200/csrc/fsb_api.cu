@@ -120,6 +120,19 @@ size_t layout(fsb::Ctx& c, char* base) {
   c.arc_adj = L.take<int>(2 * N);
   c.o_keys = L.take<unsigned long long>(N); c.o_keys2 = L.take<unsigned long long>(N);
   c.o_vals = L.take<int>(N); c.o_vals2 = L.take<int>(N); c.o_pos = L.take<int>(N);
+  c.ch_heavy = L.take<int>(N); c.ch_tmp = L.take<int>(N + 1); c.ch_tmp2 = L.take<int>(N + 1);
+  c.ch_nxt = L.take<int>(N); c.ch_nxt2 = L.take<int>(N);
+  c.ch_val = L.take<unsigned long long>(N); c.ch_val2 = L.take<unsigned long long>(N);
+  c.ch_ord = L.take<int>(N); c.ch_pos = L.take<int>(N); c.ch_ldep = L.take<int>(N); c.ch_start = L.take<int>(N);
+  c.ch_cid = L.take<int>(N); c.ch_sid = L.take<int>(N); c.ch_hist = L.take<int>(128); c.ch_goff = L.take<int>(128);
+  c.ch_tk_td = L.take<int>(N + 2048); c.ch_tk_bu = L.take<int>(N + 2048);
+  c.ch_key = L.take<unsigned>(2 * N); c.ch_skey = L.take<unsigned>(N);
+  c.la_queue = L.take<int>(N); c.la_cnt = L.take<int>(N); c.cnt_acc = L.take<int>(N); c.cnt_spl = L.take<int>(N);
+  c.la_ctl = L.take<unsigned>(128);
+  c.r_rn = L.take<int>(N); c.r_rcv = L.take<int>(8 * N); c.r_an = L.take<int>(N); c.r_ad = L.take<int>(8 * N);
+  c.r_qn = L.take<int>(N); c.r_q = L.take<int>(8 * N); c.r_dn = L.take<int>(N); c.r_dep = L.take<int>(8 * N);
+  c.r_aw = L.take<double>(8 * N); c.r_qf = L.take<double>(8 * N);
+  c.s_scan2 = L.take<int>(N + 1);
   c.done = L.take<unsigned>(N); c.ticket = L.take<unsigned>(4);
   c.water = L.take<double>(N); c.hnew = L.take<double>(N);
   c.dK = L.take<double>(N); c.dA = L.take<double>(N); c.dB = L.take<double>(N); c.dC = L.take<double>(N);
@@ -245,6 +258,7 @@ int step_once(fsb::Ctx& c) {
     stage_end(c, ST_LOCMIN);
     if (!ok) { g_err = c.err; return 1; }
     stage_begin(c, ST_FILL);
+    fsb::build_chains(c);
     fsb::fill_sweep(c);
     stage_end(c, ST_FILL);
     if (!c.sfd) {

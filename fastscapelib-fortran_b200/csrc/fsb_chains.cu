@@ -1,0 +1,518 @@
+// Heavy-path chain schedule of the receiver forest and the single-flow tree
+// sweeps that run on it (lake fill, drainage area, stream power law).
+//
+// The tree recurrences of the reference are sequential loops over the stack:
+//   hwater fill           src/FlowRouting.f90:73-89  (root -> leaves)
+//   drainage area         src/FlowRouting.f90:123-143 (leaves -> root)
+//   implicit SPL, g == 0  src/StreamPowerLaw.f90:291-373 (root -> leaves)
+// Each node only needs its receiver (top-down) or its donors (bottom-up), so
+// any schedule that respects the tree gives the same per-node arithmetic.
+//
+// Schedule.  Every node's heavy child is its donor with the largest subtree
+// (first in ascending node order on ties).  A heavy-first preorder lays every
+// heavy path out contiguously; a "chain" is one heavy path, from its head (a
+// root or a light child) to a leaf.  One thread walks a whole chain, carrying
+// the running value in registers, so a long river costs one dependent
+// arithmetic step per node instead of one inter-thread hand-off.  A chain
+// depends only on its head's parent (top-down) or on the chains hanging off
+// it (bottom-up); its "light depth" -- the number of light edges above it,
+// at most log2(nn) -- therefore orders the chains: tickets are handed out by
+// light depth (increasing for top-down sweeps, decreasing for bottom-up), and
+// within a light depth longer chains first.  Every wait then targets a chain
+// with an earlier ticket, so the sweeps cannot deadlock; warps never mix light
+// depths (groups are padded to multiples of 32).
+//
+// Heavy-first positions come from path sums over the receiver pointers
+// (pointer jumping): pos(k) = sum over the root->k path of each node's offset
+// within its parent's subtree (1 + sizes of the siblings laid out before it).
+#include <cuda/atomic>
+#include <climits>
+
+#include "fsb_kernels.cuh"
+
+namespace fsb {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// bounded wait for done[k] == epoch (relaxed polling, then an acquire
+// fence); gives up once any wait has failed
+__device__ inline void wait_flag(unsigned* done, int k, unsigned epoch, int* err) {
+  int spins = 0, back = 32;
+  while (*(volatile unsigned*)&done[k] != epoch) {
+    if (++spins > kSpinLimit) { atomicExch(err, DEV_SPIN_LIMIT); return; }
+    if ((spins & 63) == 0 && *(volatile int*)err != 0) return;
+    __nanosleep(back);
+    if (back < 512) back <<= 1;
+  }
+  __threadfence();
+}
+
+// heavy child: donor with the largest subtree, first in ascending order on ties
+__global__ void k_heavy(int nn, const int* __restrict__ ndon, const int* __restrict__ don,
+                        const int* __restrict__ size, int* __restrict__ heavy) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const int nd = ndon[k];
+    int best = -1, bs = -1;
+    for (int i = 0; i < nd; ++i) {
+      const int d = don[(size_t)k * 8 + i];
+      const int s = size[d];
+      if (s > bs) { bs = s; best = d; }
+    }
+    heavy[k] = best;
+  }
+}
+
+// sizes of the roots in ascending root order (for the root offsets)
+__global__ void k_root_sizes(int nroots, const int* __restrict__ roots, const int* __restrict__ size,
+                             int* __restrict__ out) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r <= nroots; r += gridDim.x * blockDim.x)
+    out[r] = r < nroots ? size[roots[r]] : 0;
+}
+
+// offset of each node inside its parent's heavy-first layout, light flag in
+// the high word; pointer = receiver (or -1 at roots)
+__global__ void k_hf_offsets(int nn, const int* __restrict__ rec, const int* __restrict__ ndon,
+                             const int* __restrict__ don, const int* __restrict__ size,
+                             const int* __restrict__ heavy, const int* __restrict__ root_rank,
+                             const int* __restrict__ root_off, unsigned long long* __restrict__ val,
+                             int* __restrict__ nxt) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const int r = rec[k];
+    unsigned long long v;
+    if (r == k) {
+      v = (unsigned long long)(unsigned)root_off[root_rank[k]];
+      nxt[k] = -1;
+    } else {
+      const int hv = heavy[r];
+      if (k == hv) {
+        v = 1ull;
+      } else {
+        unsigned off = 1u + (unsigned)size[hv];
+        const int nd = ndon[r];
+        for (int i = 0; i < nd; ++i) {
+          const int d = don[(size_t)r * 8 + i];
+          if (d >= k) break;
+          if (d != hv) off += (unsigned)size[d];
+        }
+        v = (unsigned long long)off | (1ull << 32);
+      }
+      nxt[k] = r;
+    }
+    val[k] = v;
+  }
+}
+
+// one synchronous pointer-jumping round of the path sums
+__global__ void k_path_jump(int nn, const unsigned long long* __restrict__ vin, const int* __restrict__ nin,
+                            unsigned long long* __restrict__ vout, int* __restrict__ nout, int* __restrict__ flag) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const int p = nin[k];
+    if (p < 0) {
+      vout[k] = vin[k];
+      nout[k] = -1;
+    } else {
+      vout[k] = vin[k] + vin[p];
+      const int pp = nin[p];
+      nout[k] = pp;
+      if (pp >= 0) *flag = 1;
+    }
+  }
+}
+
+__global__ void k_hf_order(int nn, const unsigned long long* __restrict__ val, const int* __restrict__ rec,
+                           const int* __restrict__ heavy, int* __restrict__ ord, int* __restrict__ hpos,
+                           int* __restrict__ ldep, int* __restrict__ err) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const unsigned p = (unsigned)val[k];
+    if (p >= (unsigned)nn) { atomicExch(err, DEV_STACK_ERROR); continue; }
+    ord[p] = k;
+    hpos[k] = (int)p;
+    ldep[k] = (int)(val[k] >> 32);
+  }
+}
+
+// chain starts: positions whose node is a root or a light child
+__global__ void k_chain_flags(int nn, const int* __restrict__ ord, const int* __restrict__ rec,
+                              const int* __restrict__ heavy, int* __restrict__ flag) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= nn; p += gridDim.x * blockDim.x) {
+    if (p == nn) { flag[p] = 0; continue; }
+    const int k = ord[p];
+    const int r = rec[k];
+    flag[p] = (r == k || heavy[r] != k) ? 1 : 0;
+  }
+}
+
+// chain list (start positions ascending) with sort keys
+//   top-down key:  light depth (6 bits) | ~length (26 bits)
+//   bottom-up key: (63 - light depth)   | ~length
+__global__ void k_chain_list(int nn, const int* __restrict__ flag, const int* __restrict__ scan,
+                             int* __restrict__ cstart, int* __restrict__ cid) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nn; p += gridDim.x * blockDim.x) {
+    if (!flag[p]) continue;
+    const int c = scan[p];
+    cstart[c] = p;
+    cid[c] = c;
+  }
+}
+
+__global__ void k_chain_keys(int nn, int nchains, const int* __restrict__ cstart, const int* __restrict__ ord,
+                             const int* __restrict__ ldep, unsigned* __restrict__ key_td,
+                             unsigned* __restrict__ key_bu, int* __restrict__ hist_td, int* __restrict__ hist_bu) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nchains; c += gridDim.x * blockDim.x) {
+    const int s = cstart[c];
+    const int e = (c + 1 < nchains) ? cstart[c + 1] : nn;
+    const unsigned len = (unsigned)(e - s);
+    int ld = ldep[ord[s]];
+    if (ld > 63) ld = 63;
+    const unsigned inv = 0x3ffffffu - (len > 0x3ffffffu ? 0x3ffffffu : len);
+    key_td[c] = ((unsigned)ld << 26) | inv;
+    key_bu[c] = ((unsigned)(63 - ld) << 26) | inv;
+    atomicAdd(&hist_td[ld], 1);
+    atomicAdd(&hist_bu[63 - ld], 1);
+  }
+}
+
+// per-group offsets, padded to multiples of 32 (one thread)
+__global__ void k_group_offsets(const int* __restrict__ hist, int* __restrict__ ustart, int* __restrict__ pstart,
+                                int* __restrict__ total) {
+  int u = 0, pz = 0;
+  for (int g = 0; g < 64; ++g) {
+    ustart[g] = u;
+    pstart[g] = pz;
+    u += hist[g];
+    pz += (hist[g] + 31) & ~31;
+  }
+  *total = pz;
+}
+
+__global__ void k_ticket_scatter(int nchains, const unsigned* __restrict__ skey, const int* __restrict__ sid,
+                                 const int* __restrict__ ustart, const int* __restrict__ pstart,
+                                 int* __restrict__ tickets) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nchains; t += gridDim.x * blockDim.x) {
+    const int g = (int)(skey[t] >> 26);
+    tickets[pstart[g] + (t - ustart[g])] = sid[t];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// chain sweeps
+
+struct ChainView {
+  const int* ord;      // heavy-first order
+  const int* cstart;   // chain start positions (ascending), nchains entries
+  const int* tickets;  // padded ticket list (chain ids or -1)
+  int nchains, ntickets, nn;
+  __device__ void range(int c, int& s, int& e) const {
+    s = cstart[c];
+    e = (c + 1 < nchains) ? cstart[c + 1] : nn;  // exclusive
+  }
+};
+
+constexpr int kCF = 16;  // nodes per software-pipelined chunk (fill, area)
+constexpr int kCS = 8;   // nodes per chunk (stream power)
+
+// Top-down: hwater(k) = hwater(rec) > h(k) ? hwater(rec) + 1e-8 : h(k)
+// (FlowRouting.f90:77-86); lake_depth = hwater - h.
+__global__ void __launch_bounds__(128) k_fill_chains(ChainView cv, const int* __restrict__ rec,
+                                                     const int* __restrict__ ndon, const double* __restrict__ h,
+                                                     double* __restrict__ hwater, double* __restrict__ lake_depth,
+                                                     unsigned* ticket, unsigned* done, unsigned epoch, int* err) {
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned w = 0;
+    if (lane == 0) w = atomicAdd(ticket, 32u);
+    w = __shfl_sync(FULL, w, 0);
+    if ((int)w >= cv.ntickets) break;
+    const int t = (int)w + lane;
+    const int c = t < cv.ntickets ? cv.tickets[t] : -1;
+    if (c < 0) continue;
+    int s, e;
+    cv.range(c, s, e);
+    const int k0 = cv.ord[s];
+    const int r0 = rec[k0];
+    bool root = r0 == k0;
+    double prev = 0.0;
+    if (!root) {
+      wait_flag(done, r0, epoch, err);
+      prev = __ldcg(&hwater[r0]);
+    }
+    for (int p = s; p < e; p += kCF) {
+      const int n = min(kCF, e - p);
+      int kk[kCF], nd[kCF];
+      double hh[kCF], out[kCF];
+#pragma unroll
+      for (int i = 0; i < kCF; ++i) if (i < n) kk[i] = cv.ord[p + i];
+#pragma unroll
+      for (int i = 0; i < kCF; ++i) if (i < n) { hh[i] = h[kk[i]]; nd[i] = ndon[kk[i]]; }
+#pragma unroll
+      for (int i = 0; i < kCF; ++i) if (i < n) {
+        const double v = root ? hh[i] : (prev > hh[i] ? prev + 1.0e-8 : hh[i]);
+        root = false;
+        out[i] = v;
+        prev = v;
+      }
+#pragma unroll
+      for (int i = 0; i < kCF; ++i) if (i < n) { hwater[kk[i]] = out[i]; lake_depth[kk[i]] = out[i] - hh[i]; }
+      __threadfence();
+#pragma unroll
+      for (int i = 0; i < kCF; ++i) if (i < n && nd[i] > 1) *(volatile unsigned*)&done[kk[i]] = epoch;
+    }
+  }
+}
+
+// Bottom-up single-flow area: a(k) = dx*dy*precip(k) + a(d_m) + ... + a(d_1)
+// (donors descending, the reverse-stack order of FlowRouting.f90:136-139);
+// roots add themselves.  Only the chain head is read by another chain.
+__global__ void __launch_bounds__(128) k_area_chains(ChainView cv, const int* __restrict__ rec,
+                                                     const int* __restrict__ ndon, const int* __restrict__ don,
+                                                     const double* __restrict__ precip, double dxdy,
+                                                     double* __restrict__ a, unsigned* ticket, unsigned* done,
+                                                     unsigned epoch, int* err) {
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned w = 0;
+    if (lane == 0) w = atomicAdd(ticket, 32u);
+    w = __shfl_sync(FULL, w, 0);
+    if ((int)w >= cv.ntickets) break;
+    const int t = (int)w + lane;
+    const int c = t < cv.ntickets ? cv.tickets[t] : -1;
+    if (c < 0) continue;
+    int s, e;
+    cv.range(c, s, e);
+    int child = -1;
+    double ac = 0.0;
+    for (int hi = e; hi > s; hi -= kCF) {
+      const int n = min(kCF, hi - s);
+      const int lo = hi - n;
+      int kk[kCF], nd[kCF];
+      double base[kCF];
+#pragma unroll
+      for (int i = 0; i < kCF; ++i) if (i < n) kk[i] = cv.ord[lo + i];
+#pragma unroll
+      for (int i = 0; i < kCF; ++i) if (i < n) {
+        nd[i] = ndon[kk[i]];
+        base[i] = dxdy * precip[kk[i]];
+        if (rec[kk[i]] == kk[i]) nd[i] |= 1 << 8;
+      }
+#pragma unroll
+      for (int i = kCF - 1; i >= 0; --i) if (i < n) {
+        const int k = kk[i];
+        const int ndk = nd[i] & 255;
+        double acc = base[i];
+        for (int q = ndk - 1; q >= 0; --q) {
+          const int d = don[(size_t)k * 8 + q];
+          double v;
+          if (d == child) v = ac;
+          else {
+            wait_flag(done, d, epoch, err);
+            v = __ldcg(&a[d]);
+          }
+          acc = acc + v;
+        }
+        if (nd[i] >> 8) acc = acc + acc;
+        a[k] = acc;
+        ac = acc;
+        child = k;
+      }
+    }
+    __threadfence();
+    *(volatile unsigned*)&done[cv.ord[s]] = epoch;
+  }
+}
+
+// Top-down single-flow stream power law with g == 0 (StreamPowerLaw.f90:291-373):
+// writes hnew and water; h keeps ht.  The per-node factor kf*dt*a^m/l(^n)
+// does not depend on the recurrence and is computed for a whole chunk first.
+__global__ void __launch_bounds__(128) k_spl_chains(ChainView cv, const int* __restrict__ rec,
+                                                    const int* __restrict__ ndon, const double* __restrict__ h,
+                                                    const double* __restrict__ b, const double* __restrict__ kf,
+                                                    const double* __restrict__ a, const double* __restrict__ length,
+                                                    double kfsed, double dt, double m, double n, double omega,
+                                                    int n_is_one, double* __restrict__ hnew,
+                                                    double* __restrict__ water, unsigned* ticket, unsigned* done,
+                                                    unsigned epoch, int* err) {
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned w = 0;
+    if (lane == 0) w = atomicAdd(ticket, 32u);
+    w = __shfl_sync(FULL, w, 0);
+    if ((int)w >= cv.ntickets) break;
+    const int t = (int)w + lane;
+    const int c = t < cv.ntickets ? cv.tickets[t] : -1;
+    if (c < 0) continue;
+    int s, e;
+    cv.range(c, s, e);
+    const int k0 = cv.ord[s];
+    const int r0 = rec[k0];
+    bool root = r0 == k0;
+    double hr = 0.0, wr = 0.0, htr = 0.0;
+    if (!root) {
+      wait_flag(done, r0, epoch, err);
+      hr = __ldcg(&hnew[r0]);
+      wr = __ldcg(&water[r0]);
+      htr = h[r0];
+    }
+    for (int p = s; p < e; p += kCS) {
+      const int cn = min(kCS, e - p);
+      int kk[kCS], nd[kCS];
+      double ht[kCS], fact[kCS], ho[kCS], wo[kCS];
+#pragma unroll
+      for (int i = 0; i < kCS; ++i) if (i < cn) kk[i] = cv.ord[p + i];
+#pragma unroll
+      for (int i = 0; i < kCS; ++i) if (i < cn) {
+        const int k = kk[i];
+        ht[i] = h[k];
+        nd[i] = ndon[k];
+        const double kfint = (kfsed > 0.0 && (ht[i] - b[k]) > 1.0) ? kfsed : kf[k];
+        const double l = length[k];
+        fact[i] = n_is_one ? kfint * dt * pow(a[k], m) / l : kfint * dt * pow(a[k], m) / pow(l, n);
+      }
+#pragma unroll
+      for (int i = 0; i < kCS; ++i) if (i < cn) {
+        double hk = ht[i], wk;
+        if (root) {
+          wk = ht[i];
+          root = false;
+        } else {
+          const double elev = ht[i];
+          if (elev > wr) {
+            if (n_is_one) {
+              double f = elev, df = 1.0;
+              f = f + fact[i] * hr;
+              df = df + fact[i];
+              hk = f / df;
+            } else {
+              const double tolp = 1.0e-3;
+              double errp = 2.0 * tolp;
+              int guard = 0;
+              while (errp > tolp && guard++ < 10000) {
+                double f = hk - elev, df = 1.0;
+                if (ht[i] > htr) {
+                  const double x = fmax(0.0, hk - hr);
+                  f = f + fact[i] * pow(x, n);
+                  df = df + fact[i] * n * pow(x, n - 1.0);
+                }
+                const double hn = hk - f / df;
+                errp = fabs(hn - hk);
+                hk = hk * (1.0 - omega) + hn * omega;
+              }
+            }
+            if (hk < wr) hk = wr;
+          } else {
+            hk = elev;
+          }
+          wk = fmax(wr, hk);
+        }
+        ho[i] = hk;
+        wo[i] = wk;
+        hr = hk;
+        wr = wk;
+        htr = ht[i];
+      }
+#pragma unroll
+      for (int i = 0; i < kCS; ++i) if (i < cn) { hnew[kk[i]] = ho[i]; water[kk[i]] = wo[i]; }
+      __threadfence();
+#pragma unroll
+      for (int i = 0; i < kCS; ++i) if (i < cn && nd[i] > 1) *(volatile unsigned*)&done[kk[i]] = epoch;
+    }
+  }
+}
+
+}  // namespace
+
+// Builds the heavy-first order and both ticket lists for the current
+// receiver forest (rec, ndon, don, size, roots must be current).
+void build_chains(Ctx& c) {
+  const int nn = c.nn;
+  cudaStream_t st = c.stream;
+  k_heavy<<<grid1d(nn), kBlock, 0, st>>>(nn, c.ndon, c.don, c.size, c.ch_heavy);
+  cudaMemcpyAsync(c.d_cnt + 15, c.s_scan + nn, sizeof(int), cudaMemcpyDeviceToDevice, st);
+  fetch_counters(c, 20);
+  c.nroots = c.h_cnt[15];
+  const int nroots_h = c.nroots;
+  k_root_sizes<<<grid1d(nroots_h + 1), kBlock, 0, st>>>(nroots_h, c.s_roots, c.size, c.ch_tmp);
+  c.count_launch(2);
+  exclusive_scan_int(c, c.ch_tmp, c.ch_tmp2, nroots_h + 1);
+  k_hf_offsets<<<grid1d(nn), kBlock, 0, st>>>(nn, c.rec, c.ndon, c.don, c.size, c.ch_heavy, c.s_root_rank,
+                                              c.ch_tmp2, c.ch_val, c.ch_nxt);
+  c.count_launch();
+  unsigned long long *va = c.ch_val, *vb = c.ch_val2;
+  int *na = c.ch_nxt, *nb = c.ch_nxt2;
+  for (int round = 0; round < 40; ++round) {
+    cudaMemsetAsync(c.d_cnt + 16, 0, sizeof(int), st);
+    k_path_jump<<<grid1d(nn), kBlock, 0, st>>>(nn, va, na, vb, nb, c.d_cnt + 16);
+    std::swap(va, vb);
+    std::swap(na, nb);
+    k_path_jump<<<grid1d(nn), kBlock, 0, st>>>(nn, va, na, vb, nb, c.d_cnt + 16);
+    std::swap(va, vb);
+    std::swap(na, nb);
+    c.count_launch(2);
+    fetch_counters(c, 20);
+    if (!c.h_cnt[16]) break;
+  }
+  k_hf_order<<<grid1d(nn), kBlock, 0, st>>>(nn, va, c.rec, c.ch_heavy, c.ch_ord, c.ch_pos, c.ch_ldep, c.d_err);
+  k_chain_flags<<<grid1d(nn + 1), kBlock, 0, st>>>(nn, c.ch_ord, c.rec, c.ch_heavy, c.ch_tmp);
+  c.count_launch(2);
+  exclusive_scan_int(c, c.ch_tmp, c.ch_tmp2, nn + 1);
+  cudaMemcpyAsync(c.d_cnt + 17, c.ch_tmp2 + nn, sizeof(int), cudaMemcpyDeviceToDevice, st);
+  fetch_counters(c, 20);
+  const int nchains = c.h_cnt[17];
+  c.nchains = nchains;
+  k_chain_list<<<grid1d(nn), kBlock, 0, st>>>(nn, c.ch_tmp, c.ch_tmp2, c.ch_start, c.ch_cid);
+  cudaMemsetAsync(c.ch_hist, 0, sizeof(int) * 128, st);
+  k_chain_keys<<<grid1d(nchains), kBlock, 0, st>>>(nn, nchains, c.ch_start, c.ch_ord, c.ch_ldep, c.ch_key,
+                                                   c.ch_key + nchains, c.ch_hist, c.ch_hist + 64);
+  c.count_launch(2);
+  for (int dir = 0; dir < 2; ++dir) {
+    sort_pairs_u32(c, c.ch_key + (size_t)dir * nchains, c.ch_skey, c.ch_cid, c.ch_sid, nchains, 32);
+    k_group_offsets<<<1, 1, 0, st>>>(c.ch_hist + 64 * dir, c.ch_goff, c.ch_goff + 64, c.d_cnt + 18 + dir);
+    int* tk = dir == 0 ? c.ch_tk_td : c.ch_tk_bu;
+    cudaMemsetAsync(tk, 0xff, sizeof(int) * ((size_t)nchains + 64 * 32), st);
+    k_ticket_scatter<<<grid1d(nchains), kBlock, 0, st>>>(nchains, c.ch_skey, c.ch_sid, c.ch_goff, c.ch_goff + 64, tk);
+    c.count_launch(2);
+  }
+  fetch_counters(c, 20);
+  c.ntickets_td = c.h_cnt[18];
+  c.ntickets_bu = c.h_cnt[19];
+}
+
+static void next_epoch(Ctx& c) {
+  c.epoch += 1;
+  if (c.epoch == 0) {
+    cudaMemsetAsync(c.done, 0, sizeof(unsigned) * c.nn, c.stream);
+    c.epoch = 1;
+  }
+  cudaMemsetAsync(c.ticket, 0, sizeof(unsigned), c.stream);
+}
+
+static const int kChainBlocks = 148 * 8;
+
+void fill_chains(Ctx& c) {
+  next_epoch(c);
+  ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_td, c.nchains, c.ntickets_td, c.nn};
+  k_fill_chains<<<kChainBlocks, 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.h, c.hwater, c.lake_depth, c.ticket,
+                                                    c.done, c.epoch, c.d_err);
+  c.count_launch();
+}
+
+void area_chains(Ctx& c) {
+  next_epoch(c);
+  ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_bu, c.nchains, c.ntickets_bu, c.nn};
+  k_area_chains<<<kChainBlocks, 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, c.precip, c.dx * c.dy, c.a, c.ticket,
+                                                    c.done, c.epoch, c.d_err);
+  c.count_launch();
+}
+
+void spl_chains(Ctx& c, double* hnew) {
+  next_epoch(c);
+  ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_td, c.nchains, c.ntickets_td, c.nn};
+  const int n1 = fabs(c.n - 1.0) < 2.2250738585072014e-308;
+  k_spl_chains<<<kChainBlocks, 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.h, c.b, c.kf, c.a, c.length, c.kfsed, c.dt,
+                                                   c.m, c.n, 0.875 / c.n, n1, hnew, c.water, c.ticket, c.done,
+                                                   c.epoch, c.d_err);
+  c.count_launch();
+}
+
+}  // namespace fsb

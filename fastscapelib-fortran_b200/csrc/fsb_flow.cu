@@ -1,22 +1,20 @@
-// Lake filling, multiple-flow receivers, drainage area, implicit stream power
-// law and ADI hillslope diffusion.
+// Multiple-flow receivers, multiple-flow sweeps (drainage area and implicit
+// stream power law), the stream-power epilogue and ADI hillslope diffusion.
 //
 // Reference routines restated here (fastscapelib-fortran file:line):
-//   hwater fill + lake_depth              src/FlowRouting.f90:73-89 (SFD), :183-198 (MFD h0)
-//   find_mult_rec                         src/FlowRouting.f90:147-298
-//   FlowAccumulation(SingleFlowDirection) src/FlowRouting.f90:97-143
-//   StreamPowerLaw(SingleFlowDirection)   src/StreamPowerLaw.f90:3-206, 210-400 (g == 0)
-//   Diffusion + tridag                    src/Diffusion.f90:1-202
+//   find_mult_rec                 src/FlowRouting.f90:147-298
+//   FlowAccumulation (MFD)        src/FlowRouting.f90:97-119
+//   StreamPowerLaw (MFD, g == 0)  src/StreamPowerLaw.f90:3-206
+//   Diffusion + tridag            src/Diffusion.f90:1-202
+// The single-flow tree sweeps live in fsb_chains.cu.
 //
-// Tree and DAG recurrences (fill, area, implicit erosion) run as wavefront
-// sweeps over a topological order: warps claim windows of 32 consecutive
-// positions through an atomic ticket, wait (bounded) for dependencies in
-// earlier windows through per-node epoch flags, and resolve dependencies
-// inside the window through a warp ballot and shared memory.  Every
-// dependency sits at an earlier position, so a window only waits on windows
-// claimed before it and the sweep cannot deadlock; each per-node formula
-// keeps the reference's operation order, so single-flow results are
-// bit-identical to the sequential loops.
+// Multiple-flow sweeps run over the receiver DAG with dependency counters:
+// every node starts with the number of nodes it waits for; the thread that
+// brings a counter to zero ("last arriver") continues with that node, and
+// further nodes it makes ready go to a work queue.  Nothing waits on work that
+// has not been scheduled, so the sweep needs no global order and cannot
+// deadlock; the counters' acquire/release ordering makes every dependency's
+// value visible before it is read.
 #include <cuda/atomic>
 #include <cfloat>
 
@@ -27,387 +25,226 @@ namespace fsb {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int kWarps = 4;  // warps per block in the sweep kernels
 
 __device__ inline unsigned long long ordered_key(double x) {
   unsigned long long u = (unsigned long long)__double_as_longlong(x);
   return (u & 0x8000000000000000ull) ? ~u : (u | 0x8000000000000000ull);
 }
 
-__device__ inline bool flag_ready(const unsigned* done, int k, unsigned epoch) {
-  cuda::atomic_ref<unsigned, cuda::thread_scope_device> f(*const_cast<unsigned*>(&done[k]));
-  return f.load(cuda::memory_order_acquire) == epoch;
-}
+// relaxed decrement; the caller issued a release fence before it and the
+// thread that sees the count reach zero fences again before using the node
+__device__ inline bool dec_ready(int* cnt, int r) { return atomicSub(&cnt[r], 1) == 1; }
 
-__device__ inline void flag_publish(unsigned* done, int k, unsigned epoch) {
-  cuda::atomic_ref<unsigned, cuda::thread_scope_device> f(done[k]);
-  f.store(epoch, cuda::memory_order_release);
-}
-
-// Order views: position -> node and node -> position.
-struct Fwd {
-  const int* ord;
-  const int* pos;
-  int n;
-  __device__ int at(int p) const { return ord[p]; }
-  __device__ int posof(int k) const { return pos[k]; }
-};
-struct Rev {
-  const int* ord;
-  const int* pos;
-  int n;
-  __device__ int at(int p) const { return ord[n - 1 - p]; }
-  __device__ int posof(int k) const { return n - 1 - pos[k]; }
-};
-
-// Generic wavefront over an order.  Op provides
-//   MAXDEP, Val, St,
-//   int  init(k, St&, int* deps)                  node-local work, list of dependencies
-//   Val  load(d)                                  dependency value from global memory
-//   Val  compute(k, St&, nd, const int*, const Val*)
-//   void store(k, const Val&)                     publish to global memory
-template <class Op, class Order>
-__global__ void __launch_bounds__(kWarps * 32) k_wavefront(Op op, Order od, unsigned* ticket, unsigned* done,
-                                                           unsigned epoch, int* err) {
-  using Val = typename Op::Val;
-  __shared__ Val sval[kWarps][32];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (;;) {
-    unsigned w = 0;
-    if (lane == 0) w = atomicAdd(ticket, 1u);
-    w = __shfl_sync(FULL, w, 0);
-    const long long base = (long long)w * 32;
-    if (base >= od.n) break;
-    const int p = (int)base + lane;
-    const int k = p < od.n ? od.at(p) : -1;
-    typename Op::St st;
-    int deps[Op::MAXDEP];
-    Val dv[Op::MAXDEP];
-    int dl[Op::MAXDEP];
-    int nd = 0;
-    unsigned intra = 0;  // bit s set: deps[s] sits in this window, at lane dl[s]
-    if (k >= 0) {
-      nd = op.init(k, st, deps);
-      for (int s = 0; s < nd; ++s) {
-        const int q = od.posof(deps[s]);
-        if (q >= base + 32) {  // not a topological order: report, never wait
-          atomicExch(err, DEV_STACK_ERROR);
-        } else if (q >= base) {
-          intra |= 1u << s;
-          dl[s] = q - (int)base;
-        } else {
-          int spins = 0;
-          while (!flag_ready(done, deps[s], epoch)) {
-            if (++spins > kSpinLimit) { atomicExch(err, DEV_SPIN_LIMIT); break; }
-            // once any wait has failed, stop waiting everywhere (results are void)
-            if ((spins & 255) == 0 && *(volatile int*)err != 0) break;
-            __nanosleep(20);
-          }
-          dv[s] = op.load(deps[s]);
+// ---- last-arriver sweep engine ----------------------------------------------
+// Op::process(k, ready[], nready) computes node k, then decrements the
+// counters of k's dependents and lists those that became ready.  Idle lanes
+// claim queue slots in order (one atomic per warp); a lane keeps its claim
+// until a producer fills it.  The kernel ends when every node is done.
+// Control words: ctl[0] queue head, ctl[32] queue tail, ctl[64] nodes done
+// (separate 128-byte lines).
+template <class Op>
+__global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, const int* __restrict__ prio, int* queue,
+                                                      unsigned* ctl, int* err) {
+  unsigned* qhead = ctl;
+  unsigned* qtail = ctl + 32;
+  unsigned* ndone = ctl + 64;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  int cur = -1;
+  long long slot = -1;
+  unsigned local_done = 0;
+  int back = 32;
+  for (int it = 0; it < (1 << 24); ++it) {
+    const bool want = cur < 0 && slot < 0;
+    const unsigned m = __ballot_sync(FULL, want);
+    if (m) {
+      const int leader = __ffs(m) - 1;
+      unsigned base = 0;
+      if (lane == leader) base = atomicAdd(qhead, (unsigned)__popc(m));
+      base = __shfl_sync(FULL, base, leader);
+      if (want) slot = (long long)base + __popc(m & lt);
+    }
+    if (cur < 0 && slot >= 0 && slot < nn) {
+      const int v = *(volatile int*)&queue[slot];
+      if (v >= 0) { cur = v; slot = -1; }
+    }
+    int ready[9];
+    int nr = 0;
+    if (cur >= 0) {
+      __threadfence();  // acquire: the node's inputs were published before it became ready
+      op.process(cur, ready, nr);
+      ++local_done;
+      // continue with the ready dependent that has the largest subtree of the
+      // single-flow tree: that keeps the long paths inside one thread
+      if (nr > 1) {
+        int best = 0, bs = prio[ready[0]];
+        for (int q = 1; q < nr; ++q) {
+          const int v = prio[ready[q]];
+          if (v > bs) { bs = v; best = q; }
         }
+        const int tmp = ready[0]; ready[0] = ready[best]; ready[best] = tmp;
+      }
+      cur = nr > 0 ? ready[0] : -1;
+    }
+    bool fenced = false;
+    for (int e = 1; e < 9; ++e) {  // push the other ready nodes, one atomic per warp
+      const bool has = e < nr;
+      const unsigned mm = __ballot_sync(FULL, has);
+      if (!mm) break;
+      const int leader = __ffs(mm) - 1;
+      unsigned base = 0;
+      if (lane == leader) base = atomicAdd(qtail, (unsigned)__popc(mm));
+      base = __shfl_sync(FULL, base, leader);
+      if (has) {
+        const unsigned idx = base + __popc(mm & lt);
+        if (!fenced) { __threadfence(); fenced = true; }
+        if (idx < (unsigned)nn) *(volatile int*)&queue[idx] = ready[e];
+        else atomicExch(err, DEV_OVERFLOW);
       }
     }
-    bool mine = k < 0;
-    // every pass completes at least the lowest unfinished lane: <= 32 passes
-    for (int it = 0; it < 34; ++it) {
-      const unsigned dmask = __ballot_sync(FULL, mine);
-      if (dmask == FULL) break;
-      if (!mine) {
-        bool ready = true;
-        for (int s = 0; s < nd; ++s)
-          if ((intra >> s) & 1u) ready = ready && ((dmask >> dl[s]) & 1u);
-        if (ready) {
-          for (int s = 0; s < nd; ++s)
-            if ((intra >> s) & 1u) dv[s] = sval[warp][dl[s]];
-          const Val v = op.compute(k, st, nd, deps, dv);
-          sval[warp][lane] = v;
-          op.store(k, v);
-          flag_publish(done, k, epoch);
-          mine = true;
-        }
-      }
-      __syncwarp();
+    const unsigned busy = __ballot_sync(FULL, cur >= 0);
+    if (!busy) {
+      const unsigned tot = __reduce_add_sync(FULL, local_done);
+      if (lane == 0 && tot) atomicAdd(ndone, tot);
+      local_done = 0;
+      unsigned d = 0;
+      int e = 0;
+      if (lane == 0) { d = *(volatile unsigned*)ndone; e = *(volatile int*)err; }
+      d = __shfl_sync(FULL, d, 0);
+      e = __shfl_sync(FULL, e, 0);
+      if (d >= (unsigned)nn || e != 0) return;
+      __nanosleep(back);
+      if (back < 256) back <<= 1;
+    } else {
+      back = 32;
     }
-    if (!mine) atomicExch(err, DEV_SPIN_LIMIT);
-    __syncwarp();
+  }
+  if (lane == 0) atomicExch(err, DEV_SPIN_LIMIT);
+}
+
+// initial queue: nodes whose counter is zero
+__global__ void k_seed_queue(int nn, const int* __restrict__ cnt, int* __restrict__ queue, unsigned* qtail) {
+  const int lane = threadIdx.x & 31;
+  for (int base = blockIdx.x * blockDim.x; base < nn; base += gridDim.x * blockDim.x) {
+    const int k = base + threadIdx.x;
+    const bool z = k < nn && cnt[k] == 0;
+    const unsigned m = __ballot_sync(FULL, z);
+    if (!m) continue;
+    unsigned b = 0;
+    const int leader = __ffs(m) - 1;
+    if (lane == leader) b = atomicAdd(qtail, (unsigned)__popc(m));
+    b = __shfl_sync(FULL, b, leader);
+    if (z) queue[b + __popc(m & ((1u << lane) - 1u))] = k;
   }
 }
 
-// ---- hwater fill (FlowRouting.f90:73-89 / 183-198) --------------------------
-struct FillOp {
-  static constexpr int MAXDEP = 1;
-  struct Val { double hw; };
-  struct St { double hk; int r; };
+// Compact per-node records of the multiple-flow sweeps (slot t of node k at
+// [k*8 + t]), built in parallel before the sweeps by k_mfd_records:
+//   r_rn/r_rcv      distinct receivers of k (dependents in the area sweep)
+//   r_an/r_ad/r_aw  distinct donors d of k and the summed weight of d's slots
+//                   targeting k (inputs of the area sweep)
+//   r_qn/r_q/r_qf   receivers whose erosion term is gated on (ht(k) >= ht(q),
+//                   or > for n != 1) and their factor kf*dt*(a*w)^m/l^n; bit 8
+//                   of r_qn marks mnrec(k) > 0
+//   r_dn/r_dep      donors that wait for k in the stream-power sweep
+struct MfdRecords {
+  int *rn, *rcv, *an, *ad, *qn, *q, *dn, *dep;
+  double *aw, *qf;
+};
+
+// a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115)
+struct AccMfdOp {
+  MfdRecords R;
+  const double* precip;
+  double dxdy;
+  double* a;
+  int* cnt;
+  __device__ void process(int k, int* ready, int& nr) const {
+    double acc = dxdy * precip[k];
+    const int na = R.an[k];
+    for (int t = 0; t < na; ++t) acc = acc + __ldcg(&a[R.ad[(size_t)k * 8 + t]]) * R.aw[(size_t)k * 8 + t];
+    a[k] = acc;
+    const int nrc = R.rn[k];
+    if (nrc) {
+      __threadfence();  // release a(k) before the receivers' counters drop
+      for (int t = 0; t < nrc; ++t) {
+        const int r = R.rcv[(size_t)k * 8 + t];
+        if (dec_ready(cnt, r)) ready[nr++] = r;
+      }
+    }
+  }
+};
+
+// implicit stream power law over the multiple receivers with g == 0
+// (StreamPowerLaw.f90:92-177): the new elevation goes to hnew, the water
+// surface to water; h keeps ht.
+struct SplMfdOp {
+  MfdRecords R;
   const int* rec;
   const double* h;
-  double* hwater;
-  double* lake_depth;
-  __device__ int init(int k, St& s, int* deps) const {
-    s.r = rec[k];
-    s.hk = h[k];
-    if (s.r == k) return 0;
-    deps[0] = s.r;
-    return 1;
-  }
-  __device__ Val load(int d) const { return Val{__ldcg(&hwater[d])}; }
-  __device__ Val compute(int k, St& s, int, const int*, const Val* dv) const {
-    if (s.r == k) return Val{s.hk};
-    const double hr = dv[0].hw;
-    return Val{hr > s.hk ? hr + 1.0e-8 : s.hk};
-  }
-  __device__ void store(int k, const Val& v) const {
-    hwater[k] = v.hw;
-    lake_depth[k] = v.hw - h[k];
-  }
-};
-
-// ---- single-flow drainage area (FlowRouting.f90:123-143) --------------------
-// The reverse-stack scatter a(rec)+=a(k) adds the donors of k in descending
-// order: a(k) = dx*dy*precip(k) + a(d_m) + ... + a(d_1); a root also adds
-// itself (a(rec(k)) with rec(k)==k), doubling its area.
-struct AccumSfdOp {
-  static constexpr int MAXDEP = 8;
-  struct Val { double a; };
-  struct St { double base; int root; };
-  const int* rec;
-  const int* ndon;
-  const int* don;
-  const double* precip;
-  double dxdy;
-  double* a;
-  __device__ int init(int k, St& s, int* deps) const {
-    s.base = dxdy * precip[k];
-    s.root = rec[k] == k;
-    const int nd = ndon[k];
-    for (int i = 0; i < nd; ++i) deps[i] = don[(size_t)k * 8 + i];
-    return nd;
-  }
-  __device__ Val load(int d) const { return Val{__ldcg(&a[d])}; }
-  __device__ Val compute(int, St& s, int nd, const int*, const Val* dv) const {
-    double acc = s.base;
-    for (int i = nd - 1; i >= 0; --i) acc = acc + dv[i].a;
-    if (s.root) acc = acc + acc;
-    return Val{acc};
-  }
-  __device__ void store(int k, const Val& v) const { a[k] = v.a; }
-};
-
-// ---- multiple-flow drainage area (FlowRouting.f90:97-119) -------------------
-// a(k) = dx*dy*precip(k) + sum over donors d and their slots s targeting k of
-// a(d)*mwrec(s,d).  Donors come from the precomputed 3x3 donor mask.
-struct AccumMfdOp {
-  static constexpr int MAXDEP = 8;
-  struct Val { double a; };
-  struct St { double base; };
-  Bounds bd;
-  const int* mdmask;
-  const int* mrec;
-  const int* mnrec;
-  const double* mwrec;
-  const double* precip;
-  double dxdy;
-  double* a;
-  __device__ int init(int k, St& s, int* deps) const {
-    s.base = dxdy * precip[k];
-    const int m = mdmask[k];
-    const int i = k % bd.nx, j = k / bd.nx;
-    int nd = 0;
-    for (int t = 0; t < 9; ++t) {
-      if (!((m >> t) & 1)) continue;
-      int ii = i + (t % 3) - 1, jj = j + (t / 3) - 1;
-      if (ii < 0) ii += bd.nx; else if (ii >= bd.nx) ii -= bd.nx;
-      if (jj < 0) jj += bd.ny; else if (jj >= bd.ny) jj -= bd.ny;
-      deps[nd++] = ii + jj * bd.nx;
-    }
-    return nd;
-  }
-  __device__ Val load(int d) const { return Val{__ldcg(&a[d])}; }
-  __device__ Val compute(int k, St& s, int nd, const int* deps, const Val* dv) const {
-    double acc = s.base;
-    for (int q = 0; q < nd; ++q) {
-      const int d = deps[q];
-      const int nr = mnrec[d];
-      for (int t = 0; t < nr; ++t)
-        if (mrec[(size_t)d * 8 + t] == k) acc = acc + dv[q].a * mwrec[(size_t)d * 8 + t];
-    }
-    return Val{acc};
-  }
-  __device__ void store(int k, const Val& v) const { a[k] = v.a; }
-};
-
-// ---- implicit stream power law, g == 0 (StreamPowerLaw.f90) -----------------
-// With g == 0 the Gauss-Seidel loop runs once with elev == ht; the sweep
-// visits receivers before donors and writes the new elevation to hnew while
-// h keeps ht (the elevation at the start of the step).
-struct SplSfdOp {
-  static constexpr int MAXDEP = 1;
-  struct Val { double h, w; };
-  struct St { double ht, fact, htr; int r; };
-  const int* rec;
-  const double* h;       // ht
-  const double* b;
-  const double* kf;
-  const double* a;
-  const double* length;
-  double kfsed, kfdt, m, n, omega;
-  bool n_is_one;
+  double n, omega;
+  int n_is_one;
   double* hnew;
   double* water;
-  __device__ int init(int k, St& s, int* deps) const {
-    s.r = rec[k];
-    s.ht = h[k];
-    if (s.r == k) return 0;
-    s.htr = h[s.r];
-    // kfint = kf, or kfsed where h-b > 1 (StreamPowerLaw.f90:242-243)
-    const double kfint = (kfsed > 0.0 && (s.ht - b[k]) > 1.0) ? kfsed : kf[k];
-    if (n_is_one) s.fact = kfint * kfdt * pow(a[k], m) / length[k];
-    else s.fact = kfint * kfdt * pow(a[k], m) / pow(length[k], n);
-    deps[0] = s.r;
-    return 1;
-  }
-  __device__ Val load(int d) const { return Val{__ldcg(&hnew[d]), __ldcg(&water[d])}; }
-  __device__ Val compute(int k, St& s, int, const int*, const Val* dv) const {
-    if (s.r == k) return Val{s.ht, s.ht};
-    const double hr = dv[0].h, wr = dv[0].w;
-    const double elev = s.ht;
-    double hk = s.ht;
-    if (elev > wr) {
-      if (n_is_one) {
-        double f = elev, df = 1.0;
-        f = f + s.fact * hr;
-        df = df + s.fact;
-        hk = f / df;
-      } else {
-        const double tolp = 1.0e-3;
-        double errp = 2.0 * tolp;
-        const double h0 = elev;
-        int guard = 0;
-        while (errp > tolp && guard++ < 10000) {
-          double f = hk - h0, df = 1.0;
-          if (s.ht > s.htr) {
-            const double x = fmax(0.0, hk - hr);
-            f = f + s.fact * pow(x, n);
-            df = df + s.fact * n * pow(x, n - 1.0);
+  int* cnt;
+  __device__ void process(int k, int* ready, int& nr) const {
+    const int r = rec[k];
+    const double ht = h[k];
+    double hk = ht, wk = ht;
+    if (r != k) {
+      const double wr = __ldcg(&water[r]);
+      const double elev = ht;
+      if (elev > wr) {
+        const int qn = R.qn[k];
+        if (qn & 256) {  // mnrec(k) > 0
+          const int nq = qn & 255;
+          double fact[8], hq[8];
+          for (int t = 0; t < nq; ++t) {
+            fact[t] = R.qf[(size_t)k * 8 + t];
+            hq[t] = __ldcg(&hnew[R.q[(size_t)k * 8 + t]]);
           }
-          const double hn = hk - f / df;
-          errp = fabs(hn - hk);
-          hk = hk * (1.0 - omega) + hn * omega;
-        }
-      }
-      if (hk < wr) hk = wr;
-    } else {
-      hk = elev;
-    }
-    return Val{hk, fmax(wr, hk)};
-  }
-  __device__ void store(int k, const Val& v) const {
-    hnew[k] = v.h;
-    water[k] = v.w;
-  }
-};
-
-struct SplMfdOp {
-  static constexpr int MAXDEP = 9;
-  struct Val { double h, w; };
-  struct St { double ht; double fact[8]; int gate; int nr; int r; int rdep; };
-  const int* rec;
-  const int* mrec;
-  const int* mnrec;
-  const double* mwrec;
-  const double* mlrec;
-  const double* h;  // ht
-  const double* b;
-  const double* kf;
-  const double* a;
-  double kfsed, kfdt, m, n, omega;
-  bool n_is_one;
-  double* hnew;
-  double* water;
-  __device__ int init(int k, St& s, int* deps) const {
-    s.r = rec[k];
-    s.ht = h[k];
-    s.gate = 0;
-    s.rdep = -1;
-    if (s.r == k) { s.nr = 0; return 0; }
-    const int nr = mnrec[k];
-    s.nr = nr;
-    const double ak = a[k];
-    // kfint = kf, or kfsed where h-b > 1 (StreamPowerLaw.f90:35-36)
-    const double kk = ((kfsed > 0.0 && (s.ht - b[k]) > 1.0) ? kfsed : kf[k]) * kfdt;
-    int nd = 0;
-    for (int t = 0; t < nr; ++t) {
-      const int q = mrec[(size_t)k * 8 + t];
-      const double w = mwrec[(size_t)k * 8 + t], l = mlrec[(size_t)k * 8 + t];
-      const double hq = h[q];
-      const bool g = n_is_one ? (s.ht >= hq) : (s.ht > hq);
-      if (g) s.gate |= 1 << t;
-      s.fact[t] = n_is_one ? kk * pow(ak * w, m) / l : kk * pow(ak * w, m) / pow(l, n);
-      deps[nd++] = q;
-    }
-    for (int t = 0; t < nd; ++t)
-      if (deps[t] == s.r) s.rdep = t;
-    if (s.rdep < 0) { s.rdep = nd; deps[nd++] = s.r; }
-    return nd;
-  }
-  __device__ Val load(int d) const { return Val{__ldcg(&hnew[d]), __ldcg(&water[d])}; }
-  __device__ Val compute(int k, St& s, int, const int*, const Val* dv) const {
-    if (s.r == k) return Val{s.ht, s.ht};
-    const double wr = dv[s.rdep].w;
-    const double elev = s.ht;
-    double hk = s.ht;
-    if (elev > wr) {
-      if (s.nr > 0) {
-        if (n_is_one) {
-          double f = elev, df = 1.0;
-          for (int t = 0; t < s.nr; ++t)
-            if ((s.gate >> t) & 1) {
-              f = f + s.fact[t] * dv[t].h;
-              df = df + s.fact[t];
+          if (n_is_one) {
+            double f = elev, df = 1.0;
+            for (int t = 0; t < nq; ++t) {
+              f = f + fact[t] * hq[t];
+              df = df + fact[t];
             }
-          hk = f / df;
-        } else {
-          const double tolp = 1.0e-3;
-          double errp = 2.0 * tolp;
-          const double h0 = elev;
-          int guard = 0;
-          while (errp > tolp && guard++ < 10000) {
-            double f = hk - h0, df = 1.0;
-            for (int t = 0; t < s.nr; ++t)
-              if ((s.gate >> t) & 1) {
-                const double x = fmax(0.0, hk - dv[t].h);
-                f = f + s.fact[t] * pow(x, n);
-                df = df + s.fact[t] * n * pow(x, n - 1.0);
+            hk = f / df;
+          } else {
+            const double tolp = 1.0e-3;
+            double errp = 2.0 * tolp;
+            int guard = 0;
+            while (errp > tolp && guard++ < 10000) {
+              double f = hk - elev, df = 1.0;
+              for (int t = 0; t < nq; ++t) {
+                const double x = fmax(0.0, hk - hq[t]);
+                f = f + fact[t] * pow(x, n);
+                df = df + fact[t] * n * pow(x, n - 1.0);
               }
-            const double hn = hk - f / df;
-            errp = fabs(hn - hk);
-            hk = hk * (1.0 - omega) + hn * omega;
+              const double hn = hk - f / df;
+              errp = fabs(hn - hk);
+              hk = hk * (1.0 - omega) + hn * omega;
+            }
           }
         }
+        if (hk < wr) hk = wr;
+      } else {
+        hk = elev;
       }
-      if (hk < wr) hk = wr;
-    } else {
-      hk = elev;
+      wk = fmax(wr, hk);
     }
-    return Val{hk, fmax(wr, hk)};
-  }
-  __device__ void store(int k, const Val& v) const {
-    hnew[k] = v.h;
-    water[k] = v.w;
+    hnew[k] = hk;
+    water[k] = wk;
+    const int nd = R.dn[k];
+    if (nd) {
+      __threadfence();  // release hnew(k), water(k) before the donors' counters drop
+      for (int t = 0; t < nd; ++t) {
+        const int d = R.dep[(size_t)k * 8 + t];
+        if (dec_ready(cnt, d)) ready[nr++] = d;
+      }
+    }
   }
 };
-
-template <class Op, class Order>
-void run_wavefront(Ctx& c, const Op& op, const Order& od) {
-  c.epoch += 1;
-  if (c.epoch == 0) {  // flags wrapped: clear them so no stale epoch matches
-    cudaMemsetAsync(c.done, 0, sizeof(unsigned) * c.nn, c.stream);
-    c.epoch = 1;
-  }
-  cudaMemsetAsync(c.ticket, 0, sizeof(unsigned), c.stream);
-  int blocks = 148 * 8;
-  k_wavefront<Op, Order><<<blocks, kWarps * 32, 0, c.stream>>>(op, od, c.ticket, c.done, c.epoch, c.d_err);
-  c.count_launch();
-}
 
 // ---- find_mult_rec (FlowRouting.f90:200-243) --------------------------------
 __global__ void k_mfd_receivers(Bounds bd, double p, const double* __restrict__ h0, const double* __restrict__ ltab,
@@ -454,13 +291,56 @@ __global__ void k_mfd_receivers(Bounds bd, double p, const double* __restrict__ 
   }
 }
 
-// donor mask over the 3x3 block (bit (jj+1)*3+(ii+1)) for the pull-form accumulation
-__global__ void k_mfd_donor_mask(Bounds bd, const int* __restrict__ mrec, const int* __restrict__ mnrec,
-                                 int* __restrict__ mask) {
+// Records and counters of the multiple-flow sweeps (see MfdRecords).
+//   cnt_acc(k): distinct donors of k;  cnt_spl(k): distinct gated receivers
+//   of k plus rec(k) (0 for a root).
+__global__ void k_mfd_records(Bounds bd, int n_is_one, double kfsed, double dt, double m, double n,
+                              const int* __restrict__ rec, const int* __restrict__ mrec,
+                              const int* __restrict__ mnrec, const double* __restrict__ mwrec,
+                              const double* __restrict__ mlrec, const double* __restrict__ h,
+                              const double* __restrict__ b, const double* __restrict__ kf,
+                              const double* __restrict__ a, MfdRecords R, int* __restrict__ cnt_acc,
+                              int* __restrict__ cnt_spl) {
   const int nx = bd.nx, ny = bd.ny, nn = nx * ny;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
     const int i = k % nx, j = k / nx;
-    int m = 0;
+    const size_t o = (size_t)k * 8;
+    const double htk = h[k];
+    // distinct receivers and gated receivers of k
+    const int nr = mnrec[k];
+    int rn = 0, nq = 0;
+    const int r = rec[k];
+    const double kk = ((kfsed > 0.0 && (htk - b[k]) > 1.0) ? kfsed : kf[k]) * dt;
+    const double ak = a[k];
+    for (int t = 0; t < nr; ++t) {
+      const int q = mrec[o + t];
+      bool dup = false;
+      for (int u = 0; u < t; ++u) dup |= mrec[o + u] == q;
+      if (!dup) R.rcv[o + rn++] = q;
+      const double htq = h[q];
+      if (n_is_one ? (htk >= htq) : (htk > htq)) {
+        const double w = mwrec[o + t], l = mlrec[o + t];
+        R.q[o + nq] = q;
+        R.qf[o + nq] = n_is_one ? kk * pow(ak * w, m) / l : kk * pow(ak * w, m) / pow(l, n);
+        ++nq;
+      }
+    }
+    R.rn[k] = rn;
+    R.qn[k] = nq | (nr > 0 ? 256 : 0);
+    int cs = 0;
+    if (r != k) {
+      for (int t = 0; t < nq; ++t) {
+        bool dup = false;
+        for (int u = 0; u < t; ++u) dup |= R.q[o + u] == R.q[o + t];
+        if (!dup) ++cs;
+      }
+      bool r_gated = false;
+      for (int t = 0; t < nq; ++t) r_gated |= R.q[o + t] == r;
+      if (!r_gated) ++cs;
+    }
+    cnt_spl[k] = cs;
+    // donors (area inputs) and stream-power dependents among the 3x3 neighbours
+    int an = 0, dn = 0;
     int seen[9];
     int ns = 0;
     for (int jj = -1; jj <= 1; ++jj) {
@@ -477,12 +357,23 @@ __global__ void k_mfd_donor_mask(Bounds bd, const int* __restrict__ mrec, const 
         for (int t = 0; t < ns; ++t) dup |= seen[t] == d;
         if (dup) continue;
         seen[ns++] = d;
-        const int nr = mnrec[d];
-        for (int t = 0; t < nr; ++t)
-          if (mrec[(size_t)d * 8 + t] == k) { m |= 1 << ((jj + 1) * 3 + (ii + 1)); break; }
+        const int nd = mnrec[d];
+        double wsum = 0.0;
+        int hits = 0;
+        for (int t = 0; t < nd; ++t)
+          if (mrec[(size_t)d * 8 + t] == k) { wsum = hits ? wsum + mwrec[(size_t)d * 8 + t] : mwrec[(size_t)d * 8 + t]; ++hits; }
+        if (hits && an < 8) { R.ad[o + an] = d; R.aw[o + an] = wsum; ++an; }
+        const int rd = rec[d];
+        if (rd != d) {
+          const double htd = h[d];
+          const bool gated = hits && (n_is_one ? (htd >= htk) : (htd > htk));
+          if ((gated || rd == k) && dn < 8) R.dep[o + dn++] = d;
+        }
       }
     }
-    mask[k] = m;
+    R.an[k] = an;
+    R.dn[k] = dn;
+    cnt_acc[k] = an;
   }
 }
 
@@ -628,29 +519,94 @@ __global__ void k_diff_ycoef(Bounds bd, double dt2, double dx2, double dy2, cons
 }
 
 // tridag (Diffusion.f90:164-202) for independent systems s in [s0, s1):
-// element t of system s at [t*L + s]; the solution overwrites F.
-__global__ void k_thomas(int N, int L, int s0, int s1, const double* __restrict__ A, const double* __restrict__ B,
-                         const double* __restrict__ C, double* __restrict__ F, double* __restrict__ G,
-                         int* __restrict__ err) {
-  const int s = s0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= s1) return;
-  double bet = B[s];
-  if (bet == 0.0) { atomicExch(err, DEV_TRIDAG_ZERO); return; }
-  double up = F[s] / bet;
-  F[s] = up;
-  for (int t = 1; t < N; ++t) {
-    const size_t o = (size_t)t * L + s;
-    const double g = C[o - L] / bet;
-    G[o] = g;
-    bet = B[o] - A[o] * g;
-    if (bet == 0.0) { atomicExch(err, DEV_TRIDAG_ZERO); return; }
-    up = (F[o] - A[o] * up) / bet;
-    F[o] = up;
+// element t of system s at [t*L + s]; the solution overwrites F.  A block
+// of 32 threads solves 32 systems; coefficients are staged through shared
+// memory in chunks of kTC steps so that the sequential recurrence only waits
+// on arithmetic, not on DRAM latency.
+constexpr int kTC = 32;
+__device__ inline void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ inline void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+__global__ void __launch_bounds__(32) k_thomas(int N, int L, int s0, int s1, const double* __restrict__ A,
+                                               const double* __restrict__ B, const double* __restrict__ C,
+                                               double* __restrict__ F, double* __restrict__ G,
+                                               int* __restrict__ err) {
+  __shared__ double sa[kTC][33], sb[kTC][33], sc[kTC][33], sf[kTC][33];
+  const int lane = threadIdx.x;
+  const int s = s0 + blockIdx.x * 32 + lane;
+  const bool act = s < s1;
+  double bet = 0.0, up = 0.0;
+  bool bad = false;
+  for (int t0 = 0; t0 < N; t0 += kTC) {
+    const int tn = min(kTC, N - t0);
+    if (act) {  // all loads of the chunk in flight at once
+      for (int r = 0; r < tn; ++r) {
+        const size_t o = (size_t)(t0 + r) * L + s;
+        cp_async8(&sa[r][lane], &A[o]);
+        cp_async8(&sb[r][lane], &B[o]);
+        cp_async8(&sf[r][lane], &F[o]);
+        if (t0 + r > 0) cp_async8(&sc[r][lane], &C[o - L]);
+      }
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncwarp();
+    if (act && !bad) {
+      for (int r = 0; r < tn; ++r) {
+        const int t = t0 + r;
+        if (t == 0) {
+          bet = sb[0][lane];
+          if (bet == 0.0) { bad = true; break; }
+          up = sf[0][lane] / bet;
+          sf[0][lane] = up;
+          sc[0][lane] = 0.0;
+        } else {
+          const double g = sc[r][lane] / bet;
+          sc[r][lane] = g;
+          bet = sb[r][lane] - sa[r][lane] * g;
+          if (bet == 0.0) { bad = true; break; }
+          up = (sf[r][lane] - sa[r][lane] * up) / bet;
+          sf[r][lane] = up;
+        }
+      }
+    }
+    __syncwarp();
+    if (act)
+      for (int r = 0; r < tn; ++r) {
+        const size_t o = (size_t)(t0 + r) * L + s;
+        F[o] = sf[r][lane];
+        G[o] = sc[r][lane];
+      }
+    __syncwarp();
   }
-  for (int t = N - 2; t >= 0; --t) {
-    const size_t o = (size_t)t * L + s;
-    up = F[o] - G[o + L] * up;
-    F[o] = up;
+  if (bad) { atomicExch(err, DEV_TRIDAG_ZERO); return; }
+  // back substitution u(t) = u(t) - gam(t+1)*u(t+1), chunked from the end
+  if (act) up = F[(size_t)(N - 1) * L + s];
+  for (int t1 = N - 1; t1 > 0; t1 -= kTC) {
+    const int tlo = max(0, t1 - kTC);
+    const int tn = t1 - tlo;
+    if (act)
+      for (int r = 0; r < tn; ++r) {
+        const size_t o = (size_t)(tlo + r) * L + s;
+        cp_async8(&sf[r][lane], &F[o]);
+        cp_async8(&sc[r][lane], &G[o + L]);
+      }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncwarp();
+    if (act)
+      for (int r = tn - 1; r >= 0; --r) {
+        up = sf[r][lane] - sc[r][lane] * up;
+        sf[r][lane] = up;
+      }
+    __syncwarp();
+    if (act)
+      for (int r = 0; r < tn; ++r) F[(size_t)(tlo + r) * L + s] = sf[r][lane];
+    __syncwarp();
   }
 }
 
@@ -694,72 +650,89 @@ __global__ void k_diff_finish(Bounds bd, double dt, const double* __restrict__ U
 
 // ============================================================================
 
-void fill_sweep(Ctx& c) {
-  FillOp op{c.rec, c.h, c.hwater, c.lake_depth};
-  run_wavefront(c, op, Fwd{c.stack, c.pos, c.nn});
-}
-
 void mfd_receivers(Ctx& c) {
   const int nn = c.nn;
   k_mfd_receivers<<<grid1d(nn), kBlock, 0, c.stream>>>(c.bd, c.p, c.hwater, c.ltab, c.mrec, c.mnrec, c.mwrec, c.mlrec);
-  k_mfd_donor_mask<<<grid1d(nn), kBlock, 0, c.stream>>>(c.bd, c.mrec, c.mnrec, c.mdmask);
-  k_order_keys<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, c.stack, c.hwater, c.o_keys, c.o_vals);
-  c.count_launch(3);
-  sort_pairs_u64(c, c.o_keys, c.o_keys2, c.o_vals, c.o_vals2, nn);
-  k_order_finish<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, c.o_vals2, c.o_pos, c.mstack);
   c.count_launch();
+  if (c.capture) {  // a topological order of mrec (the reference's mstack is a LIFO Kahn order)
+    k_order_keys<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, c.stack, c.hwater, c.o_keys, c.o_vals);
+    c.count_launch();
+    sort_pairs_u64(c, c.o_keys, c.o_keys2, c.o_vals, c.o_vals2, nn);
+    k_order_finish<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, c.o_vals2, c.o_pos, c.mstack);
+    c.count_launch();
+  }
 }
 
+static MfdRecords records(Ctx& c) {
+  return MfdRecords{c.r_rn, c.r_rcv, c.r_an, c.r_ad, c.r_qn, c.r_q, c.r_dn, c.r_dep, c.r_aw, c.r_qf};
+}
+
+template <class Op>
+static void run_last_arriver(Ctx& c, Op op, const int* cnt0) {
+  const int nn = c.nn;
+  cudaMemcpyAsync(op.cnt, cnt0, sizeof(int) * nn, cudaMemcpyDeviceToDevice, c.stream);
+  cudaMemsetAsync(c.la_queue, 0xff, sizeof(int) * nn, c.stream);
+  cudaMemsetAsync(c.la_ctl, 0, sizeof(unsigned) * 128, c.stream);
+  k_seed_queue<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, cnt0, c.la_queue, c.la_ctl + 32);
+  k_last_arriver<Op><<<148 * 4, 128, 0, c.stream>>>(op, nn, c.size, c.la_queue, c.la_ctl, c.d_err);
+  c.count_launch(2);
+}
+
+void fill_sweep(Ctx& c) { fill_chains(c); }
+
 void accumulate(Ctx& c) {
-  const double dxdy = c.dx * c.dy;
+  if (!c.sfd) {  // donor/receiver records (the erosion factors are rebuilt after the area)
+    const int n1 = fabs(c.n - 1.0) < DBL_MIN;
+    k_mfd_records<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec, c.mnrec,
+                                                         c.mwrec, c.mlrec, c.h, c.b, c.kf, c.a, records(c),
+                                                         c.cnt_acc, c.cnt_spl);
+    c.count_launch();
+  }
   if (c.sfd) {
-    AccumSfdOp op{c.rec, c.ndon, c.don, c.precip, dxdy, c.a};
-    run_wavefront(c, op, Rev{c.stack, c.pos, c.nn});
+    area_chains(c);
   } else {
-    AccumMfdOp op{c.bd, c.mdmask, c.mrec, c.mnrec, c.mwrec, c.precip, dxdy, c.a};
-    run_wavefront(c, op, Rev{c.o_vals2, c.o_pos, c.nn});
+    AccMfdOp op{records(c), c.precip, c.dx * c.dy, c.a, c.la_cnt};
+    run_last_arriver(c, op, c.cnt_acc);
   }
 }
 
 void stream_power(Ctx& c) {
-  const bool n1 = fabs(c.n - 1.0) < DBL_MIN;
+  const int n1 = fabs(c.n - 1.0) < DBL_MIN;
   const double omega = 0.875 / c.n;
-  double* hnew = c.hnew;
   if (c.sfd) {
-    SplSfdOp op{c.rec, c.h, c.b, c.kf, c.a, c.length, c.kfsed, c.dt, c.m, c.n, omega, n1, hnew, c.water};
-    run_wavefront(c, op, Fwd{c.stack, c.pos, c.nn});
+    spl_chains(c, c.hnew);
   } else {
-    SplMfdOp op{c.rec, c.mrec, c.mnrec, c.mwrec, c.mlrec, c.h, c.b, c.kf, c.a, c.kfsed, c.dt, c.m, c.n, omega, n1,
-                hnew, c.water};
-    run_wavefront(c, op, Fwd{c.o_vals2, c.o_pos, c.nn});
+    // the erosion factors need the drainage area: build the records now
+    k_mfd_records<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec, c.mnrec,
+                                                         c.mwrec, c.mlrec, c.h, c.b, c.kf, c.a, records(c),
+                                                         c.cnt_acc, c.cnt_spl);
+    c.count_launch();
+    SplMfdOp op{records(c), c.rec, c.h, c.n, omega, n1, c.hnew, c.water, c.la_cnt};
+    run_last_arriver(c, op, c.cnt_spl);
   }
-  k_spl_finish<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nn, c.dt, hnew, c.h, c.b, c.etot, c.erate, c.sedflux);
+  k_spl_finish<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nn, c.dt, c.hnew, c.h, c.b, c.etot, c.erate, c.sedflux);
   c.count_launch();
 }
 
 void diffusion(Ctx& c) {
   const int nx = c.nx, ny = c.ny, nn = c.nn;
   const double dt2 = c.dt / 2.0, dx2 = c.dx * c.dx, dy2 = c.dy * c.dy;
-  double *K = c.dK, *A = c.dA, *B = c.dB, *C = c.dC, *F = c.dF, *G = c.dG;
+  double *K = c.dK, *A = c.dA, *B = c.dB, *C = c.dC, *F = c.dF, *G = c.dG, *Z = c.dZ;
   k_diff_kdint<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, c.kdsed, c.kd, c.h, c.b, K);
   c.count_launch();
-  if (ny >= 3) {
+  {
     dim3 g((nx + 127) / 128, ny - 2);
     k_diff_xcoef<<<g, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, c.h, A, B, C, F);
     // systems are rows j=1..ny-2 with element i at [i*ny + j]
-    k_thomas<<<(ny - 2 + 63) / 64, 64, 0, c.stream>>>(nx, ny, 1, ny - 1, A, B, C, F, G, c.d_err);
-    c.count_launch(2);
+    k_thomas<<<(ny - 2 + 31) / 32, 32, 0, c.stream>>>(nx, ny, 1, ny - 1, A, B, C, F, G, c.d_err);
+    dim3 g2((nx + 31) / 32, (ny + 31) / 32);
+    k_diff_xgather<<<g2, dim3(32, 8), 0, c.stream>>>(c.bd, F, c.h, Z);
+    c.count_launch(3);
   }
-  double* Z = c.dZ;
   {
-    dim3 g((nx + 31) / 32, (ny + 31) / 32);
-    k_diff_xgather<<<g, dim3(32, 8), 0, c.stream>>>(c.bd, F, c.h, Z);
-    c.count_launch();
-  }
-  if (nx >= 3) {
     dim3 g((nx + 127) / 128, ny);
     k_diff_ycoef<<<g, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, Z, A, B, C, F);
-    k_thomas<<<(nx - 2 + 63) / 64, 64, 0, c.stream>>>(ny, nx, 1, nx - 1, A, B, C, F, G, c.d_err);
+    k_thomas<<<(nx - 2 + 31) / 32, 32, 0, c.stream>>>(ny, nx, 1, nx - 1, A, B, C, F, G, c.d_err);
     c.count_launch(2);
   }
   k_diff_finish<<<grid1d(nn), kBlock, 0, c.stream>>>(c.bd, c.dt, F, c.h, c.b, c.etot, c.erate);

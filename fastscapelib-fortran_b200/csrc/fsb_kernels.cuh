@@ -83,6 +83,20 @@ struct Ctx {
   // MFD order
   unsigned long long *o_keys = nullptr, *o_keys2 = nullptr;
   int *o_vals = nullptr, *o_vals2 = nullptr, *o_pos = nullptr;
+  // heavy-path chain schedule (fsb_chains.cu)
+  int *ch_heavy = nullptr, *ch_tmp = nullptr, *ch_tmp2 = nullptr, *ch_nxt = nullptr, *ch_nxt2 = nullptr;
+  unsigned long long *ch_val = nullptr, *ch_val2 = nullptr;
+  int *ch_ord = nullptr, *ch_pos = nullptr, *ch_ldep = nullptr, *ch_start = nullptr, *ch_cid = nullptr,
+      *ch_sid = nullptr, *ch_hist = nullptr, *ch_goff = nullptr, *ch_tk_td = nullptr, *ch_tk_bu = nullptr;
+  unsigned *ch_key = nullptr, *ch_skey = nullptr;
+  int nchains = 0, ntickets_td = 0, ntickets_bu = 0, nroots = 0;
+  // last-arriver sweeps (multiple flow)
+  int *la_queue = nullptr, *la_cnt = nullptr, *cnt_acc = nullptr, *cnt_spl = nullptr;
+  int *r_rn = nullptr, *r_rcv = nullptr, *r_an = nullptr, *r_ad = nullptr, *r_qn = nullptr, *r_q = nullptr,
+      *r_dn = nullptr, *r_dep = nullptr;
+  double *r_aw = nullptr, *r_qf = nullptr;
+  unsigned* la_ctl = nullptr;  // head, tail, done count
+  int* s_scan2 = nullptr;
   // sweeps
   unsigned *done = nullptr;  // epoch flags per node
   unsigned epoch = 0;
@@ -130,6 +144,12 @@ void fetch_counters(Ctx& c, int n);  // d_cnt[0..n) -> h_cnt (synchronises the s
 
 // LocalMinima (fsb_locmin.cu); returns false and sets c.err on failure
 bool local_minima(Ctx& c);
+
+// chains (fsb_chains.cu)
+void build_chains(Ctx& c);          // heavy-first order + ticket lists of the current forest
+void fill_chains(Ctx& c);
+void area_chains(Ctx& c);
+void spl_chains(Ctx& c, double* hnew);
 
 // flow (fsb_flow.cu)
 void fill_sweep(Ctx& c);            // hwater along the stack (SFD lake fill / MFD h0)

@@ -619,8 +619,8 @@ bool local_minima(Ctx& c) {
   k_copy_nroots<<<1, 1, 0, st>>>(c.s_scan + nn, c.d_cnt);
   k_pos_root_flags<<<grid1d(nn), kBlock, 0, st>>>(nn, c.stack, c.rec, c.s_flag);
   c.count_launch(2);
-  inclusive_scan_int(c, c.s_flag, c.s_scan, nn);
-  k_basins<<<grid1d(nn), kBlock, 0, st>>>(nn, c.stack, c.s_scan, c.basins);
+  inclusive_scan_int(c, c.s_flag, c.s_scan2, nn);
+  k_basins<<<grid1d(nn), kBlock, 0, st>>>(nn, c.stack, c.s_scan2, c.basins);
   c.count_launch();
   fetch_counters(c, 10);
   const int nroots = c.h_cnt[C_NBASINS];
