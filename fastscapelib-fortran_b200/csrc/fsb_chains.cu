@@ -391,8 +391,16 @@ __global__ void __launch_bounds__(128) k_spl_chains(ChainView cv, const int* __r
                 double f = hk - elev, df = 1.0;
                 if (ht[i] > htr) {
                   const double x = fmax(0.0, hk - hr);
-                  f = f + fact[i] * pow(x, n);
-                  df = df + fact[i] * n * pow(x, n - 1.0);
+                  double pn, pn1;
+                  if (n == 1.5) {  // x^1.5 = x*sqrt(x), x^0.5 = sqrt(x)
+                    pn1 = sqrt(x);
+                    pn = x * pn1;
+                  } else {
+                    pn = pow(x, n);
+                    pn1 = pow(x, n - 1.0);
+                  }
+                  f = f + fact[i] * pn;
+                  df = df + fact[i] * n * pn1;
                 }
                 const double hn = hk - f / df;
                 errp = fabs(hn - hk);

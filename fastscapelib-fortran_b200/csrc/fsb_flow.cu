@@ -152,6 +152,36 @@ struct MfdRecords {
   double *aw, *qf;
 };
 
+// x^n and n*x^(n-1) for the Newton update.  For n = 1.5 they are evaluated
+// as x*sqrt(x) and 1.5*sqrt(x) (sqrt is correctly rounded); otherwise with pow.
+struct NewtonPow {
+  double n;
+  int half3;  // n == 1.5
+  __device__ void eval(double x, double& pn, double& pn1) const {
+    if (half3) {
+      const double r = sqrt(x);
+      pn = x * r;
+      pn1 = r;
+    } else {
+      pn = pow(x, n);
+      pn1 = pow(x, n - 1.0);
+    }
+  }
+};
+
+__device__ inline void load8i(const int* p, int* v) {
+  const int4 a = *reinterpret_cast<const int4*>(p), b = *reinterpret_cast<const int4*>(p + 4);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+__device__ inline void load8d(const double* p, double* v) {
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const double2 a = reinterpret_cast<const double2*>(p)[t];
+    v[2 * t] = a.x;
+    v[2 * t + 1] = a.y;
+  }
+}
+
 // a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115)
 struct AccMfdOp {
   MfdRecords R;
@@ -160,17 +190,24 @@ struct AccMfdOp {
   double* a;
   int* cnt;
   __device__ void process(int k, int* ready, int& nr) const {
+    const size_t o = (size_t)k * 8;
+    int ad[8], rcv[8];
+    double aw[8], av[8];
+    const int na = R.an[k], nrc = R.rn[k];
+    load8i(R.ad + o, ad);
+    load8d(R.aw + o, aw);
+    load8i(R.rcv + o, rcv);
     double acc = dxdy * precip[k];
-    const int na = R.an[k];
-    for (int t = 0; t < na; ++t) acc = acc + __ldcg(&a[R.ad[(size_t)k * 8 + t]]) * R.aw[(size_t)k * 8 + t];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) if (t < na) av[t] = __ldcg(&a[ad[t]]);
+#pragma unroll
+    for (int t = 0; t < 8; ++t) if (t < na) acc = acc + av[t] * aw[t];
     a[k] = acc;
-    const int nrc = R.rn[k];
     if (nrc) {
       __threadfence();  // release a(k) before the receivers' counters drop
-      for (int t = 0; t < nrc; ++t) {
-        const int r = R.rcv[(size_t)k * 8 + t];
-        if (dec_ready(cnt, r)) ready[nr++] = r;
-      }
+#pragma unroll
+      for (int t = 0; t < 8; ++t)
+        if (t < nrc && dec_ready(cnt, rcv[t])) ready[nr++] = rcv[t];
     }
   }
 };
@@ -182,33 +219,39 @@ struct SplMfdOp {
   MfdRecords R;
   const int* rec;
   const double* h;
-  double n, omega;
+  NewtonPow np;
+  double omega;
   int n_is_one;
   double* hnew;
   double* water;
   int* cnt;
   __device__ void process(int k, int* ready, int& nr) const {
+    const size_t o = (size_t)k * 8;
     const int r = rec[k];
     const double ht = h[k];
+    const int qn = R.qn[k], nd = R.dn[k];
+    int q[8], dep[8];
+    double fact[8], hq[8];
+    load8i(R.q + o, q);
+    load8d(R.qf + o, fact);
+    load8i(R.dep + o, dep);
     double hk = ht, wk = ht;
     if (r != k) {
+      const int nq = qn & 255;
       const double wr = __ldcg(&water[r]);
+#pragma unroll
+      for (int t = 0; t < 8; ++t) if (t < nq) hq[t] = __ldcg(&hnew[q[t]]);
       const double elev = ht;
       if (elev > wr) {
-        const int qn = R.qn[k];
         if (qn & 256) {  // mnrec(k) > 0
-          const int nq = qn & 255;
-          double fact[8], hq[8];
-          for (int t = 0; t < nq; ++t) {
-            fact[t] = R.qf[(size_t)k * 8 + t];
-            hq[t] = __ldcg(&hnew[R.q[(size_t)k * 8 + t]]);
-          }
           if (n_is_one) {
             double f = elev, df = 1.0;
-            for (int t = 0; t < nq; ++t) {
-              f = f + fact[t] * hq[t];
-              df = df + fact[t];
-            }
+#pragma unroll
+            for (int t = 0; t < 8; ++t)
+              if (t < nq) {
+                f = f + fact[t] * hq[t];
+                df = df + fact[t];
+              }
             hk = f / df;
           } else {
             const double tolp = 1.0e-3;
@@ -216,11 +259,15 @@ struct SplMfdOp {
             int guard = 0;
             while (errp > tolp && guard++ < 10000) {
               double f = hk - elev, df = 1.0;
-              for (int t = 0; t < nq; ++t) {
-                const double x = fmax(0.0, hk - hq[t]);
-                f = f + fact[t] * pow(x, n);
-                df = df + fact[t] * n * pow(x, n - 1.0);
-              }
+#pragma unroll
+              for (int t = 0; t < 8; ++t)
+                if (t < nq) {
+                  const double x = fmax(0.0, hk - hq[t]);
+                  double pn, pn1;
+                  np.eval(x, pn, pn1);
+                  f = f + fact[t] * pn;
+                  df = df + fact[t] * np.n * pn1;
+                }
               const double hn = hk - f / df;
               errp = fabs(hn - hk);
               hk = hk * (1.0 - omega) + hn * omega;
@@ -235,13 +282,11 @@ struct SplMfdOp {
     }
     hnew[k] = hk;
     water[k] = wk;
-    const int nd = R.dn[k];
     if (nd) {
       __threadfence();  // release hnew(k), water(k) before the donors' counters drop
-      for (int t = 0; t < nd; ++t) {
-        const int d = R.dep[(size_t)k * 8 + t];
-        if (dec_ready(cnt, d)) ready[nr++] = d;
-      }
+#pragma unroll
+      for (int t = 0; t < 8; ++t)
+        if (t < nd && dec_ready(cnt, dep[t])) ready[nr++] = dep[t];
     }
   }
 };
@@ -707,7 +752,7 @@ void stream_power(Ctx& c) {
                                                          c.mwrec, c.mlrec, c.h, c.b, c.kf, c.a, records(c),
                                                          c.cnt_acc, c.cnt_spl);
     c.count_launch();
-    SplMfdOp op{records(c), c.rec, c.h, c.n, omega, n1, c.hnew, c.water, c.la_cnt};
+    SplMfdOp op{records(c), c.rec, c.h, NewtonPow{c.n, c.n == 1.5}, omega, n1, c.hnew, c.water, c.la_cnt};
     run_last_arriver(c, op, c.cnt_spl);
   }
   k_spl_finish<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nn, c.dt, c.hnew, c.h, c.b, c.etot, c.erate, c.sedflux);
