@@ -288,6 +288,11 @@ int step_once(fsb::Ctx& c) {
 
 }  // namespace
 
+namespace fsb {
+// lets other translation units report through fsb_last_error()
+int report_error(const std::string& msg) { return fail(msg); }
+}  // namespace fsb
+
 extern "C" {
 
 const char* fsb_last_error(void) { return g_err.c_str(); }

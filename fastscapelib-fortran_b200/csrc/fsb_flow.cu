@@ -784,4 +784,30 @@ void diffusion(Ctx& c) {
   c.count_launch();
 }
 
+// The same ADI step on caller-supplied arrays: `scratch` holds 7*nx*ny
+// doubles (kdint, the four coefficient arrays, the forward factors and the
+// x-pass result); `err` receives DEV_TRIDAG_ZERO on a zero pivot.
+void diffusion_raw(const Bounds& bd, double dx, double dy, double dt, double kdsed, const double* kd, double* h,
+                   double* b, double* etot, double* erate, double* scratch, int* err, cudaStream_t st) {
+  const int nx = bd.nx, ny = bd.ny, nn = nx * ny;
+  const double dt2 = dt / 2.0, dx2 = dx * dx, dy2 = dy * dy;
+  double* K = scratch;
+  double* A = K + nn;
+  double* B = A + nn;
+  double* C = B + nn;
+  double* F = C + nn;
+  double* G = F + nn;
+  double* Z = G + nn;
+  k_diff_kdint<<<grid1d(nn), kBlock, 0, st>>>(nn, kdsed, kd, h, b, K);
+  dim3 gx((nx + 127) / 128, ny - 2);
+  k_diff_xcoef<<<gx, 128, 0, st>>>(bd, dt2, dx2, dy2, K, h, A, B, C, F);
+  k_thomas<<<(ny - 2 + 31) / 32, 32, 0, st>>>(nx, ny, 1, ny - 1, A, B, C, F, G, err);
+  dim3 gt((nx + 31) / 32, (ny + 31) / 32);
+  k_diff_xgather<<<gt, dim3(32, 8), 0, st>>>(bd, F, h, Z);
+  dim3 gy((nx + 127) / 128, ny);
+  k_diff_ycoef<<<gy, 128, 0, st>>>(bd, dt2, dx2, dy2, K, Z, A, B, C, F);
+  k_thomas<<<(nx - 2 + 31) / 32, 32, 0, st>>>(ny, nx, 1, nx - 1, A, B, C, F, G, err);
+  k_diff_finish<<<grid1d(nn), kBlock, 0, st>>>(bd, dt, F, h, b, etot, erate);
+}
+
 }  // namespace fsb

@@ -126,6 +126,9 @@ struct Ctx {
   std::string err;
 };
 
+// sets the message fsb_last_error() returns; returns 1 (fsb_api.cu)
+int report_error(const std::string& msg);
+
 // routing (fsb_routing.cu)
 void launch_uplift(Ctx& c);
 void launch_find_receiver(Ctx& c, const double* h, int* rec, double* length);
@@ -157,5 +160,7 @@ void mfd_receivers(Ctx& c);         // find_mult_rec: mrec, mnrec, mlrec, mwrec,
 void accumulate(Ctx& c);            // drainage area
 void stream_power(Ctx& c);          // implicit stream power law (g == 0)
 void diffusion(Ctx& c);             // ADI hillslope diffusion
+void diffusion_raw(const Bounds& bd, double dx, double dy, double dt, double kdsed, const double* kd, double* h,
+                   double* b, double* etot, double* erate, double* scratch, int* err, cudaStream_t st);
 
 }  // namespace fsb
