@@ -35,16 +35,23 @@ __device__ inline unsigned long long ordered_key(double x) {
 // thread that sees the count reach zero fences again before using the node
 __device__ inline bool dec_ready(int* cnt, int r) { return atomicSub(&cnt[r], 1) == 1; }
 
+// Reads a dependency's value produced by another thread: through L2
+// (__ldcg), after the acquire fence of the hand-off.
+struct Loc {
+  __device__ double ld(const double* p, int) const { return __ldcg(p); }
+};
+
 // ---- last-arriver sweep engine ----------------------------------------------
-// Op::process(k, ready[], nready) computes node k, then decrements the
-// counters of k's dependents and lists those that became ready.  Idle lanes
-// claim queue slots in order (one atomic per warp); a lane keeps its claim
+// Op::run(k, dep[], loc) computes node k, stores its outputs and lists k's
+// dependents; the engine then decrements their counters, continues with the
+// ready dependent of largest subtree and queues the other ready ones.  Idle
+// lanes claim queue slots in order (one atomic per warp) and keep a claim
 // until a producer fills it.  The kernel ends when every node is done.
 // Control words: ctl[0] queue head, ctl[32] queue tail, ctl[64] nodes done
 // (separate 128-byte lines).
 template <class Op>
-__global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, const int* __restrict__ prio, int* queue,
-                                                      unsigned* ctl, int* err) {
+__global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, const int* __restrict__ prio,
+                                                      int* queue, unsigned* ctl, int* err) {
   unsigned* qhead = ctl;
   unsigned* qtail = ctl + 32;
   unsigned* ndone = ctl + 64;
@@ -68,26 +75,29 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, const int* 
       const int v = *(volatile int*)&queue[slot];
       if (v >= 0) { cur = v; slot = -1; }
     }
-    int ready[9];
+    int ready[8];
     int nr = 0;
     if (cur >= 0) {
       __threadfence();  // acquire: the node's inputs were published before it became ready
-      op.process(cur, ready, nr);
+      int dep[8], pr[8];
+      const int nd = op.run(cur, dep, Loc{});
+      for (int t = 0; t < nd; ++t) pr[t] = prio[dep[t]];
+      if (nd) {
+        __threadfence();  // release the node's outputs before its dependents' counters drop
+        for (int t = 0; t < nd; ++t)
+          if (dec_ready(cnt, dep[t])) { pr[nr] = pr[t]; ready[nr++] = dep[t]; }
+      }
       ++local_done;
-      // continue with the ready dependent that has the largest subtree of the
-      // single-flow tree: that keeps the long paths inside one thread
-      if (nr > 1) {
-        int best = 0, bs = prio[ready[0]];
-        for (int q = 1; q < nr; ++q) {
-          const int v = prio[ready[q]];
-          if (v > bs) { bs = v; best = q; }
-        }
+      if (nr > 1) {  // continue with the ready dependent of largest subtree
+        int best = 0;
+        for (int q = 1; q < nr; ++q)
+          if (pr[q] > pr[best]) best = q;
         const int tmp = ready[0]; ready[0] = ready[best]; ready[best] = tmp;
       }
       cur = nr > 0 ? ready[0] : -1;
     }
     bool fenced = false;
-    for (int e = 1; e < 9; ++e) {  // push the other ready nodes, one atomic per warp
+    for (int e = 1; e < 8; ++e) {  // queue the other ready nodes, one atomic per warp
       const bool has = e < nr;
       const unsigned mm = __ballot_sync(FULL, has);
       if (!mm) break;
@@ -169,6 +179,8 @@ struct NewtonPow {
   }
 };
 
+__device__ inline void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 __device__ inline void load8i(const int* p, int* v) {
   const int4 a = *reinterpret_cast<const int4*>(p), b = *reinterpret_cast<const int4*>(p + 4);
   v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
@@ -182,39 +194,43 @@ __device__ inline void load8d(const double* p, double* v) {
   }
 }
 
-// a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115)
+// a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115);
+// k's dependents are its distinct receivers.
 struct AccMfdOp {
   MfdRecords R;
   const double* precip;
   double dxdy;
   double* a;
-  int* cnt;
-  __device__ void process(int k, int* ready, int& nr) const {
+  __device__ int run(int k, int* dep, const Loc& loc) const {
     const size_t o = (size_t)k * 8;
-    int ad[8], rcv[8];
+    int ad[8];
     double aw[8], av[8];
     const int na = R.an[k], nrc = R.rn[k];
     load8i(R.ad + o, ad);
     load8d(R.aw + o, aw);
-    load8i(R.rcv + o, rcv);
+    load8i(R.rcv + o, dep);
+#pragma unroll
+    for (int t = 0; t < 8; ++t)  // the receivers come next in this sweep
+      if (t < nrc) {
+        const size_t ro = (size_t)dep[t] * 8;
+        prefetch_l2(R.ad + ro);
+        prefetch_l2(R.aw + ro);
+        prefetch_l2(R.aw + ro + 4);
+        prefetch_l2(R.rcv + ro);
+      }
     double acc = dxdy * precip[k];
 #pragma unroll
-    for (int t = 0; t < 8; ++t) if (t < na) av[t] = __ldcg(&a[ad[t]]);
+    for (int t = 0; t < 8; ++t) if (t < na) av[t] = loc.ld(&a[ad[t]], ad[t]);
 #pragma unroll
     for (int t = 0; t < 8; ++t) if (t < na) acc = acc + av[t] * aw[t];
     a[k] = acc;
-    if (nrc) {
-      __threadfence();  // release a(k) before the receivers' counters drop
-#pragma unroll
-      for (int t = 0; t < 8; ++t)
-        if (t < nrc && dec_ready(cnt, rcv[t])) ready[nr++] = rcv[t];
-    }
+    return nrc;
   }
 };
 
 // implicit stream power law over the multiple receivers with g == 0
 // (StreamPowerLaw.f90:92-177): the new elevation goes to hnew, the water
-// surface to water; h keeps ht.
+// surface to water; h keeps ht.  k's dependents are the donors that read it.
 struct SplMfdOp {
   MfdRecords R;
   const int* rec;
@@ -224,23 +240,31 @@ struct SplMfdOp {
   int n_is_one;
   double* hnew;
   double* water;
-  int* cnt;
-  __device__ void process(int k, int* ready, int& nr) const {
+  __device__ int run(int k, int* dep, const Loc& loc) const {
     const size_t o = (size_t)k * 8;
     const int r = rec[k];
     const double ht = h[k];
     const int qn = R.qn[k], nd = R.dn[k];
-    int q[8], dep[8];
+    int q[8];
     double fact[8], hq[8];
     load8i(R.q + o, q);
     load8d(R.qf + o, fact);
     load8i(R.dep + o, dep);
+#pragma unroll
+    for (int t = 0; t < 8; ++t)  // the donors come next in this sweep
+      if (t < nd) {
+        const size_t ro = (size_t)dep[t] * 8;
+        prefetch_l2(R.q + ro);
+        prefetch_l2(R.qf + ro);
+        prefetch_l2(R.qf + ro + 4);
+        prefetch_l2(R.dep + ro);
+      }
     double hk = ht, wk = ht;
     if (r != k) {
       const int nq = qn & 255;
-      const double wr = __ldcg(&water[r]);
+      const double wr = loc.ld(&water[r], r);
 #pragma unroll
-      for (int t = 0; t < 8; ++t) if (t < nq) hq[t] = __ldcg(&hnew[q[t]]);
+      for (int t = 0; t < 8; ++t) if (t < nq) hq[t] = loc.ld(&hnew[q[t]], q[t]);
       const double elev = ht;
       if (elev > wr) {
         if (qn & 256) {  // mnrec(k) > 0
@@ -282,12 +306,7 @@ struct SplMfdOp {
     }
     hnew[k] = hk;
     water[k] = wk;
-    if (nd) {
-      __threadfence();  // release hnew(k), water(k) before the donors' counters drop
-#pragma unroll
-      for (int t = 0; t < 8; ++t)
-        if (t < nd && dec_ready(cnt, dep[t])) ready[nr++] = dep[t];
-    }
+    return nd;
   }
 };
 
@@ -713,13 +732,13 @@ static MfdRecords records(Ctx& c) {
 }
 
 template <class Op>
-static void run_last_arriver(Ctx& c, Op op, const int* cnt0) {
+static void run_sweep(Ctx& c, Op op, const int* cnt0) {
   const int nn = c.nn;
-  cudaMemcpyAsync(op.cnt, cnt0, sizeof(int) * nn, cudaMemcpyDeviceToDevice, c.stream);
+  cudaMemcpyAsync(c.la_cnt, cnt0, sizeof(int) * nn, cudaMemcpyDeviceToDevice, c.stream);
   cudaMemsetAsync(c.la_queue, 0xff, sizeof(int) * nn, c.stream);
   cudaMemsetAsync(c.la_ctl, 0, sizeof(unsigned) * 128, c.stream);
   k_seed_queue<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, cnt0, c.la_queue, c.la_ctl + 32);
-  k_last_arriver<Op><<<148 * 4, 128, 0, c.stream>>>(op, nn, c.size, c.la_queue, c.la_ctl, c.d_err);
+  k_last_arriver<Op><<<148 * 4, 128, 0, c.stream>>>(op, nn, c.la_cnt, c.size, c.la_queue, c.la_ctl, c.d_err);
   c.count_launch(2);
 }
 
@@ -736,8 +755,8 @@ void accumulate(Ctx& c) {
   if (c.sfd) {
     area_chains(c);
   } else {
-    AccMfdOp op{records(c), c.precip, c.dx * c.dy, c.a, c.la_cnt};
-    run_last_arriver(c, op, c.cnt_acc);
+    AccMfdOp op{records(c), c.precip, c.dx * c.dy, c.a};
+    run_sweep(c, op, c.cnt_acc);
   }
 }
 
@@ -752,8 +771,8 @@ void stream_power(Ctx& c) {
                                                          c.mwrec, c.mlrec, c.h, c.b, c.kf, c.a, records(c),
                                                          c.cnt_acc, c.cnt_spl);
     c.count_launch();
-    SplMfdOp op{records(c), c.rec, c.h, NewtonPow{c.n, c.n == 1.5}, omega, n1, c.hnew, c.water, c.la_cnt};
-    run_last_arriver(c, op, c.cnt_spl);
+    SplMfdOp op{records(c), c.rec, c.h, NewtonPow{c.n, c.n == 1.5}, omega, n1, c.hnew, c.water};
+    run_sweep(c, op, c.cnt_spl);
   }
   k_spl_finish<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nn, c.dt, c.hnew, c.h, c.b, c.etot, c.erate, c.sedflux);
   c.count_launch();
