@@ -46,7 +46,7 @@ __device__ inline void wait_flag(unsigned* done, int k, unsigned epoch, int* err
     __nanosleep(back);
     if (back < 512) back <<= 1;
   }
-  __threadfence();
+  fence_acq_rel();
 }
 
 // heavy child: donor with the largest subtree, first in ascending order on ties
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(128) k_fill_chains(ChainView cv, const int* __
       }
 #pragma unroll
       for (int i = 0; i < kCF; ++i) if (i < n) { hwater[kk[i]] = out[i]; lake_depth[kk[i]] = out[i] - hh[i]; }
-      __threadfence();
+      fence_acq_rel();
 #pragma unroll
       for (int i = 0; i < kCF; ++i) if (i < n && nd[i] > 1) *(volatile unsigned*)&done[kk[i]] = epoch;
     }
@@ -317,7 +317,7 @@ __global__ void __launch_bounds__(128) k_area_chains(ChainView cv, const int* __
         child = k;
       }
     }
-    __threadfence();
+    fence_acq_rel();
     *(volatile unsigned*)&done[cv.ord[s]] = epoch;
   }
 }
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(128) k_spl_chains(ChainView cv, const int* __r
       }
 #pragma unroll
       for (int i = 0; i < kCS; ++i) if (i < cn) { hnew[kk[i]] = ho[i]; water[kk[i]] = wo[i]; }
-      __threadfence();
+      fence_acq_rel();
 #pragma unroll
       for (int i = 0; i < kCS; ++i) if (i < cn && nd[i] > 1) *(volatile unsigned*)&done[kk[i]] = epoch;
     }

@@ -47,4 +47,13 @@ enum DeviceError : int {
 
 constexpr int kSpinLimit = 1 << 21;  // polls (~1 s) before a bounded wait gives up
 
+#ifdef __CUDACC__
+// Acquire/release fence at GPU scope.  Hand-offs between threads use the
+// pattern "write; fence; relaxed atomic or flag store" on the producer side
+// and "relaxed atomic or flag load; fence; read" on the consumer side, which
+// needs acquire-release ordering only -- not the sequentially consistent
+// fence that __threadfence() issues.
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+#endif
+
 }  // namespace fsb

@@ -78,12 +78,12 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, c
     int ready[8];
     int nr = 0;
     if (cur >= 0) {
-      __threadfence();  // acquire: the node's inputs were published before it became ready
+      fence_acq_rel();  // acquire: the node's inputs were published before it became ready
       int dep[8], pr[8];
       const int nd = op.run(cur, dep, Loc{});
       for (int t = 0; t < nd; ++t) pr[t] = prio[dep[t]];
       if (nd) {
-        __threadfence();  // release the node's outputs before its dependents' counters drop
+        fence_acq_rel();  // release the node's outputs before its dependents' counters drop
         for (int t = 0; t < nd; ++t)
           if (dec_ready(cnt, dep[t])) { pr[nr] = pr[t]; ready[nr++] = dep[t]; }
       }
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, c
       base = __shfl_sync(FULL, base, leader);
       if (has) {
         const unsigned idx = base + __popc(mm & lt);
-        if (!fenced) { __threadfence(); fenced = true; }
+        if (!fenced) { fence_acq_rel(); fenced = true; }
         if (idx < (unsigned)nn) *(volatile int*)&queue[idx] = ready[e];
         else atomicExch(err, DEV_OVERFLOW);
       }
@@ -179,7 +179,7 @@ struct NewtonPow {
   }
 };
 
-__device__ inline void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+__device__ inline void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
 __device__ inline void load8i(const int* p, int* v) {
   const int4 a = *reinterpret_cast<const int4*>(p), b = *reinterpret_cast<const int4*>(p + 4);
@@ -210,13 +210,15 @@ struct AccMfdOp {
     load8d(R.aw + o, aw);
     load8i(R.rcv + o, dep);
 #pragma unroll
-    for (int t = 0; t < 8; ++t)  // the receivers come next in this sweep
+    for (int t = 0; t < 8; ++t)  // the receivers come next, usually in this thread
       if (t < nrc) {
         const size_t ro = (size_t)dep[t] * 8;
-        prefetch_l2(R.ad + ro);
-        prefetch_l2(R.aw + ro);
-        prefetch_l2(R.aw + ro + 4);
-        prefetch_l2(R.rcv + ro);
+        prefetch_l1(R.ad + ro);
+        prefetch_l1(R.aw + ro);
+        prefetch_l1(R.aw + ro + 4);
+        prefetch_l1(R.rcv + ro);
+        prefetch_l1(&R.an[dep[t]]);
+        prefetch_l1(&R.rn[dep[t]]);
       }
     double acc = dxdy * precip[k];
 #pragma unroll
@@ -251,13 +253,17 @@ struct SplMfdOp {
     load8d(R.qf + o, fact);
     load8i(R.dep + o, dep);
 #pragma unroll
-    for (int t = 0; t < 8; ++t)  // the donors come next in this sweep
+    for (int t = 0; t < 8; ++t)  // the donors come next, usually in this thread
       if (t < nd) {
         const size_t ro = (size_t)dep[t] * 8;
-        prefetch_l2(R.q + ro);
-        prefetch_l2(R.qf + ro);
-        prefetch_l2(R.qf + ro + 4);
-        prefetch_l2(R.dep + ro);
+        prefetch_l1(R.q + ro);
+        prefetch_l1(R.qf + ro);
+        prefetch_l1(R.qf + ro + 4);
+        prefetch_l1(R.dep + ro);
+        prefetch_l1(&R.qn[dep[t]]);
+        prefetch_l1(&R.dn[dep[t]]);
+        prefetch_l1(&rec[dep[t]]);
+        prefetch_l1(&h[dep[t]]);
       }
     double hk = ht, wk = ht;
     if (r != k) {
