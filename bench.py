@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", type=int, default=2049)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=4)
     return ap.parse_args()
 
 
@@ -87,8 +87,15 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    procs = max(1, min(os.cpu_count() or 1, 16))
-    # bounded sample: the reference needs ~5 s per 2049^2 step on one core
+    # one single-threaded instance per host core, as many as host memory allows
+    # (about 2.5 GB per 2049^2 instance); each needs ~4 s per 2049^2 step
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        import psutil
+        mem_cap = int(psutil.virtual_memory().available / (2.5e9 * (args.size / 2049.0) ** 2))
+    except Exception:
+        mem_cap = cores
+    procs = max(1, min(cores, mem_cap))
     with mp.get_context("spawn").Pool(procs) as pool:
         t0 = time.perf_counter()
         res = pool.map(_oracle_worker, [(args.size, 12345 + r, args.warmup, args.steps)
