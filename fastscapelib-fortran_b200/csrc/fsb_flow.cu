@@ -209,17 +209,6 @@ struct AccMfdOp {
     load8i(R.ad + o, ad);
     load8d(R.aw + o, aw);
     load8i(R.rcv + o, dep);
-#pragma unroll
-    for (int t = 0; t < 8; ++t)  // the receivers come next, usually in this thread
-      if (t < nrc) {
-        const size_t ro = (size_t)dep[t] * 8;
-        prefetch_l1(R.ad + ro);
-        prefetch_l1(R.aw + ro);
-        prefetch_l1(R.aw + ro + 4);
-        prefetch_l1(R.rcv + ro);
-        prefetch_l1(&R.an[dep[t]]);
-        prefetch_l1(&R.rn[dep[t]]);
-      }
     double acc = dxdy * precip[k];
 #pragma unroll
     for (int t = 0; t < 8; ++t) if (t < na) av[t] = loc.ld(&a[ad[t]], ad[t]);
