@@ -129,9 +129,7 @@ size_t layout(fsb::Ctx& c, char* base) {
   c.ch_key = L.take<unsigned>(2 * N); c.ch_skey = L.take<unsigned>(N);
   c.la_queue = L.take<int>(N); c.la_cnt = L.take<int>(N); c.cnt_acc = L.take<int>(N); c.cnt_spl = L.take<int>(N);
   c.la_ctl = L.take<unsigned>(128);
-  c.r_rn = L.take<int>(N); c.r_rcv = L.take<int>(8 * N); c.r_an = L.take<int>(N); c.r_ad = L.take<int>(8 * N);
-  c.r_qn = L.take<int>(N); c.r_q = L.take<int>(8 * N); c.r_dn = L.take<int>(N); c.r_dep = L.take<int>(8 * N);
-  c.r_aw = L.take<double>(8 * N); c.r_qf = L.take<double>(8 * N);
+  c.mfd_line = L.take<double>(16 * N); c.hw = L.take<double>(2 * N);
   c.s_scan2 = L.take<int>(N + 1);
   c.done = L.take<unsigned>(N); c.ticket = L.take<unsigned>(4);
   c.water = L.take<double>(N); c.hnew = L.take<double>(N);
@@ -193,6 +191,7 @@ int check_device_error(fsb::Ctx& c) {
       case fsb::DEV_STACK_ERROR: return fail("error in stack");
       case fsb::DEV_TRIDAG_ZERO: return fail("tridag failed");
       case fsb::DEV_OVERFLOW: return fail("device: buffer overflow");
+      case fsb::DEV_NOT_ADJACENT: return fail("device: a receiver is not a neighbour of its donor");
       default: return fail("device error " + std::to_string(e));
     }
   }

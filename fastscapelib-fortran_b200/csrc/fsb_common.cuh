@@ -43,6 +43,7 @@ enum DeviceError : int {
   DEV_STACK_ERROR = 2,      // a traversal did not cover every node
   DEV_TRIDAG_ZERO = 3,      // zero pivot in the tridiagonal solve
   DEV_OVERFLOW = 4,         // a data-dependent buffer bound was exceeded
+  DEV_NOT_ADJACENT = 5,     // a receiver is not one of the node's 3x3 neighbours
 };
 
 constexpr int kSpinLimit = 1 << 21;  // polls (~1 s) before a bounded wait gives up

@@ -31,10 +31,6 @@ __device__ inline unsigned long long ordered_key(double x) {
   return (u & 0x8000000000000000ull) ? ~u : (u | 0x8000000000000000ull);
 }
 
-// relaxed decrement; the caller issued a release fence before it and the
-// thread that sees the count reach zero fences again before using the node
-__device__ inline bool dec_ready(int* cnt, int r) { return atomicSub(&cnt[r], 1) == 1; }
-
 // Reads a dependency's value produced by another thread: through L2
 // (__ldcg), after the acquire fence of the hand-off.
 struct Loc {
@@ -42,16 +38,28 @@ struct Loc {
 };
 
 // ---- last-arriver sweep engine ----------------------------------------------
-// Op::run(k, dep[], loc) computes node k, stores its outputs and lists k's
-// dependents; the engine then decrements their counters, continues with the
-// ready dependent of largest subtree and queues the other ready ones.  Idle
-// lanes claim queue slots in order (one atomic per warp) and keep a claim
-// until a producer fills it.  The kernel ends when every node is done.
+// Op::run(k, dep[], pr[], loc) computes node k, stores its outputs and lists
+// k's dependents with their priorities; the engine then decrements their
+// counters, continues with the ready dependent of largest priority (subtree
+// size) and queues the other ready ones.  Idle lanes claim queue slots in
+// order (one atomic per warp) and keep a claim until a producer fills it.
+// The kernel ends when every node is done.
 // Control words: ctl[0] queue head, ctl[32] queue tail, ctl[64] nodes done
 // (separate 128-byte lines).
-template <class Op>
-__global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, const int* __restrict__ prio,
-                                                      int* queue, unsigned* ctl, int* err) {
+// Only the first LANES lanes of a warp take nodes: a warp moves through a hop
+// in lockstep, so fewer nodes per warp shorten the critical node's wait on
+// its warp mates' loads and Newton iterations.  The sweeps are bound by their
+// critical path, not by node throughput; at 2049^2 (B200) 8 lanes suit the
+// area sweep and 1 lane the stream-power sweep (32 lanes: 25.8 and 46.1 ms,
+// these: 24.4 and 41.2 ms).
+#ifndef FSB_LANES_ACC
+#define FSB_LANES_ACC 8
+#endif
+#ifndef FSB_LANES_SPL
+#define FSB_LANES_SPL 1
+#endif
+template <class Op, int LANES>
+__global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, int* queue, unsigned* ctl, int* err) {
   unsigned* qhead = ctl;
   unsigned* qtail = ctl + 32;
   unsigned* ndone = ctl + 64;
@@ -62,7 +70,7 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, c
   unsigned local_done = 0;
   int back = 32;
   for (int it = 0; it < (1 << 24); ++it) {
-    const bool want = cur < 0 && slot < 0;
+    const bool want = lane < LANES && cur < 0 && slot < 0;
     const unsigned m = __ballot_sync(FULL, want);
     if (m) {
       const int leader = __ffs(m) - 1;
@@ -75,41 +83,48 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, c
       const int v = *(volatile int*)&queue[slot];
       if (v >= 0) { cur = v; slot = -1; }
     }
-    int ready[8];
-    int nr = 0;
+    int dep[8];
+    unsigned rdy = 0;  // bit t: dependent t became ready and goes to the queue
     if (cur >= 0) {
       fence_acq_rel();  // acquire: the node's inputs were published before it became ready
-      int dep[8], pr[8];
-      const int nd = op.run(cur, dep, Loc{});
-      for (int t = 0; t < nd; ++t) pr[t] = prio[dep[t]];
+      unsigned pr[8];
+      const int nd = op.run(cur, dep, pr, Loc{});
+      int nxt = -1;
       if (nd) {
         fence_acq_rel();  // release the node's outputs before its dependents' counters drop
-        for (int t = 0; t < nd; ++t)
-          if (dec_ready(cnt, dep[t])) { pr[nr] = pr[t]; ready[nr++] = dep[t]; }
+        int old[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) old[t] = t < nd ? atomicSub(&cnt[dep[t]], 1) : 0;
+        unsigned bp = 0;
+        int bi = -1;
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+          if (t < nd && old[t] == 1) {
+            rdy |= 1u << t;
+            if (bi < 0 || pr[t] > bp) { bp = pr[t]; bi = t; nxt = dep[t]; }
+          }
+        if (bi >= 0) rdy &= ~(1u << bi);
       }
       ++local_done;
-      if (nr > 1) {  // continue with the ready dependent of largest subtree
-        int best = 0;
-        for (int q = 1; q < nr; ++q)
-          if (pr[q] > pr[best]) best = q;
-        const int tmp = ready[0]; ready[0] = ready[best]; ready[best] = tmp;
-      }
-      cur = nr > 0 ? ready[0] : -1;
+      cur = nxt;
     }
-    bool fenced = false;
-    for (int e = 1; e < 8; ++e) {  // queue the other ready nodes, one atomic per warp
-      const bool has = e < nr;
-      const unsigned mm = __ballot_sync(FULL, has);
-      if (!mm) break;
-      const int leader = __ffs(mm) - 1;
-      unsigned base = 0;
-      if (lane == leader) base = atomicAdd(qtail, (unsigned)__popc(mm));
-      base = __shfl_sync(FULL, base, leader);
-      if (has) {
-        const unsigned idx = base + __popc(mm & lt);
-        if (!fenced) { fence_acq_rel(); fenced = true; }
-        if (idx < (unsigned)nn) *(volatile int*)&queue[idx] = ready[e];
-        else atomicExch(err, DEV_OVERFLOW);
+    if (__ballot_sync(FULL, rdy != 0)) {  // queue the other ready nodes, one atomic per warp
+      bool fenced = false;
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const bool has = (rdy >> t) & 1u;
+        const unsigned mm = __ballot_sync(FULL, has);
+        if (!mm) continue;
+        const int leader = __ffs(mm) - 1;
+        unsigned base = 0;
+        if (lane == leader) base = atomicAdd(qtail, (unsigned)__popc(mm));
+        base = __shfl_sync(FULL, base, leader);
+        if (has) {
+          const unsigned idx = base + __popc(mm & lt);
+          if (!fenced) { fence_acq_rel(); fenced = true; }
+          if (idx < (unsigned)nn) *(volatile int*)&queue[idx] = dep[t];
+          else atomicExch(err, DEV_OVERFLOW);
+        }
       }
     }
     const unsigned busy = __ballot_sync(FULL, cur >= 0);
@@ -132,6 +147,7 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, c
   if (lane == 0) atomicExch(err, DEV_SPIN_LIMIT);
 }
 
+
 // initial queue: nodes whose counter is zero
 __global__ void k_seed_queue(int nn, const int* __restrict__ cnt, int* __restrict__ queue, unsigned* qtail) {
   const int lane = threadIdx.x & 31;
@@ -148,18 +164,68 @@ __global__ void k_seed_queue(int nn, const int* __restrict__ cnt, int* __restric
   }
 }
 
-// Compact per-node records of the multiple-flow sweeps (slot t of node k at
-// [k*8 + t]), built in parallel before the sweeps by k_mfd_records:
-//   r_rn/r_rcv      distinct receivers of k (dependents in the area sweep)
-//   r_an/r_ad/r_aw  distinct donors d of k and the summed weight of d's slots
-//                   targeting k (inputs of the area sweep)
-//   r_qn/r_q/r_qf   receivers whose erosion term is gated on (ht(k) >= ht(q),
-//                   or > for n != 1) and their factor kf*dt*(a*w)^m/l^n; bit 8
-//                   of r_qn marks mnrec(k) > 0
-//   r_dn/r_dep      donors that wait for k in the stream-power sweep
-struct MfdRecords {
-  int *rn, *rcv, *an, *ad, *qn, *q, *dn, *dep;
-  double *aw, *qf;
+// ---- per-node records of the multiple-flow sweeps ---------------------------
+// Each node has one 128-byte line, built in parallel before a sweep, holding
+// everything the sweep reads about the node except its dependencies' values.
+// Neighbours are 4-bit codes 1 + 3*(dj+1) + (di+1) (0 = empty slot), eight to
+// a 32-bit word with slot t in bits 4t..4t+3, filled from slot 0; they are
+// decoded with the grid's wrap-around.  Priorities are the upper 16 bits of
+// the float value of the neighbour's single-flow subtree size (monotonic).
+//
+// Area line:    aw[8]  summed weight of donor t's slots targeting k
+//               base   dx*dy*precip(k)
+//               don    codes of the distinct donors (inputs)
+//               rcv    codes of the distinct receivers (dependents), pr[8]
+// Stream-power line:
+//               fact[8] kf*dt*(a*w)^m/l^n of receiver slot t whose erosion
+//                       term is gated on (ht(k) >= ht(q), or > for n != 1)
+//               ht      h(k)
+//               q       codes of those receiver slots
+//               dep     codes of the donors that wait for k (gated, or rec == k), pr[8]
+//               meta    code of rec(k) (0: k is a root); bit 4 set when mnrec(k) > 0
+struct __align__(128) AccLine {
+  double aw[8];
+  double base;
+  unsigned don, rcv;
+  unsigned short pr[8];
+  int pad[8];
+};
+struct __align__(128) SplLine {
+  double fact[8];
+  double ht;
+  unsigned q, dep;
+  unsigned short pr[8];
+  int meta;
+  int pad[7];
+};
+static_assert(sizeof(AccLine) == 128 && sizeof(SplLine) == 128, "one line per node");
+
+__device__ inline unsigned short prio16(int size) { return (unsigned short)(__float_as_uint((float)size) >> 16); }
+
+__device__ inline unsigned nbr_code(int di, int dj) { return 1u + 3u * (unsigned)(dj + 1) + (unsigned)(di + 1); }
+
+// code of neighbour q of node (i, j); sets *err when q is not a 3x3 neighbour
+__device__ inline unsigned nbr_code_of(int i, int j, int q, int nx, int ny, int* err) {
+  int di = q % nx - i, dj = q / nx - j;
+  if (di > 1) di -= nx; else if (di < -1) di += nx;
+  if (dj > 1) dj -= ny; else if (dj < -1) dj += ny;
+  if (di < -1 || di > 1 || dj < -1 || dj > 1 || (di == 0 && dj == 0)) {
+    atomicExch(err, DEV_NOT_ADJACENT);
+    return 0u;
+  }
+  return nbr_code(di, dj);
+}
+
+struct NbrDecoder {
+  int nx, ny, i, j;
+  __device__ NbrDecoder(int k, int nx_, int ny_) : nx(nx_), ny(ny_), i(k % nx_), j(k / nx_) {}
+  __device__ int at(unsigned code) const {
+    const int c = (int)code - 1;
+    int x = i + c % 3 - 1, y = j + c / 3 - 1;
+    x += x < 0 ? nx : (x >= nx ? -nx : 0);
+    y += y < 0 ? ny : (y >= ny ? -ny : 0);
+    return x + y * nx;
+  }
 };
 
 // x^n and n*x^(n-1) for the Newton update.  For n = 1.5 they are evaluated
@@ -181,95 +247,103 @@ struct NewtonPow {
 
 __device__ inline void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
-__device__ inline void load8i(const int* p, int* v) {
-  const int4 a = *reinterpret_cast<const int4*>(p), b = *reinterpret_cast<const int4*>(p + 4);
-  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-}
-__device__ inline void load8d(const double* p, double* v) {
+// the first N 16-byte words of a record line (read-only during the sweep)
+template <int N>
+union LineWords {
+  int4 v[N];
+  double d[2 * N];
+  unsigned u[4 * N];
+  unsigned short s[8 * N];
+  __device__ explicit LineWords(const void* p) {
 #pragma unroll
-  for (int t = 0; t < 4; ++t) {
-    const double2 a = reinterpret_cast<const double2*>(p)[t];
-    v[2 * t] = a.x;
-    v[2 * t + 1] = a.y;
+    for (int t = 0; t < N; ++t) v[t] = __ldg(reinterpret_cast<const int4*>(p) + t);
   }
-}
+};
 
 // a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115);
 // k's dependents are its distinct receivers.
 struct AccMfdOp {
-  MfdRecords R;
-  const double* precip;
-  double dxdy;
+  const AccLine* line;
+  int nx, ny;
   double* a;
-  __device__ int run(int k, int* dep, const Loc& loc) const {
-    const size_t o = (size_t)k * 8;
-    int ad[8];
-    double aw[8], av[8];
-    const int na = R.an[k], nrc = R.rn[k];
-    load8i(R.ad + o, ad);
-    load8d(R.aw + o, aw);
-    load8i(R.rcv + o, dep);
-    double acc = dxdy * precip[k];
+  __device__ int run(int k, int* dep, unsigned* pr, const Loc& loc) const {
+    const LineWords<6> L(line + k);  // aw[0..7] = d[0..7], base = d[8], don = u[18], rcv = u[19], pr = s[40..47]
+    const NbrDecoder nb(k, nx, ny);
+    const unsigned dc = L.u[18], rc = L.u[19];
+    double av[8];
 #pragma unroll
-    for (int t = 0; t < 8; ++t) if (t < na) av[t] = loc.ld(&a[ad[t]], ad[t]);
+    for (int t = 0; t < 8; ++t) {
+      const unsigned c = (dc >> (4 * t)) & 15u;
+      if (c) { const int d = nb.at(c); av[t] = loc.ld(&a[d], d); }
+    }
+    int nd = 0;
 #pragma unroll
-    for (int t = 0; t < 8; ++t) if (t < na) acc = acc + av[t] * aw[t];
+    for (int t = 0; t < 8; ++t) {
+      const unsigned c = (rc >> (4 * t)) & 15u;
+      if (c) {
+        dep[t] = nb.at(c);
+        pr[t] = L.s[40 + t];
+        prefetch_l1(line + dep[t]);  // the receivers come next, usually in this thread
+        nd = t + 1;
+      }
+    }
+    double acc = L.d[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if ((dc >> (4 * t)) & 15u) acc = acc + av[t] * L.d[t];
     a[k] = acc;
-    return nrc;
+    return nd;
   }
 };
 
 // implicit stream power law over the multiple receivers with g == 0
-// (StreamPowerLaw.f90:92-177): the new elevation goes to hnew, the water
-// surface to water; h keeps ht.  k's dependents are the donors that read it.
+// (StreamPowerLaw.f90:92-177): the new elevation and the water surface go to
+// hw[k] = (h, water); h keeps ht.  k's dependents are the donors that read it.
 struct SplMfdOp {
-  MfdRecords R;
-  const int* rec;
-  const double* h;
+  const SplLine* line;
+  int nx, ny;
   NewtonPow np;
   double omega;
   int n_is_one;
-  double* hnew;
-  double* water;
-  __device__ int run(int k, int* dep, const Loc& loc) const {
-    const size_t o = (size_t)k * 8;
-    const int r = rec[k];
-    const double ht = h[k];
-    const int qn = R.qn[k], nd = R.dn[k];
-    int q[8];
-    double fact[8], hq[8];
-    load8i(R.q + o, q);
-    load8d(R.qf + o, fact);
-    load8i(R.dep + o, dep);
+  double2* hw;
+  __device__ int run(int k, int* dep, unsigned* pr, const Loc& loc) const {
+    // fact = d[0..7], ht = d[8], q = u[18], dep = u[19], pr = s[40..47], meta = u[24]
+    const LineWords<7> L(line + k);
+    const NbrDecoder nb(k, nx, ny);
+    const unsigned qc = L.u[18], dc = L.u[19], meta = L.u[24];
+    const double ht = L.d[8];
+    int nd = 0;
 #pragma unroll
-    for (int t = 0; t < 8; ++t)  // the donors come next, usually in this thread
-      if (t < nd) {
-        const size_t ro = (size_t)dep[t] * 8;
-        prefetch_l1(R.q + ro);
-        prefetch_l1(R.qf + ro);
-        prefetch_l1(R.qf + ro + 4);
-        prefetch_l1(R.dep + ro);
-        prefetch_l1(&R.qn[dep[t]]);
-        prefetch_l1(&R.dn[dep[t]]);
-        prefetch_l1(&rec[dep[t]]);
-        prefetch_l1(&h[dep[t]]);
+    for (int t = 0; t < 8; ++t) {
+      const unsigned c = (dc >> (4 * t)) & 15u;
+      if (c) {
+        dep[t] = nb.at(c);
+        pr[t] = L.s[40 + t];
+        prefetch_l1(line + dep[t]);  // the donors come next, usually in this thread
+        nd = t + 1;
       }
+    }
     double hk = ht, wk = ht;
-    if (r != k) {
-      const int nq = qn & 255;
-      const double wr = loc.ld(&water[r], r);
+    const unsigned rcode = meta & 15u;
+    if (rcode) {
+      const int r = nb.at(rcode);
+      double hq[8];
+      const double wr = loc.ld(&hw[r].y, r);
 #pragma unroll
-      for (int t = 0; t < 8; ++t) if (t < nq) hq[t] = loc.ld(&hnew[q[t]], q[t]);
+      for (int t = 0; t < 8; ++t) {
+        const unsigned c = (qc >> (4 * t)) & 15u;
+        if (c) { const int q = nb.at(c); hq[t] = loc.ld(&hw[q].x, q); }
+      }
       const double elev = ht;
       if (elev > wr) {
-        if (qn & 256) {  // mnrec(k) > 0
+        if (meta & 16u) {  // mnrec(k) > 0
           if (n_is_one) {
             double f = elev, df = 1.0;
 #pragma unroll
             for (int t = 0; t < 8; ++t)
-              if (t < nq) {
-                f = f + fact[t] * hq[t];
-                df = df + fact[t];
+              if ((qc >> (4 * t)) & 15u) {
+                f = f + L.d[t] * hq[t];
+                df = df + L.d[t];
               }
             hk = f / df;
           } else {
@@ -280,12 +354,12 @@ struct SplMfdOp {
               double f = hk - elev, df = 1.0;
 #pragma unroll
               for (int t = 0; t < 8; ++t)
-                if (t < nq) {
+                if ((qc >> (4 * t)) & 15u) {
                   const double x = fmax(0.0, hk - hq[t]);
                   double pn, pn1;
                   np.eval(x, pn, pn1);
-                  f = f + fact[t] * pn;
-                  df = df + fact[t] * np.n * pn1;
+                  f = f + L.d[t] * pn;
+                  df = df + L.d[t] * np.n * pn1;
                 }
               const double hn = hk - f / df;
               errp = fabs(hn - hk);
@@ -299,11 +373,11 @@ struct SplMfdOp {
       }
       wk = fmax(wr, hk);
     }
-    hnew[k] = hk;
-    water[k] = wk;
+    hw[k] = make_double2(hk, wk);
     return nd;
   }
 };
+
 
 // ---- find_mult_rec (FlowRouting.f90:200-243) --------------------------------
 __global__ void k_mfd_receivers(Bounds bd, double p, const double* __restrict__ h0, const double* __restrict__ ltab,
@@ -350,58 +424,35 @@ __global__ void k_mfd_receivers(Bounds bd, double p, const double* __restrict__ 
   }
 }
 
-// Records and counters of the multiple-flow sweeps (see MfdRecords).
-//   cnt_acc(k): distinct donors of k;  cnt_spl(k): distinct gated receivers
-//   of k plus rec(k) (0 for a root).
-__global__ void k_mfd_records(Bounds bd, int n_is_one, double kfsed, double dt, double m, double n,
-                              const int* __restrict__ rec, const int* __restrict__ mrec,
-                              const int* __restrict__ mnrec, const double* __restrict__ mwrec,
-                              const double* __restrict__ mlrec, const double* __restrict__ h,
-                              const double* __restrict__ b, const double* __restrict__ kf,
-                              const double* __restrict__ a, MfdRecords R, int* __restrict__ cnt_acc,
-                              int* __restrict__ cnt_spl) {
+// Area lines and counters: cnt_acc(k) = number of distinct donors of k.
+__global__ void k_acc_lines(Bounds bd, double dxdy, const int* __restrict__ mrec, const int* __restrict__ mnrec,
+                            const double* __restrict__ mwrec, const double* __restrict__ precip,
+                            const int* __restrict__ prio, AccLine* __restrict__ line, int* __restrict__ cnt_acc,
+                            int* err) {
   const int nx = bd.nx, ny = bd.ny, nn = nx * ny;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
     const int i = k % nx, j = k / nx;
     const size_t o = (size_t)k * 8;
-    const double htk = h[k];
-    // distinct receivers and gated receivers of k
+    AccLine L;
+    // distinct receivers (dependents)
     const int nr = mnrec[k];
-    int rn = 0, nq = 0;
-    const int r = rec[k];
-    const double kk = ((kfsed > 0.0 && (htk - b[k]) > 1.0) ? kfsed : kf[k]) * dt;
-    const double ak = a[k];
+    unsigned rcv = 0;
+    int rn = 0;
+    for (int t = 0; t < 8; ++t) L.pr[t] = 0;
     for (int t = 0; t < nr; ++t) {
       const int q = mrec[o + t];
       bool dup = false;
       for (int u = 0; u < t; ++u) dup |= mrec[o + u] == q;
-      if (!dup) R.rcv[o + rn++] = q;
-      const double htq = h[q];
-      if (n_is_one ? (htk >= htq) : (htk > htq)) {
-        const double w = mwrec[o + t], l = mlrec[o + t];
-        R.q[o + nq] = q;
-        R.qf[o + nq] = n_is_one ? kk * pow(ak * w, m) / l : kk * pow(ak * w, m) / pow(l, n);
-        ++nq;
-      }
+      if (dup) continue;
+      rcv |= nbr_code_of(i, j, q, nx, ny, err) << (4 * rn);
+      L.pr[rn] = prio16(prio[q]);
+      ++rn;
     }
-    R.rn[k] = rn;
-    R.qn[k] = nq | (nr > 0 ? 256 : 0);
-    int cs = 0;
-    if (r != k) {
-      for (int t = 0; t < nq; ++t) {
-        bool dup = false;
-        for (int u = 0; u < t; ++u) dup |= R.q[o + u] == R.q[o + t];
-        if (!dup) ++cs;
-      }
-      bool r_gated = false;
-      for (int t = 0; t < nq; ++t) r_gated |= R.q[o + t] == r;
-      if (!r_gated) ++cs;
-    }
-    cnt_spl[k] = cs;
-    // donors (area inputs) and stream-power dependents among the 3x3 neighbours
-    int an = 0, dn = 0;
+    // distinct donors among the 3x3 neighbours and the summed weight of their slots to k
+    unsigned don = 0;
+    int an = 0, ns = 0;
     int seen[9];
-    int ns = 0;
+    for (int t = 0; t < 8; ++t) L.aw[t] = 0.0;
     for (int jj = -1; jj <= 1; ++jj) {
       int y = j + jj;
       if (y < 0) { if (!bd.ycyc) continue; y += ny; }
@@ -421,20 +472,102 @@ __global__ void k_mfd_records(Bounds bd, int n_is_one, double kfsed, double dt, 
         int hits = 0;
         for (int t = 0; t < nd; ++t)
           if (mrec[(size_t)d * 8 + t] == k) { wsum = hits ? wsum + mwrec[(size_t)d * 8 + t] : mwrec[(size_t)d * 8 + t]; ++hits; }
-        if (hits && an < 8) { R.ad[o + an] = d; R.aw[o + an] = wsum; ++an; }
-        const int rd = rec[d];
-        if (rd != d) {
-          const double htd = h[d];
-          const bool gated = hits && (n_is_one ? (htd >= htk) : (htd > htk));
-          if ((gated || rd == k) && dn < 8) R.dep[o + dn++] = d;
-        }
+        if (hits && an < 8) { don |= nbr_code(ii, jj) << (4 * an); L.aw[an] = wsum; ++an; }
       }
     }
-    R.an[k] = an;
-    R.dn[k] = dn;
+    L.base = dxdy * precip[k];
+    L.don = don;
+    L.rcv = rcv;
+    for (int t = 0; t < 8; ++t) L.pad[t] = 0;
+    line[k] = L;
     cnt_acc[k] = an;
   }
 }
+
+// Stream-power lines and counters: cnt_spl(k) = distinct gated receivers of k
+// plus rec(k) when it is not among them (0 for a root).
+__global__ void k_spl_lines(Bounds bd, int n_is_one, double kfsed, double dt, double m, double n,
+                            const int* __restrict__ rec, const int* __restrict__ mrec, const int* __restrict__ mnrec,
+                            const double* __restrict__ mwrec, const double* __restrict__ mlrec,
+                            const double* __restrict__ h, const double* __restrict__ b, const double* __restrict__ kf,
+                            const double* __restrict__ a, const int* __restrict__ prio, SplLine* __restrict__ line,
+                            int* __restrict__ cnt_spl, int* err) {
+  const int nx = bd.nx, ny = bd.ny, nn = nx * ny;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const int i = k % nx, j = k / nx;
+    const size_t o = (size_t)k * 8;
+    SplLine L;
+    const double htk = h[k];
+    const int nr = mnrec[k];
+    const int r = rec[k];
+    const double kk = ((kfsed > 0.0 && (htk - b[k]) > 1.0) ? kfsed : kf[k]) * dt;
+    const double ak = a[k];
+    int qv[8];
+    unsigned qc = 0;
+    int nq = 0;
+    for (int t = 0; t < 8; ++t) { L.fact[t] = 0.0; L.pr[t] = 0; }
+    for (int t = 0; t < nr; ++t) {
+      const int q = mrec[o + t];
+      if (n_is_one ? (htk >= h[q]) : (htk > h[q])) {
+        const double w = mwrec[o + t], l = mlrec[o + t];
+        qv[nq] = q;
+        qc |= nbr_code_of(i, j, q, nx, ny, err) << (4 * nq);
+        L.fact[nq] = n_is_one ? kk * pow(ak * w, m) / l : kk * pow(ak * w, m) / pow(l, n);
+        ++nq;
+      }
+    }
+    int cs = 0;
+    if (r != k) {
+      for (int t = 0; t < nq; ++t) {
+        bool dup = false;
+        for (int u = 0; u < t; ++u) dup |= qv[u] == qv[t];
+        if (!dup) ++cs;
+      }
+      bool r_gated = false;
+      for (int t = 0; t < nq; ++t) r_gated |= qv[t] == r;
+      if (!r_gated) ++cs;
+    }
+    // donors that wait for k: they read hnew(k) (gated) or water(k) (rec == k)
+    unsigned dc = 0;
+    int dn = 0, ns = 0;
+    int seen[9];
+    for (int jj = -1; jj <= 1; ++jj) {
+      int y = j + jj;
+      if (y < 0) { if (!bd.ycyc) continue; y += ny; }
+      if (y >= ny) { if (!bd.ycyc) continue; y -= ny; }
+      for (int ii = -1; ii <= 1; ++ii) {
+        int x = i + ii;
+        if (x < 0) { if (!bd.xcyc) continue; x += nx; }
+        if (x >= nx) { if (!bd.xcyc) continue; x -= nx; }
+        const int d = x + y * nx;
+        if (d == k) continue;
+        bool dup = false;
+        for (int t = 0; t < ns; ++t) dup |= seen[t] == d;
+        if (dup) continue;
+        seen[ns++] = d;
+        const int rd = rec[d];
+        if (rd == d) continue;
+        bool hits = false;
+        const int nd = mnrec[d];
+        for (int t = 0; t < nd; ++t) hits |= mrec[(size_t)d * 8 + t] == k;
+        const bool gated = hits && (n_is_one ? (h[d] >= htk) : (h[d] > htk));
+        if ((gated || rd == k) && dn < 8) {
+          dc |= nbr_code(ii, jj) << (4 * dn);
+          L.pr[dn] = prio16(prio[d]);
+          ++dn;
+        }
+      }
+    }
+    L.ht = htk;
+    L.q = qc;
+    L.dep = dc;
+    L.meta = (int)((r != k ? nbr_code_of(i, j, r, nx, ny, err) : 0u) | (nr > 0 ? 16u : 0u));
+    for (int t = 0; t < 7; ++t) L.pad[t] = 0;
+    line[k] = L;
+    cnt_spl[k] = cs;
+  }
+}
+
 
 // topological order for the MFD sweeps: ascending h0, ties in stack order
 __global__ void k_order_keys(int nn, const int* __restrict__ stack, const double* __restrict__ h0,
@@ -456,11 +589,12 @@ __global__ void k_order_finish(int nn, const int* __restrict__ ord, int* __restr
 
 // SPL epilogue (StreamPowerLaw.f90:380-393 with g == 0): b=min(h,b),
 // etot=etot+ht-h, erate=(ht-h)/dt, Sedflux=ht-h.
-__global__ void k_spl_finish(int nn, double dt, const double* __restrict__ hnew, double* __restrict__ h,
+// The new elevation of node k is hnew[k * stride].
+__global__ void k_spl_finish(int nn, double dt, const double* __restrict__ hnew, int stride, double* __restrict__ h,
                              double* __restrict__ b, double* __restrict__ etot, double* __restrict__ erate,
                              double* __restrict__ sedflux) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
-    const double ht = h[k], hn = hnew[k];
+    const double ht = h[k], hn = hnew[(size_t)k * stride];
     b[k] = fmin(hn, b[k]);
     etot[k] = etot[k] + ht - hn;
     erate[k] = (ht - hn) / dt;
@@ -722,37 +856,29 @@ void mfd_receivers(Ctx& c) {
   }
 }
 
-static MfdRecords records(Ctx& c) {
-  return MfdRecords{c.r_rn, c.r_rcv, c.r_an, c.r_ad, c.r_qn, c.r_q, c.r_dn, c.r_dep, c.r_aw, c.r_qf};
-}
-
-template <class Op>
+template <int LANES, class Op>
 static void run_sweep(Ctx& c, Op op, const int* cnt0) {
   const int nn = c.nn;
   cudaMemcpyAsync(c.la_cnt, cnt0, sizeof(int) * nn, cudaMemcpyDeviceToDevice, c.stream);
   cudaMemsetAsync(c.la_queue, 0xff, sizeof(int) * nn, c.stream);
   cudaMemsetAsync(c.la_ctl, 0, sizeof(unsigned) * 128, c.stream);
   k_seed_queue<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, cnt0, c.la_queue, c.la_ctl + 32);
-  k_last_arriver<Op><<<148 * 4, 128, 0, c.stream>>>(op, nn, c.la_cnt, c.size, c.la_queue, c.la_ctl, c.d_err);
+  k_last_arriver<Op, LANES><<<148 * 4, 128, 0, c.stream>>>(op, nn, c.la_cnt, c.la_queue, c.la_ctl, c.d_err);
   c.count_launch(2);
 }
 
 void fill_sweep(Ctx& c) { fill_chains(c); }
 
 void accumulate(Ctx& c) {
-  if (!c.sfd) {  // donor/receiver records (the erosion factors are rebuilt after the area)
-    const int n1 = fabs(c.n - 1.0) < DBL_MIN;
-    k_mfd_records<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec, c.mnrec,
-                                                         c.mwrec, c.mlrec, c.h, c.b, c.kf, c.a, records(c),
-                                                         c.cnt_acc, c.cnt_spl);
-    c.count_launch();
-  }
   if (c.sfd) {
     area_chains(c);
-  } else {
-    AccMfdOp op{records(c), c.precip, c.dx * c.dy, c.a};
-    run_sweep(c, op, c.cnt_acc);
+    return;
   }
+  AccLine* line = static_cast<AccLine*>(c.mfd_line);
+  k_acc_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, c.dx * c.dy, c.mrec, c.mnrec, c.mwrec, c.precip, c.size,
+                                                     line, c.cnt_acc, c.d_err);
+  c.count_launch();
+  run_sweep<FSB_LANES_ACC>(c, AccMfdOp{line, c.nx, c.ny, c.a}, c.cnt_acc);
 }
 
 void stream_power(Ctx& c) {
@@ -760,16 +886,18 @@ void stream_power(Ctx& c) {
   const double omega = 0.875 / c.n;
   if (c.sfd) {
     spl_chains(c, c.hnew);
-  } else {
-    // the erosion factors need the drainage area: build the records now
-    k_mfd_records<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec, c.mnrec,
-                                                         c.mwrec, c.mlrec, c.h, c.b, c.kf, c.a, records(c),
-                                                         c.cnt_acc, c.cnt_spl);
+    k_spl_finish<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nn, c.dt, c.hnew, 1, c.h, c.b, c.etot, c.erate, c.sedflux);
     c.count_launch();
-    SplMfdOp op{records(c), c.rec, c.h, NewtonPow{c.n, c.n == 1.5}, omega, n1, c.hnew, c.water};
-    run_sweep(c, op, c.cnt_spl);
+    return;
   }
-  k_spl_finish<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nn, c.dt, c.hnew, c.h, c.b, c.etot, c.erate, c.sedflux);
+  // the erosion factors need the drainage area: the lines are built now
+  SplLine* line = static_cast<SplLine*>(c.mfd_line);
+  k_spl_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec, c.mnrec, c.mwrec,
+                                                     c.mlrec, c.h, c.b, c.kf, c.a, c.size, line, c.cnt_spl, c.d_err);
+  c.count_launch();
+  double2* hw = reinterpret_cast<double2*>(c.hw);
+  run_sweep<FSB_LANES_SPL>(c, SplMfdOp{line, c.nx, c.ny, NewtonPow{c.n, c.n == 1.5}, omega, n1, hw}, c.cnt_spl);
+  k_spl_finish<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nn, c.dt, c.hw, 2, c.h, c.b, c.etot, c.erate, c.sedflux);
   c.count_launch();
 }
 

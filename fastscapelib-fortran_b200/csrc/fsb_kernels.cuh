@@ -92,9 +92,8 @@ struct Ctx {
   int nchains = 0, ntickets_td = 0, ntickets_bu = 0, nroots = 0;
   // last-arriver sweeps (multiple flow)
   int *la_queue = nullptr, *la_cnt = nullptr, *cnt_acc = nullptr, *cnt_spl = nullptr;
-  int *r_rn = nullptr, *r_rcv = nullptr, *r_an = nullptr, *r_ad = nullptr, *r_qn = nullptr, *r_q = nullptr,
-      *r_dn = nullptr, *r_dep = nullptr;
-  double *r_aw = nullptr, *r_qf = nullptr;
+  void* mfd_line = nullptr;  // one 128-byte record per node (area, then stream power)
+  double* hw = nullptr;      // (elevation, water surface) pairs of the stream-power sweep
   unsigned* la_ctl = nullptr;  // head, tail, done count
   int* s_scan2 = nullptr;
   // sweeps
