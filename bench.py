@@ -9,6 +9,13 @@ the same trajectory.  The grid's working set (~4 GB) is far larger than the
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
+Two more workloads (one GPU, reported on their own JSON line):
+
+    python bench.py --workload batched   # 256 uneven single-flow grids, 100 steps each,
+                                         # run concurrently by a Batch (fsb_batch_*)
+    python bench.py --workload served    # multiple-flow requests with Poisson arrivals at
+                                         # five rates: p50/p99 latency and node-steps/s
+
 Multi-GPU runs are independent replicas (one instance per GPU, no collective):
 a single grid's routing tree, basin graph and implicit solves are global
 dependencies, so the path does not shard; value = nodes*steps of all ranks /
@@ -46,6 +53,15 @@ def parse():
     ap.add_argument("--size", type=int, default=2049)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--workload", default="mfd", choices=["mfd", "batched", "served"])
+    ap.add_argument("--workers", type=int, default=32, help="batch worker streams")
+    ap.add_argument("--grids", type=int, default=256, help="batched: number of grids")
+    ap.add_argument("--job-steps", type=int, default=100, help="batched: steps per grid")
+    ap.add_argument("--requests", type=int, default=12, help="served: requests per rate")
+    ap.add_argument("--step-scale", type=float, default=0.2,
+                    help="served: scale of the 20..400 steps per request")
+    ap.add_argument("--max-side", type=int, default=4097, help="served: largest grid side")
+    ap.add_argument("--mem-budget", type=float, default=150e9, help="device bytes for jobs")
     return ap.parse_args()
 
 
@@ -300,9 +316,157 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# many grids on one GPU: batched and served forms
+
+def _batch_cpu_sample(wls, seconds=10.0):
+    """The oracle (1 thread) on the first grids of a list, two steps each."""
+    import oracle as O
+    t = nodes = 0.0
+    used = 0
+    for w in wls:
+        w.apply(O)
+        t0 = time.perf_counter()
+        for _ in range(2):
+            O.fastscape_execute_step()
+        t += time.perf_counter() - t0
+        nodes += 2 * w.nn
+        used += 1
+        if t > seconds:
+            break
+    return {"value": nodes / t, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"first {used} grids x 2 steps, C++ restatement of the reference (oracle/), "
+                      f"1 thread, {t:.1f} s"}
+
+
+def run_batched(args):
+    import numpy as np
+    import torch
+    import fastscapelib_fortran as fs
+    from fastscapelib_fortran import workloads as W
+
+    torch.cuda.set_device(0)
+    wls = W.uneven_d8(args.grids, nsteps=args.job_steps)
+    cpu = None if args.no_cpu_baseline else _batch_cpu_sample(wls)
+    # the work table is submitted largest grid first, so that no large grid
+    # starts last and runs alone at the end
+    wls.sort(key=lambda w: -w.nn * w.nsteps)
+    node_steps = sum(w.nn * w.nsteps for w in wls)
+    with fs.Batch(workers=args.workers, mem_budget=int(args.mem_budget)) as b:
+        # warm-up: one small job per worker (library, streams, memory pool)
+        b.run([w.job() for w in W.uneven_d8(args.workers, seed=999, nsteps=max(args.warmup, 1),
+                                            lo=129, hi=257)])
+        jobs = [w.job() for w in wls]
+        clocks = ClockSampler(0, os.path.join(ROOT, "gpurun_out", "clocks_batched.csv")
+                              if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp/clocks_batched.csv")
+        t0 = time.perf_counter()
+        b.run(jobs)
+        wall = time.perf_counter() - t0
+        clk = clocks.stop()
+    lat = np.array([j.t_end - j.t_submit for j in jobs])
+    sides = np.array([w.nx for w in wls])
+    value = node_steps / wall
+    line = {
+        "metric": "node-steps/s, 256 uneven single-flow grids run concurrently (FP64)",
+        "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.job_steps, "warmup": args.warmup,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"uneven_d8 x{len(wls)} (sides {sides.min()}..{sides.max()}, "
+                               f"{args.job_steps} steps each, bc=1111, p=-2, per-grid kf,m,n,kd,U)",
+                   "grids": len(wls), "total_nodes": int(sum(w.nn for w in wls)),
+                   "workers": args.workers, "order": "largest first",
+                   "timing": "host wall clock, first submit to last result",
+                   "l2": "working set >> 126 MB L2"},
+        "e2e": {"value": value, "unit": UNIT,
+                "h2d_bytes_per_step": int(sum(4 * 8 * w.nn for w in wls)) // args.job_steps,
+                "d2h_bytes_per_step": int(sum(8 * w.nn for w in wls)) // args.job_steps},
+        "job_latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "clocks": clk, "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_served(args):
+    import threading
+
+    import numpy as np
+    import torch
+    import fastscapelib_fortran as fs
+    from fastscapelib_fortran import workloads as W
+
+    torch.cuda.set_device(0)
+    scale = args.step_scale
+    steps = (max(1, int(round(20 * scale))), max(1, int(round(400 * scale))))
+
+    def requests(seed):
+        return W.served_mfd(args.requests, seed=seed, hi=args.max_side, steps=steps)
+
+    def serve(b, reqs, rate, rng):
+        """Submits at Poisson arrival times; returns (latencies, node-steps/s)."""
+        gaps = rng.exponential(1.0 / rate, len(reqs)) if rate > 0 else np.zeros(len(reqs))
+        arrivals = np.cumsum(gaps) - gaps[0]
+        ids = [None] * len(reqs)
+        jobs = [r.job() for r in reqs]
+        t0 = time.perf_counter()
+
+        def submitter():
+            for k, job in enumerate(jobs):
+                dt = t0 + arrivals[k] - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                ids[k] = b.submit(job)
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        for jid in ids:
+            b.wait(jid)
+        span = max(j.t_end for j in jobs) - min(j.t_submit for j in jobs)
+        lat = np.array([j.t_end - j.t_submit for j in jobs])
+        return lat, sum(r.nn * r.nsteps for r in reqs) / span
+
+    levels = []
+    with fs.Batch(workers=args.workers, mem_budget=int(args.mem_budget)) as b:
+        b.run([w.job() for w in W.served_mfd(args.workers, seed=999, hi=513, steps=(2, 2))])
+        # capacity: all requests of a probe set at once
+        probe = requests(777)
+        lat, thr = serve(b, probe, 0.0, np.random.default_rng(0))
+        work = np.mean([r.nn * r.nsteps for r in probe])
+        mu = thr / work  # requests per second the GPU completes when saturated
+        clocks = ClockSampler(0, os.path.join(ROOT, "gpurun_out", "clocks_served.csv")
+                              if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp/clocks_served.csv")
+        for lv, frac in enumerate((0.2, 0.4, 0.6, 0.8, 0.95)):
+            rate = frac * mu
+            lat, thr = serve(b, requests(1000 + lv), rate, np.random.default_rng(lv))
+            levels.append({"rate_per_s": rate, "load": frac, "requests": len(lat),
+                           "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                           "node_steps_per_s": thr})
+        clk = clocks.stop()
+    top = levels[-1]
+    line = {
+        "metric": "served multiple-flow requests: p50/p99 latency (s) and node-steps/s (FP64)",
+        "value": top["node_steps_per_s"], "unit": UNIT, "n_gpus": 1, "steps": None,
+        "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"served_mfd: sides 257..{args.max_side}, steps {steps[0]}..{steps[1]}, "
+                               f"{args.requests} Poisson requests per rate, rates = "
+                               f"(0.2..0.95) x saturated capacity {mu:.3f}/s",
+                   "workers": args.workers, "mem_budget": args.mem_budget,
+                   "timing": "host wall clock from each arrival to its result"},
+        "e2e": {"value": top["node_steps_per_s"], "unit": UNIT, "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": None},
+        "capacity_req_per_s": mu, "levels": levels, "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.workload == "batched":
+        run_batched(args)
+    elif args.workload == "served":
+        run_served(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <mutex>
 
 #include "fsb_kernels.cuh"
 #include "../../include/fastscape_b200.h"
@@ -22,6 +23,30 @@ struct fsb_ctx {
 };
 
 namespace {
+
+// Small pinned host buffers (counter read-backs) are recycled across
+// instances instead of freed: freeing pinned memory synchronises the device,
+// which would stall the other instances' streams.
+std::mutex g_pinned_mu;
+std::vector<int*> g_pinned_free;
+
+int* pinned_counters() {
+  std::lock_guard<std::mutex> lk(g_pinned_mu);
+  if (g_pinned_free.empty()) {
+    const int kBuffers = 64;
+    int* block = nullptr;
+    if (cudaMallocHost((void**)&block, sizeof(int) * 32 * kBuffers) != cudaSuccess) return nullptr;
+    for (int k = kBuffers - 1; k >= 0; --k) g_pinned_free.push_back(block + 32 * k);
+  }
+  int* p = g_pinned_free.back();
+  g_pinned_free.pop_back();
+  return p;
+}
+
+void recycle_counters(int* p) {
+  std::lock_guard<std::mutex> lk(g_pinned_mu);
+  g_pinned_free.push_back(p);
+}
 
 thread_local std::string g_err;
 
@@ -310,7 +335,7 @@ static void release(fsb::Ctx& c) {
     c.ev_pending[s] = false;
   }
   if (c.owns_arena && c.arena) cudaFree(c.arena);
-  if (c.h_cnt) cudaFreeHost(c.h_cnt);
+  if (c.h_cnt) recycle_counters(c.h_cnt);
   c.arena = nullptr;
   c.h_cnt = nullptr;
   c.owns_arena = false;
@@ -371,7 +396,8 @@ int fsb_setup(fsb_ctx* h, void* arena, size_t bytes) {
   layout(c, c.arena);
   // zero the whole arena once so that no index array ever holds garbage
   FSB_CUDA(cudaMemsetAsync(c.arena, 0, need, c.stream));
-  FSB_CUDA(cudaMallocHost((void**)&c.h_cnt, sizeof(int) * 32));
+  c.h_cnt = pinned_counters();
+  if (!c.h_cnt) return fail("pinned host memory for the counters could not be allocated");
   // defaults of SetUp
   decode_bc(c, 1111);
   std::vector<double> hv(c.nn);

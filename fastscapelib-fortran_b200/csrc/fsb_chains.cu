@@ -265,6 +265,10 @@ __global__ void __launch_bounds__(128) k_fill_chains(ChainView cv, const int* __
 // Bottom-up single-flow area: a(k) = dx*dy*precip(k) + a(d_m) + ... + a(d_1)
 // (donors descending, the reverse-stack order of FlowRouting.f90:136-139);
 // roots add themselves.  Only the chain head is read by another chain.
+// Each chunk first lists its light donors (heads of other chains), reads all
+// their done flags at once, fences once and reads all their areas at once;
+// the chain recurrence then runs in registers in the original summation order.
+constexpr int kLight = 16;  // light donors fetched together per chunk
 __global__ void __launch_bounds__(128) k_area_chains(ChainView cv, const int* __restrict__ rec,
                                                      const int* __restrict__ ndon, const int* __restrict__ don,
                                                      const double* __restrict__ precip, double dxdy,
@@ -296,6 +300,28 @@ __global__ void __launch_bounds__(128) k_area_chains(ChainView cv, const int* __
         base[i] = dxdy * precip[kk[i]];
         if (rec[kk[i]] == kk[i]) nd[i] |= 1 << 8;
       }
+      // light donors of the chunk in processing order (i descending, q descending);
+      // the heavy child of kk[i] is the next node down the chain
+      int lid[kLight];
+      double lv[kLight];
+      int nl = 0;
+      for (int i = n - 1; i >= 0; --i) {
+        const int k = kk[i];
+        const int heavy = i + 1 < n ? kk[i + 1] : child;
+        for (int q = (nd[i] & 255) - 1; q >= 0; --q) {
+          const int d = don[(size_t)k * 8 + q];
+          if (d != heavy && nl < kLight) lid[nl++] = d;
+        }
+      }
+      if (nl) {
+        bool ready = true;
+        for (int j = 0; j < nl; ++j) ready &= *(volatile unsigned*)&done[lid[j]] == epoch;
+        if (!ready)
+          for (int j = 0; j < nl; ++j) wait_flag(done, lid[j], epoch, err);
+        fence_acq_rel();
+        for (int j = 0; j < nl; ++j) lv[j] = __ldcg(&a[lid[j]]);
+      }
+      int jl = 0;
 #pragma unroll
       for (int i = kCF - 1; i >= 0; --i) if (i < n) {
         const int k = kk[i];
@@ -305,7 +331,8 @@ __global__ void __launch_bounds__(128) k_area_chains(ChainView cv, const int* __
           const int d = don[(size_t)k * 8 + q];
           double v;
           if (d == child) v = ac;
-          else {
+          else if (jl < kLight) v = lv[jl++];
+          else {  // more light donors than one fetch holds: read this one on its own
             wait_flag(done, d, epoch, err);
             v = __ldcg(&a[d]);
           }
@@ -495,12 +522,23 @@ static void next_epoch(Ctx& c) {
   cudaMemsetAsync(c.ticket, 0, sizeof(unsigned), c.stream);
 }
 
-static const int kChainBlocks = 148 * 8;
+// Persistent chain sweeps: up to 8 blocks per SM, and one block per 4096
+// tickets below that.  Most chains of a sweep wait for others, so a few
+// threads per thousand chains keep the critical path busy (at 2049^2 the
+// sweeps take the same time as with one thread per chain), and the sweeps of
+// small and mid-size grids leave the GPU to other streams.
+#ifndef FSB_CHAIN_TICKETS_PER_BLOCK
+#define FSB_CHAIN_TICKETS_PER_BLOCK 4096
+#endif
+static int chain_blocks(int ntickets) {
+  const int want = (ntickets + FSB_CHAIN_TICKETS_PER_BLOCK - 1) / FSB_CHAIN_TICKETS_PER_BLOCK;
+  return want < 1 ? 1 : (want > 148 * 8 ? 148 * 8 : want);
+}
 
 void fill_chains(Ctx& c) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_td, c.nchains, c.ntickets_td, c.nn};
-  k_fill_chains<<<kChainBlocks, 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.h, c.hwater, c.lake_depth, c.ticket,
+  k_fill_chains<<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.h, c.hwater, c.lake_depth, c.ticket,
                                                     c.done, c.epoch, c.d_err);
   c.count_launch();
 }
@@ -508,7 +546,7 @@ void fill_chains(Ctx& c) {
 void area_chains(Ctx& c) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_bu, c.nchains, c.ntickets_bu, c.nn};
-  k_area_chains<<<kChainBlocks, 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, c.precip, c.dx * c.dy, c.a, c.ticket,
+  k_area_chains<<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, c.precip, c.dx * c.dy, c.a, c.ticket,
                                                     c.done, c.epoch, c.d_err);
   c.count_launch();
 }
@@ -517,7 +555,7 @@ void spl_chains(Ctx& c, double* hnew) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_td, c.nchains, c.ntickets_td, c.nn};
   const int n1 = fabs(c.n - 1.0) < 2.2250738585072014e-308;
-  k_spl_chains<<<kChainBlocks, 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.h, c.b, c.kf, c.a, c.length, c.kfsed, c.dt,
+  k_spl_chains<<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.h, c.b, c.kf, c.a, c.length, c.kfsed, c.dt,
                                                    c.m, c.n, 0.875 / c.n, n1, hnew, c.water, c.ticket, c.done,
                                                    c.epoch, c.d_err);
   c.count_launch();

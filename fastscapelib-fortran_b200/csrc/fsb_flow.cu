@@ -15,6 +15,7 @@
 // has not been scheduled, so the sweep needs no global order and cannot
 // deadlock; the counters' acquire/release ordering makes every dependency's
 // value visible before it is read.
+#include <algorithm>
 #include <cuda/atomic>
 #include <cfloat>
 
@@ -863,7 +864,10 @@ static void run_sweep(Ctx& c, Op op, const int* cnt0) {
   cudaMemsetAsync(c.la_queue, 0xff, sizeof(int) * nn, c.stream);
   cudaMemsetAsync(c.la_ctl, 0, sizeof(unsigned) * 128, c.stream);
   k_seed_queue<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, cnt0, c.la_queue, c.la_ctl + 32);
-  k_last_arriver<Op, LANES><<<148 * 4, 128, 0, c.stream>>>(op, nn, c.la_cnt, c.la_queue, c.la_ctl, c.d_err);
+  // 4 blocks per SM (register bound) on large grids; small grids take about
+  // one block per 1024 nodes and leave the rest of the GPU to other streams
+  const int blocks = std::max(8, std::min(148 * 4, nn / 1024));
+  k_last_arriver<Op, LANES><<<blocks, 128, 0, c.stream>>>(op, nn, c.la_cnt, c.la_queue, c.la_ctl, c.d_err);
   c.count_launch(2);
 }
 

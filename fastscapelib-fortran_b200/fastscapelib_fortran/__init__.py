@@ -26,6 +26,12 @@ from __future__ import annotations
 import ctypes
 import os
 
+# Batches run one CUDA stream per worker; the driver maps streams onto this
+# many hardware work queues (default 8), so more queues keep the workers'
+# kernels from waiting on each other.  Read when the CUDA context is created,
+# i.e. effective when this package is imported before CUDA is first used.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 import numpy as np
 
 try:
@@ -90,6 +96,14 @@ _sig("fsb_synchronize", _vp)
 _sig("fsb_launch_count", _vp, res=ctypes.c_longlong)
 _sig("fsb_set_profile", _vp, _i)
 _sig("fsb_stage_times", _vp, _vp, _vp, _i, _i)
+
+_sig("fsb_batch_create", ctypes.POINTER(_vp), _i, _i, ctypes.c_size_t)
+_sig("fsb_batch_submit", _vp, _vp, ctypes.POINTER(ctypes.c_longlong))
+_sig("fsb_batch_wait", _vp, ctypes.c_longlong, ctypes.POINTER(_i), _vp)
+_sig("fsb_batch_run", _vp, _vp, _i, _vp, _vp)
+_sig("fsb_batch_memory", _vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t),
+     ctypes.POINTER(_i), ctypes.POINTER(_i))
+_sig("fsb_batch_destroy", _vp)
 
 STAGES = ("uplift", "receivers", "stack", "local_minima", "lake_fill", "mfd_receivers",
           "drainage_area", "stream_power", "diffusion")
@@ -313,6 +327,140 @@ class FastScape:
 
 
 # ---------------------------------------------------------------------------
+# Many grids on one device
+
+class _JobRow(ctypes.Structure):
+    """fsb_job of include/fastscape_b200.h."""
+    _fields_ = [("nx", _i), ("ny", _i), ("bc", _i), ("nsteps", _i),
+                ("xl", _d), ("yl", _d), ("dt", _d),
+                ("kfsed", _d), ("m", _d), ("n", _d), ("kdsed", _d), ("g1", _d), ("g2", _d),
+                ("p", _d),
+                ("kf", _vp), ("kd", _vp), ("u", _vp), ("h0", _vp), ("precip", _vp),
+                ("h_out", _vp), ("a_out", _vp), ("etot_out", _vp)]
+
+
+def _f64(a, nn, name):
+    a = np.ascontiguousarray(np.broadcast_to(np.asarray(a, dtype=np.float64), (nn,))
+                             if np.ndim(a) == 0 else np.asarray(a, dtype=np.float64).reshape(-1))
+    if a.size != nn:
+        raise ValueError(f"{name} has {a.size} values, the grid has {nn} nodes")
+    return np.ascontiguousarray(a)
+
+
+class Job:
+    """One grid of a batch: the sequence init / set_nx_ny / setup / set_xl_yl /
+    set_dt / init_h / set_erosional_parameters / set_u / set_precip / set_bc /
+    ``nsteps`` x execute_step / copy_h of the reference's API, as one unit of
+    work.  Arrays are float64 with nx*ny values (scalars are broadcast).
+    After the batch has run it, ``h`` (and ``a`` / ``etot`` when asked for)
+    hold the results and ``t_submit``, ``t_start``, ``t_end`` its times."""
+
+    def __init__(self, nx, ny, xl, yl, dt, h0, kf, kd, u, m, n, p, bc=1111, nsteps=1,
+                 kfsed=-1.0, kdsed=-1.0, g1=0.0, g2=0.0, precip=None, want_area=False,
+                 want_etot=False):
+        nn = int(nx) * int(ny)
+        self.nx, self.ny, self.nsteps, self.bc = int(nx), int(ny), int(nsteps), int(bc)
+        self.xl, self.yl, self.dt = float(xl), float(yl), float(dt)
+        self.m, self.n, self.p = float(m), float(n), float(p)
+        self.kfsed, self.kdsed, self.g1, self.g2 = float(kfsed), float(kdsed), float(g1), float(g2)
+        self.h0 = _f64(h0, nn, "h0")
+        self.kf = _f64(kf, nn, "kf")
+        self.kd = _f64(kd, nn, "kd")
+        self.u = _f64(u, nn, "u")
+        self.precip = None if precip is None else _f64(precip, nn, "precip")
+        self.h = np.empty(nn)
+        self.a = np.empty(nn) if want_area else None
+        self.etot = np.empty(nn) if want_etot else None
+        self.t_submit = self.t_start = self.t_end = float("nan")
+        self.status = None
+
+    @property
+    def nn(self) -> int:
+        return self.nx * self.ny
+
+    def _row(self) -> _JobRow:
+        ptr = lambda a: None if a is None else a.ctypes.data  # noqa: E731
+        return _JobRow(self.nx, self.ny, self.bc, self.nsteps, self.xl, self.yl, self.dt,
+                       self.kfsed, self.m, self.n, self.kdsed, self.g1, self.g2, self.p,
+                       ptr(self.kf), ptr(self.kd), ptr(self.u), ptr(self.h0), ptr(self.precip),
+                       ptr(self.h), ptr(self.a), ptr(self.etot))
+
+
+class Batch:
+    """Runs Jobs concurrently on one CUDA device (``fsb_batch_*``): ``workers``
+    threads with one stream each, admission by device memory within
+    ``mem_budget`` bytes (0: 90% of the free memory), jobs started in
+    submission order.  ``submit`` returns at once; ``wait`` blocks (without
+    the GIL) until that job is done; ``run`` does both for a list."""
+
+    def __init__(self, workers: int = 32, mem_budget: int = 0, device: int | None = None):
+        dev = torch.cuda.current_device() if device is None else int(device)
+        b = _vp()
+        _check(_lib.fsb_batch_create(ctypes.byref(b), dev, int(workers), int(mem_budget)))
+        self._b = b
+        self._jobs: dict[int, Job] = {}
+
+    def submit(self, job: Job) -> int:
+        jid = ctypes.c_longlong()
+        _check(_lib.fsb_batch_submit(self._b, ctypes.byref(job._row()), ctypes.byref(jid)))
+        job.t_submit = float("nan")
+        self._jobs[jid.value] = job
+        return jid.value
+
+    def wait(self, jid: int) -> Job:
+        job = self._jobs.pop(jid)
+        st = _i()
+        t = np.zeros(3)
+        rc = _lib.fsb_batch_wait(self._b, jid, ctypes.byref(st), t.ctypes.data)
+        job.status = st.value
+        job.t_submit, job.t_start, job.t_end = (float(x) for x in t)
+        _check(rc)
+        return job
+
+    def run(self, jobs) -> list:
+        ids = [self.submit(j) for j in jobs]
+        errors = []
+        for jid in ids:
+            try:
+                self.wait(jid)
+            except RuntimeError as exc:
+                errors.append(str(exc))
+        if errors:
+            raise RuntimeError(errors[0])
+        return list(jobs)
+
+    def memory(self) -> dict:
+        used, budget = ctypes.c_size_t(), ctypes.c_size_t()
+        running, pending = _i(), _i()
+        _check(_lib.fsb_batch_memory(self._b, ctypes.byref(used), ctypes.byref(budget),
+                                     ctypes.byref(running), ctypes.byref(pending)))
+        return {"in_use": used.value, "budget": budget.value, "running": running.value,
+                "pending": pending.value}
+
+    def close(self) -> None:
+        if getattr(self, "_b", None):
+            for jid in list(self._jobs):
+                try:
+                    self.wait(jid)
+                except RuntimeError:
+                    pass
+            _lib.fsb_batch_destroy(self._b)
+            self._b = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
 # Module-level API of the reference (one default instance per process)
 _default: FastScape | None = None
 
@@ -422,4 +570,4 @@ def fastscape_copy_lake_depth(lp):
     _inst().copy("lake_depth", lp)
 
 
-__all__ = [n for n in dir() if n.startswith("fastscape_")] + ["FastScape", "LIB_PATH"]
+__all__ = [n for n in dir() if n.startswith("fastscape_")] + ["FastScape", "Job", "Batch", "LIB_PATH"]

@@ -11,6 +11,12 @@ shapes, sizes and value distributions of the benchmark configurations:
   kd=5e-2, dt=500, 500 steps.
 * ``closed_basin_8193``: 8193x8193, 50 m spacing, h~U[0,50), bc=0101
   (y cyclic), p=1, kf=1e-5, m=0.5, n=1, kd=1e-2, dt=200, 50 steps.
+* ``uneven_d8`` (many grids at once): 256 square grids with sides drawn
+  log-uniform in [129, 1025] (odd), 100 m spacing, per grid kf~logU[1e-6,1e-4],
+  m~U[0.35,0.6], n~U[1,2], kd~logU[1e-3,1e-1], interior uplift U[1e-4,2e-3],
+  h~U[0,1), bc=1111, single flow direction, dt=1000, 100 steps.
+* ``served_mfd`` (requests): sides log-uniform in [257, 4097] (odd), steps
+  uniform in 20..400, the parameters of ``mfd_2049``, each from its own seed.
 
 Arrays are float64 in the reference layout ij = i + (j-1)*nx (x fastest),
 i.e. numpy ``reshape(ny, nx)``.  Any side length can be substituted to get a
@@ -49,6 +55,13 @@ class Workload:
     @property
     def nn(self) -> int:
         return self.nx * self.ny
+
+    def job(self, **kw):
+        """This workload as a batch Job (fastscapelib_fortran.Job)."""
+        from . import Job
+        return Job(self.nx, self.ny, self.xl, self.yl, self.dt, self.h0, self.kf, self.kd, self.u,
+                   self.m, self.n, self.p, bc=self.bc, nsteps=self.nsteps, kfsed=self.kfsed,
+                   kdsed=self.kdsed, g1=self.g1, g2=self.g2, **kw)
 
     def apply(self, api) -> None:
         """Drive a fastscape_* API module (reference-shaped) through set-up."""
@@ -106,3 +119,44 @@ def closed_basin(nx: int = 8193, ny: int | None = None, seed: int = 12345,
     return Workload("closed_basin_%dx%d" % (nx, ny), nx, ny, 50.0 * (nx - 1), 50.0 * (ny - 1),
                     200.0, 101, np.full(nn, 1.0e-5), -1.0, 0.5, 1.0, np.full(nn, 1.0e-2), -1.0,
                     0.0, 0.0, 1.0, _interior(nx, ny, 5.0e-4), h0, nsteps)
+
+
+def _odd_side(rng, lo: int, hi: int) -> int:
+    s = int(round(float(np.exp(rng.uniform(np.log(lo), np.log(hi))))))
+    s += 1 - s % 2
+    return max(lo, min(hi, s))
+
+
+def uneven_d8(count: int = 256, seed: int = 12345, nsteps: int = 100, lo: int = 129,
+              hi: int = 1025) -> list:
+    """Many uneven single-flow grids (per-grid parameters drawn from `seed`,
+    initial elevation of grid k from seed + k)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        nx = _odd_side(rng, lo, hi)
+        kf = 10.0 ** rng.uniform(-6.0, -4.0)
+        m = rng.uniform(0.35, 0.6)
+        n = rng.uniform(1.0, 2.0)
+        kd = 10.0 ** rng.uniform(-3.0, -1.0)
+        up = rng.uniform(1.0e-4, 2.0e-3)
+        nn = nx * nx
+        h0 = np.random.default_rng(seed + k).random(nn)
+        out.append(Workload("uneven_d8_%d_%dx%d" % (k, nx, nx), nx, nx, 100.0 * (nx - 1),
+                            100.0 * (nx - 1), 1.0e3, 1111, np.full(nn, kf), -1.0, m, n,
+                            np.full(nn, kd), -1.0, 0.0, 0.0, -2.0, _interior(nx, nx, up), h0,
+                            nsteps))
+    return out
+
+
+def served_mfd(count: int, seed: int = 12345, lo: int = 257, hi: int = 4097,
+               steps: tuple = (20, 400)) -> list:
+    """Requests of the served configuration: multiple-flow grids with the
+    parameters of ``mfd``, uneven sizes and step counts."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        nx = _odd_side(rng, lo, hi)
+        ns = int(rng.integers(steps[0], steps[1] + 1))
+        out.append(mfd(nx, seed=seed + 1 + k, nsteps=ns))
+    return out

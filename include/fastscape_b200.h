@@ -164,6 +164,52 @@ int fsb_diffusion_step_noalloc(int nx, int ny, double xl, double yl, double dt, 
                                const double* kd, double* h, double* b, double* etot, double* erate,
                                void* stream);
 
+/* ---- many grids on one device ----
+   No counterpart in the reference, which holds one grid per process
+   (src/FastScape_ctx.f90:9-36).  A batch runs jobs -- a grid, its parameters
+   and a number of continental steps, each the sequence FastScape_Init /
+   Set_NX_NY / Setup / Set_XL_YL / Set_DT / Init_H / Set_Erosional_Parameters /
+   Set_U / Set_Precip / Set_BC / Execute_Step x nsteps / Copy_H / Destroy of
+   src/FastScape_api.f90 -- on worker threads with one CUDA stream each, so
+   that jobs overlap on the GPU.  A job starts when its device workspace fits
+   within the batch's memory budget beside the running jobs; jobs start in
+   submission order.  Results do not depend on what else runs. */
+typedef struct fsb_batch fsb_batch;
+typedef struct fsb_job {
+  int nx, ny;            /* grid size                                  api:475 */
+  int bc;                /* boundary code                              api:602 */
+  int nsteps;            /* continental steps to run                   api:201 */
+  double xl, yl;         /* domain size                                api:491 */
+  double dt;             /* time step                                  api:507 */
+  double kfsed, m, n, kdsed, g1, g2, p;  /* erosional scalars          api:523 */
+  const double* kf;      /* [nx*ny] host arrays                        api:523 */
+  const double* kd;      /* [nx*ny]                                    api:523 */
+  const double* u;       /* [nx*ny] uplift rate                        api:618 */
+  const double* h0;      /* [nx*ny] initial elevation                  api:267 */
+  const double* precip;  /* [nx*ny] or NULL for 1                      api:712 */
+  double* h_out;         /* [nx*ny] elevation after nsteps, or NULL    api:299 */
+  double* a_out;         /* [nx*ny] drainage area, or NULL             api:347 */
+  double* etot_out;      /* [nx*ny] total erosion, or NULL             api:331 */
+} fsb_job;
+/* `workers` threads (1..256) on CUDA device `device`; `mem_budget` bytes of
+   device memory for job workspaces (0: 90% of the memory free now). */
+int fsb_batch_create(fsb_batch** out, int device, int workers, size_t mem_budget);
+/* Queues a job; the arrays it points to must stay valid until it is waited
+   for.  A job whose workspace exceeds the whole budget is refused. */
+int fsb_batch_submit(fsb_batch* b, const fsb_job* job, long long* id);
+/* Blocks until job `id` has finished and forgets it; `status` receives 0 or
+   the job's error code (whose message fsb_last_error then returns) and
+   `times` (may be NULL) its submit, start and end times in seconds on one
+   monotonic clock. */
+int fsb_batch_wait(fsb_batch* b, long long id, int* status, double* times);
+/* Submits `njobs` jobs and waits for all of them; status[k] and
+   times[3k..3k+2] as fsb_batch_wait (either may be NULL). */
+int fsb_batch_run(fsb_batch* b, const fsb_job* jobs, int njobs, int* status, double* times);
+/* Device bytes held by running jobs, the budget, running and queued jobs. */
+int fsb_batch_memory(fsb_batch* b, size_t* in_use, size_t* budget, int* running, int* pending);
+/* Waits for every submitted job, then stops the workers and frees the batch. */
+int fsb_batch_destroy(fsb_batch* b);
+
 /* ---- the reference's Fortran entry points (src/FastScape_api.f90) ---- */
 void fastscape_init_(void);                                        /* api:146 */
 void fastscape_setup_(void);                                       /* api:160 */
