@@ -42,7 +42,8 @@ struct Loc {
 // Op::run(k, dep[], pr[], loc) computes node k, stores its outputs and lists
 // k's dependents with their priorities; the engine then decrements their
 // counters, continues with the ready dependent of largest priority (subtree
-// size) and queues the other ready ones.  Idle lanes claim queue slots in
+// size), prefetching its record (Op::prefetch), and queues the other ready
+// ones.  Idle lanes claim queue slots in
 // order (one atomic per warp) and keep a claim until a producer fills it.
 // The kernel ends when every node is done.
 // Control words: ctl[0] queue head, ctl[32] queue tail, ctl[64] nodes done
@@ -102,8 +103,8 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, i
       const int nd = op.run(cur, dep, pr, Loc{});
       int nxt = -1;
       if (nd) {
-        fence_acq_rel();  // release the node's outputs before its dependents' counters drop
         int old[8];
+        fence_acq_rel();  // release the node's outputs before its dependents' counters drop
 #pragma unroll
         for (int t = 0; t < 8; ++t) old[t] = t < nd ? atomicSub(&cnt[dep[t]], 1) : 0;
         unsigned bp = 0;
@@ -115,6 +116,7 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, i
             if (bi < 0 || pr[t] > bp) { bp = pr[t]; bi = t; nxt = dep[t]; }
           }
         if (bi >= 0) rdy &= ~(1u << bi);
+        if (nxt >= 0) op.prefetch(nxt);  // the continuation's record line into L1
       }
       ++local_done;
       cur = nxt;
@@ -277,6 +279,7 @@ struct AccMfdOp {
   const AccLine* line;
   int nx, ny;
   double* a;
+  __device__ void prefetch(int k) const { prefetch_l1(line + k); }
   __device__ int run(int k, int* dep, unsigned* pr, const Loc& loc) const {
     const LineWords<6> L(line + k);  // aw[0..7] = d[0..7], base = d[8], don = u[18], rcv = u[19], pr = s[40..47]
     const NbrDecoder nb(k, nx, ny);
@@ -294,7 +297,6 @@ struct AccMfdOp {
       if (c) {
         dep[t] = nb.at(c);
         pr[t] = L.s[40 + t];
-        prefetch_l1(line + dep[t]);  // the receivers come next, usually in this thread
         nd = t + 1;
       }
     }
@@ -313,6 +315,7 @@ struct AccMfdOp {
 struct SplMfdOp {
   const SplLine* line;
   int nx, ny;
+  __device__ void prefetch(int k) const { prefetch_l1(line + k); }
   NewtonPow np;
   double omega;
   int n_is_one;
@@ -330,7 +333,6 @@ struct SplMfdOp {
       if (c) {
         dep[t] = nb.at(c);
         pr[t] = L.s[40 + t];
-        prefetch_l1(line + dep[t]);  // the donors come next, usually in this thread
         nd = t + 1;
       }
     }
