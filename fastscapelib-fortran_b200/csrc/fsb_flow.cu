@@ -16,6 +16,7 @@
 // deadlock; the counters' acquire/release ordering makes every dependency's
 // value visible before it is read.
 #include <algorithm>
+#include <cmath>
 #include <cuda/atomic>
 #include <cfloat>
 
@@ -60,15 +61,19 @@ struct Loc {
 #ifndef FSB_LANES_SPL
 #define FSB_LANES_SPL 1
 #endif
-// Grid of a sweep: one block per NODES_PER_BLOCK nodes, 8 to 592 blocks.
-// Idle lanes poll the work queue, so more blocks than the critical path can
-// use slow it down: at 2049^2 256 blocks beat 592 (stream power 35.4 against
-// 40.1 ms, area unchanged), and smaller grids leave SMs to other streams.
-#ifndef FSB_NPB_ACC
-#define FSB_NPB_ACC 16384
+// Grid of a sweep: sqrt(nn)/SIDE_DIV blocks, 8 to 592 (4 per SM).  The
+// sweeps are bound by their critical path, whose length grows with the grid
+// side, and the nodes in flight it needs grow with the side too; idle lanes
+// poll the work queue, so more blocks than that slow a sweep down.  Measured
+// on B200 (area with side/4, stream power with side/8): 513^2 17 ms/step
+// against 32 with one block per 16384 nodes; 2049^2 unchanged (256 blocks
+// for stream power beat 592: 35 against 40 ms).  Smaller grids leave the
+// rest of the GPU to other streams.
+#ifndef FSB_SIDE_DIV_ACC
+#define FSB_SIDE_DIV_ACC 4
 #endif
-#ifndef FSB_NPB_SPL
-#define FSB_NPB_SPL 16384
+#ifndef FSB_SIDE_DIV_SPL
+#define FSB_SIDE_DIV_SPL 8
 #endif
 template <class Op, int LANES>
 __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, int* queue, unsigned* ctl, int* err) {
@@ -869,14 +874,14 @@ void mfd_receivers(Ctx& c) {
   }
 }
 
-template <int LANES, int NODES_PER_BLOCK, class Op>
+template <int LANES, int SIDE_DIV, class Op>
 static void run_sweep(Ctx& c, Op op, const int* cnt0) {
   const int nn = c.nn;
   cudaMemcpyAsync(c.la_cnt, cnt0, sizeof(int) * nn, cudaMemcpyDeviceToDevice, c.stream);
   cudaMemsetAsync(c.la_queue, 0xff, sizeof(int) * nn, c.stream);
   cudaMemsetAsync(c.la_ctl, 0, sizeof(unsigned) * 128, c.stream);
   k_seed_queue<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, cnt0, c.la_queue, c.la_ctl + 32);
-  const int blocks = std::max(8, std::min(148 * 4, nn / NODES_PER_BLOCK));
+  const int blocks = std::max(8, std::min(148 * 4, (int)std::sqrt((double)nn) / SIDE_DIV));
   k_last_arriver<Op, LANES><<<blocks, 128, 0, c.stream>>>(op, nn, c.la_cnt, c.la_queue, c.la_ctl, c.d_err);
   c.count_launch(2);
 }
@@ -892,7 +897,7 @@ void accumulate(Ctx& c) {
   k_acc_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, c.dx * c.dy, c.mrec, c.mnrec, c.mwrec, c.precip, c.size,
                                                      line, c.cnt_acc, c.d_err);
   c.count_launch();
-  run_sweep<FSB_LANES_ACC, FSB_NPB_ACC>(c, AccMfdOp{line, c.nx, c.ny, c.a}, c.cnt_acc);
+  run_sweep<FSB_LANES_ACC, FSB_SIDE_DIV_ACC>(c, AccMfdOp{line, c.nx, c.ny, c.a}, c.cnt_acc);
 }
 
 void stream_power(Ctx& c) {
@@ -910,7 +915,7 @@ void stream_power(Ctx& c) {
                                                      c.mlrec, c.h, c.b, c.kf, c.a, c.size, line, c.cnt_spl, c.d_err);
   c.count_launch();
   double2* hw = reinterpret_cast<double2*>(c.hw);
-  run_sweep<FSB_LANES_SPL, FSB_NPB_SPL>(c, SplMfdOp{line, c.nx, c.ny, NewtonPow{c.n, c.n == 1.5}, omega, n1, hw}, c.cnt_spl);
+  run_sweep<FSB_LANES_SPL, FSB_SIDE_DIV_SPL>(c, SplMfdOp{line, c.nx, c.ny, NewtonPow{c.n, c.n == 1.5}, omega, n1, hw}, c.cnt_spl);
   k_spl_finish<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nn, c.dt, c.hw, 2, c.h, c.b, c.etot, c.erate, c.sedflux);
   c.count_launch();
 }
