@@ -158,6 +158,7 @@ size_t layout(fsb::Ctx& c, char* base) {
   c.s_scan2 = L.take<int>(N + 1);
   c.done = L.take<unsigned>(N); c.ticket = L.take<unsigned>(4);
   c.water = L.take<double>(N); c.hnew = L.take<double>(N);
+  c.catch0 = L.take<double>(N); c.catchv = L.take<double>(N); c.red = L.take<double>(3 * 512 + 8);
   c.dK = L.take<double>(N); c.dA = L.take<double>(N); c.dB = L.take<double>(N); c.dC = L.take<double>(N);
   c.dF = L.take<double>(N); c.dG = L.take<double>(N); c.dZ = L.take<double>(N);
   c.d_err = L.take<int>(4); c.d_cnt = L.take<int>(32);
@@ -196,6 +197,7 @@ double* field_ptr(fsb::Ctx& c, int f) {
     case FSB_LENGTH: return c.length;
     case FSB_HWATER: return c.hwater;
     case FSB_SEDFLUX: return c.sedflux;
+    case FSB_CATCHMENT: return c.catchv;
     case FSB_U: return c.u;
     case FSB_PRECIP: return c.precip;
     case FSB_KF: return c.kf;
@@ -305,6 +307,7 @@ int step_once(fsb::Ctx& c) {
     stage_end(c, ST_DIFFUSION);
   }
   c.step += 1;
+  if (c.runSPL) c.routed = true;
   const int rc = check_device_error(c);
   collect_stage_times(c);
   return rc;
@@ -407,9 +410,13 @@ int fsb_setup(fsb_ctx* h, void* arena, size_t bytes) {
   for (int j = 0; j < c.ny; ++j) { hv[(size_t)j * c.nx] = 0.0; hv[(size_t)j * c.nx + c.nx - 1] = 0.0; }
   FSB_CUDA(cudaMemcpyAsync(c.h, hv.data(), sizeof(double) * c.nn, cudaMemcpyHostToDevice, c.stream));
   FSB_CUDA(cudaMemcpyAsync(c.b, hv.data(), sizeof(double) * c.nn, cudaMemcpyHostToDevice, c.stream));
+  // catch0 continues the same stream (SetUp's second random_number, ctx:94)
+  std::vector<double> cv(c.nn);
+  for (int i = 0; i < c.nn; ++i) cv[i] = xorshift_uniform(s);
+  FSB_CUDA(cudaMemcpyAsync(c.catch0, cv.data(), sizeof(double) * c.nn, cudaMemcpyHostToDevice, c.stream));
   std::vector<double> ones(c.nn, 1.0);
   FSB_CUDA(cudaMemcpyAsync(c.precip, ones.data(), sizeof(double) * c.nn, cudaMemcpyHostToDevice, c.stream));
-  for (double* f : {c.u, c.etot, c.erate, c.a, c.length, c.lake_depth, c.hwater, c.sedflux, c.kf, c.kd})
+  for (double* f : {c.u, c.etot, c.erate, c.a, c.length, c.lake_depth, c.hwater, c.sedflux, c.kf, c.kd, c.catchv})
     FSB_CUDA(cudaMemsetAsync(f, 0, sizeof(double) * c.nn, c.stream));
   FSB_CUDA(cudaMemsetAsync(c.done, 0, sizeof(unsigned) * c.nn, c.stream));
   FSB_CUDA(cudaMemsetAsync(c.s_flag, 0, sizeof(int) * (c.nn + 1), c.stream));
@@ -420,6 +427,7 @@ int fsb_setup(fsb_ctx* h, void* arena, size_t bytes) {
   c.sfd = false;
   c.p = 1.0;
   c.step = 0;
+  c.routed = false;
   c.setup_done = true;
   return 0;
 }
@@ -530,6 +538,144 @@ int fsb_copy_field(fsb_ctx* h, int field, double* dst, int where) {
   const cudaMemcpyKind kind = where == FSB_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   FSB_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * h->c.nn, kind, h->c.stream));
   if (where != FSB_DEVICE) FSB_CUDA(cudaStreamSynchronize(h->c.stream));
+  return 0;
+}
+
+static int copy_out(fsb::Ctx& c, const double* src, double* dst, int where) {
+  if (!dst) return fail("null destination");
+  const cudaMemcpyKind kind = where == FSB_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  FSB_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * c.nn, kind, c.stream));
+  FSB_CUDA(cudaStreamSynchronize(c.stream));
+  return check_device_error(c);
+}
+
+int fsb_copy_chi(fsb_ctx* h, double* dst, int where) {
+  if (need_setup(h, "CopyChi")) return 1;
+  fsb::Ctx& c = h->c;
+  double* chi = c.hnew;  // free between steps
+  if (!c.routed) {
+    FSB_CUDA(cudaMemsetAsync(chi, 0, sizeof(double) * c.nn, c.stream));
+  } else {
+    const double a0 = (c.xl / (c.nx - 1)) * (c.yl / (c.ny - 1)) * 10.0;
+    fsb::chi_chains(c, a0, c.m / c.n, chi);
+  }
+  return copy_out(c, chi, dst, where);
+}
+
+int fsb_copy_slope(fsb_ctx* h, double* dst, int where) {
+  if (need_setup(h, "CopySlope")) return 1;
+  fsb::slope_field(h->c, h->c.dK);
+  return copy_out(h->c, h->c.dK, dst, where);
+}
+
+int fsb_copy_curvature(fsb_ctx* h, double* dst, int where) {
+  if (need_setup(h, "CopyCurvature")) return 1;
+  fsb::curvature_field(h->c, h->c.dK);
+  return copy_out(h->c, h->c.dK, dst, where);
+}
+
+int fsb_get_fluxes(fsb_ctx* h, double* tectonic, double* erosion, double* boundary) {
+  if (need_setup(h, "GetFluxes")) return 1;
+  if (!tectonic || !erosion || !boundary) return fail("GetFluxes: null output");
+  fsb::Ctx& c = h->c;
+  double* flux = c.hnew;  // free between steps
+  if (!c.routed)          // no stack yet: the flux is erate itself
+    FSB_CUDA(cudaMemcpyAsync(flux, c.erate, sizeof(double) * c.nn, cudaMemcpyDeviceToDevice, c.stream));
+  else if (c.sfd)
+    fsb::flux_chains(c, flux);
+  else
+    fsb::flux_mfd(c, flux);
+  fsb::flux_sums(c, flux, c.red, c.red + 3 * 512);
+  double s3[3];
+  FSB_CUDA(cudaMemcpyAsync(s3, c.red + 3 * 512, sizeof s3, cudaMemcpyDeviceToHost, c.stream));
+  FSB_CUDA(cudaStreamSynchronize(c.stream));
+  if (check_device_error(c)) return 1;
+  const double surf = c.xl * c.yl / (c.nx - 1) / (c.ny - 1);
+  *tectonic = s3[0] * surf;
+  *erosion = s3[1] * surf;
+  *boundary = s3[2] * surf;
+  return 0;
+}
+
+int fsb_set_all_layers(fsb_ctx* h, const double* dh, int where) {
+  if (need_setup(h, "SetAllLayers")) return 1;
+  fsb::Ctx& c = h->c;
+  const double* src = dh;
+  if (where != FSB_DEVICE) {
+    if (upload(c, c.dK, dh, where)) return 1;
+    src = c.dK;
+  }
+  fsb::add_layers(c, src);
+  FSB_CUDA(cudaStreamSynchronize(c.stream));
+  return 0;
+}
+
+extern "C++" {
+namespace {
+template <class T>
+std::vector<T> to_host(fsb::Ctx& c, const T* src) {
+  std::vector<T> v(c.nn);
+  cudaMemcpyAsync(v.data(), src, sizeof(T) * c.nn, cudaMemcpyDeviceToHost, c.stream);
+  cudaStreamSynchronize(c.stream);
+  return v;
+}
+void min_mean_max(const std::vector<double>& v, double& lo, double& mean, double& hi) {
+  lo = hi = v.empty() ? 0.0 : v[0];
+  double s = 0.0;
+  for (double x : v) { lo = std::min(lo, x); hi = std::max(hi, x); s += x; }
+  mean = v.empty() ? 0.0 : s / v.size();
+}
+}  // namespace
+}  // extern "C++"
+
+int fsb_view(fsb_ctx* h) {
+  if (need_setup(h, "View")) return 1;
+  fsb::Ctx& c = h->c;
+  double lo, mean, hi, kfm, kdm;
+  min_mean_max(to_host(c, c.kf), lo, kfm, hi);
+  min_mean_max(to_host(c, c.kd), lo, kdm, hi);
+  std::printf(" FastScapeContext:\n");
+  std::printf(" nx,ny %d %d\n nn %d\n step %d\n", c.nx, c.ny, c.nn, c.step);
+  std::printf(" xl,yl %.15g %.15g\n dt %.15g\n", c.xl, c.yl, c.dt);
+  std::printf(" Kf,Kfsed,,m,n,Kd,Kdsed,G1,G2 %.15g %.15g %.15g %.15g %.15g %.15g %.15g %.15g\n", kfm, c.kfsed,
+              c.m, c.n, kdm, c.kdsed, c.g1, c.g2);
+  std::printf(" ibc %d\n", c.ibc);
+  min_mean_max(to_host(c, c.h), lo, mean, hi);
+  std::printf(" h %.15g %.15g %.15g\n", lo, mean, hi);
+  min_mean_max(to_host(c, c.u), lo, mean, hi);
+  std::printf(" u %.15g %.15g %.15g\n", lo, mean, hi);
+  std::fflush(stdout);
+  return 0;
+}
+
+int fsb_debug(fsb_ctx* h) {
+  if (need_setup(h, "Debug")) return 1;
+  fsb::Ctx& c = h->c;
+  const std::vector<int> rec = to_host(c, c.rec), ndon = to_host(c, c.ndon), stack = to_host(c, c.stack);
+  long long nil = 0, sdon = 0, self = 0, minima = 0;
+  std::vector<char> seen(c.nn, 0);
+  for (int k = 0; k < c.nn; ++k) {
+    if (stack[k] >= 0 && stack[k] < c.nn) seen[stack[k]] = 1;
+    sdon += ndon[k];
+    self += rec[k] == k;
+  }
+  for (int k = 0; k < c.nn; ++k) nil += !seen[k];  // nodes the stack misses
+  for (int j = c.bd.j1; j <= c.bd.j2; ++j)
+    for (int i = c.bd.i1; i <= c.bd.i2; ++i) minima += rec[(size_t)j * c.nx + i] == j * c.nx + i;
+  std::printf(" --------------------------------------------------------\n");
+  std::printf(" Time step %d\n Debug information\n", c.step);
+  std::printf(" Total number of nodes (nx*ny) %d\n", c.nn);
+  std::printf(" Stack size %d\n", c.routed ? c.nn : 0);
+  std::printf(" Number of nil elements in stack %lld\n", c.routed ? nil : 0LL);
+  std::printf(" Total number of donors %lld\n Total number of self donors %lld\n", sdon, self);
+  std::printf(" Total number of local minima %lld\n", minima);
+  std::printf(" Number of Gauss-Siedel iterations (SPL) %d\n", c.routed ? 1 : 0);
+  std::printf(" Timing (device milliseconds, accumulated while profiling is on):\n");
+  static const char* names[] = {"Uplift", "Receivers", "Stack", "LocalMinima", "LakeFill", "MFDReceivers",
+                                "DrainageArea", "SPL", "Diffusion"};
+  for (int s = 0; s < fsb::Ctx::kStages && s < 9; ++s)
+    if (c.stage_calls[s]) std::printf(" %s: %.6g\n", names[s], c.stage_ms[s]);
+  std::fflush(stdout);
   return 0;
 }
 
@@ -688,5 +834,13 @@ void fastscape_reset_cumulative_erosion_(void) { die_on(fsb_reset_cumulative_ero
 void fastscape_set_h_(double* hp) { die_on(fsb_set_h(g_single, hp, FSB_HOST)); }
 void fastscape_set_basement_(double* bp) { die_on(fsb_set_basement(g_single, bp, FSB_HOST)); }
 void fastscape_set_precip_(double* pp) { die_on(fsb_set_precip(g_single, pp, FSB_HOST)); }
+void fastscape_copy_chi_(double* p) { die_on(fsb_copy_chi(g_single, p, FSB_HOST)); }
+void fastscape_copy_slope_(double* p) { die_on(fsb_copy_slope(g_single, p, FSB_HOST)); }
+void fastscape_copy_curvature_(double* p) { die_on(fsb_copy_curvature(g_single, p, FSB_HOST)); }
+void fastscape_copy_catchment_(double* p) { die_on(fsb_copy_field(g_single, FSB_CATCHMENT, p, FSB_HOST)); }
+void fastscape_get_fluxes_(double* t, double* e, double* b) { die_on(fsb_get_fluxes(g_single, t, e, b)); }
+void fastscape_set_all_layers_(double* dh) { die_on(fsb_set_all_layers(g_single, dh, FSB_HOST)); }
+void fastscape_view_(void) { die_on(fsb_view(g_single)); }
+void fastscape_debug_(void) { die_on(fsb_debug(g_single)); }
 
 }  // extern "C"

@@ -269,6 +269,10 @@ __global__ void __launch_bounds__(128) k_fill_chains(ChainView cv, const int* __
 // their done flags at once, fences once and reads all their areas at once;
 // the chain recurrence then runs in registers in the original summation order.
 constexpr int kLight = 16;  // light donors fetched together per chunk
+// With CLAMP the same recurrence gives compute_fluxes' sediment flux
+// (FastScape_ctx.f90:864-869): base erate, max(0, .) before the node's value
+// goes downstream (and before a root adds itself).
+template <bool CLAMP>
 __global__ void __launch_bounds__(128) k_area_chains(ChainView cv, const int* __restrict__ rec,
                                                      const int* __restrict__ ndon, const int* __restrict__ don,
                                                      const double* __restrict__ precip, double dxdy,
@@ -338,6 +342,7 @@ __global__ void __launch_bounds__(128) k_area_chains(ChainView cv, const int* __
           }
           acc = acc + v;
         }
+        if (CLAMP) acc = fmax(0.0, acc);
         if (nd[i] >> 8) acc = acc + acc;
         a[k] = acc;
         ac = acc;
@@ -346,6 +351,58 @@ __global__ void __launch_bounds__(128) k_area_chains(ChainView cv, const int* __
     }
     fence_acq_rel();
     *(volatile unsigned*)&done[cv.ord[s]] = epoch;
+  }
+}
+
+// CopyChi (FastScape_ctx.f90:228-251) top down: chi(k) = chi(rec(k)) +
+// (a0/a(k))^(m/n) * length(k) where a(k) > a0, else 0; a root starts from 0.
+__global__ void __launch_bounds__(128) k_chi_chains(ChainView cv, const int* __restrict__ rec,
+                                                    const int* __restrict__ ndon, const double* __restrict__ a,
+                                                    const double* __restrict__ length, double a0, double mn,
+                                                    double* __restrict__ chi, unsigned* ticket, unsigned* done,
+                                                    unsigned epoch, int* err) {
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned w = 0;
+    if (lane == 0) w = atomicAdd(ticket, 32u);
+    w = __shfl_sync(FULL, w, 0);
+    if ((int)w >= cv.ntickets) break;
+    const int t = (int)w + lane;
+    const int c = t < cv.ntickets ? cv.tickets[t] : -1;
+    if (c < 0) continue;
+    int s, e;
+    cv.range(c, s, e);
+    const int k0 = cv.ord[s];
+    const int r0 = rec[k0];
+    double prev = 0.0;
+    if (r0 != k0) {
+      wait_flag(done, r0, epoch, err);
+      prev = __ldcg(&chi[r0]);
+    }
+    for (int p = s; p < e; p += kCF) {
+      const int n = min(kCF, e - p);
+      int kk[kCF], nd[kCF];
+      double term[kCF], aa[kCF], out[kCF];
+#pragma unroll
+      for (int i = 0; i < kCF; ++i) if (i < n) kk[i] = cv.ord[p + i];
+#pragma unroll
+      for (int i = 0; i < kCF; ++i) if (i < n) {
+        aa[i] = a[kk[i]];
+        nd[i] = ndon[kk[i]];
+        term[i] = pow(a0 / aa[i], mn) * length[kk[i]];
+      }
+#pragma unroll
+      for (int i = 0; i < kCF; ++i) if (i < n) {
+        const double v = aa[i] > a0 ? prev + term[i] : 0.0;
+        out[i] = v;
+        prev = v;
+      }
+#pragma unroll
+      for (int i = 0; i < kCF; ++i) if (i < n) chi[kk[i]] = out[i];
+      fence_acq_rel();
+#pragma unroll
+      for (int i = 0; i < kCF; ++i) if (i < n && nd[i] > 1) *(volatile unsigned*)&done[kk[i]] = epoch;
+    }
   }
 }
 
@@ -546,8 +603,24 @@ void fill_chains(Ctx& c) {
 void area_chains(Ctx& c) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_bu, c.nchains, c.ntickets_bu, c.nn};
-  k_area_chains<<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, c.precip, c.dx * c.dy, c.a, c.ticket,
-                                                    c.done, c.epoch, c.d_err);
+  k_area_chains<false><<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, c.precip, c.dx * c.dy,
+                                                                        c.a, c.ticket, c.done, c.epoch, c.d_err);
+  c.count_launch();
+}
+
+void flux_chains(Ctx& c, double* flux) {
+  next_epoch(c);
+  ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_bu, c.nchains, c.ntickets_bu, c.nn};
+  k_area_chains<true><<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, c.erate, 1.0, flux,
+                                                                       c.ticket, c.done, c.epoch, c.d_err);
+  c.count_launch();
+}
+
+void chi_chains(Ctx& c, double a0, double mn, double* chi) {
+  next_epoch(c);
+  ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_td, c.nchains, c.ntickets_td, c.nn};
+  k_chi_chains<<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.a, c.length, a0, mn, chi, c.ticket,
+                                                                c.done, c.epoch, c.d_err);
   c.count_launch();
 }
 

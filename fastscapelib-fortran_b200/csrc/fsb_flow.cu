@@ -279,11 +279,14 @@ union LineWords {
 };
 
 // a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115);
-// k's dependents are its distinct receivers.
+// k's dependents are its distinct receivers.  With `clamp` set and lines
+// built on erate it is compute_fluxes' sediment flux (FastScape_ctx.f90:871-877):
+// max(0, .) before the node's value goes downstream.
 struct AccMfdOp {
   const AccLine* line;
   int nx, ny;
   double* a;
+  int clamp;
   __device__ void prefetch(int k) const { prefetch_l1(line + k); }
   __device__ int run(int k, int* dep, unsigned* pr, const Loc& loc) const {
     const LineWords<6> L(line + k);  // aw[0..7] = d[0..7], base = d[8], don = u[18], rcv = u[19], pr = s[40..47]
@@ -309,6 +312,7 @@ struct AccMfdOp {
 #pragma unroll
     for (int t = 0; t < 8; ++t)
       if ((dc >> (4 * t)) & 15u) acc = acc + av[t] * L.d[t];
+    if (clamp) acc = fmax(0.0, acc);
     a[k] = acc;
     return nd;
   }
@@ -897,7 +901,15 @@ void accumulate(Ctx& c) {
   k_acc_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, c.dx * c.dy, c.mrec, c.mnrec, c.mwrec, c.precip, c.size,
                                                      line, c.cnt_acc, c.d_err);
   c.count_launch();
-  run_sweep<FSB_LANES_ACC, FSB_SIDE_DIV_ACC>(c, AccMfdOp{line, c.nx, c.ny, c.a}, c.cnt_acc);
+  run_sweep<FSB_LANES_ACC, FSB_SIDE_DIV_ACC>(c, AccMfdOp{line, c.nx, c.ny, c.a, 0}, c.cnt_acc);
+}
+
+void flux_mfd(Ctx& c, double* flux) {
+  AccLine* line = static_cast<AccLine*>(c.mfd_line);
+  k_acc_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, 1.0, c.mrec, c.mnrec, c.mwrec, c.erate, c.size, line,
+                                                     c.cnt_acc, c.d_err);
+  c.count_launch();
+  run_sweep<FSB_LANES_ACC, FSB_SIDE_DIV_ACC>(c, AccMfdOp{line, c.nx, c.ny, flux, 1}, c.cnt_acc);
 }
 
 void stream_power(Ctx& c) {

@@ -32,6 +32,7 @@ struct Ctx {
   bool sfd = false, runSPL = false, runDiffusion = false, runUplift = false;
   bool setup_done = false;
   bool capture = false;  // keep LocalMinima intermediates of the last step
+  bool routed = false;   // a step has built receivers, stack, chains and area
   int step = 0;
   cudaStream_t stream = 0;
   long long launches = 0;  // kernels launched by this instance
@@ -46,6 +47,8 @@ struct Ctx {
   double *h = nullptr, *b = nullptr, *u = nullptr, *kf = nullptr, *kd = nullptr, *precip = nullptr;
   double *etot = nullptr, *erate = nullptr, *a = nullptr, *length = nullptr, *lake_depth = nullptr;
   double *hwater = nullptr, *sedflux = nullptr;
+  double *catch0 = nullptr, *catchv = nullptr;  // catchment seeds (SetUp) and labels (ctx:17,94)
+  double* red = nullptr;                         // 3*512 partial sums + 3 results (get_fluxes)
   int *rec = nullptr, *ndon = nullptr, *don = nullptr /*8*nn*/, *stack = nullptr;
   int *pos = nullptr, *size = nullptr;
   int *mrec = nullptr /*8*nn*/, *mnrec = nullptr, *mstack = nullptr, *mdmask = nullptr;
@@ -152,6 +155,15 @@ void build_chains(Ctx& c);          // heavy-first order + ticket lists of the c
 void fill_chains(Ctx& c);
 void area_chains(Ctx& c);
 void spl_chains(Ctx& c, double* hnew);
+void flux_chains(Ctx& c, double* flux);               // compute_fluxes' flux, single flow
+void chi_chains(Ctx& c, double a0, double mn, double* chi);
+void flux_mfd(Ctx& c, double* flux);                  // compute_fluxes' flux, multiple flow
+// derived fields (fsb_derived.cu)
+void catchment(Ctx& c);                               // catch = catch0 of the root, before LocalMinima
+void slope_field(Ctx& c, double* out);
+void curvature_field(Ctx& c, double* out);
+void add_layers(Ctx& c, const double* dh);
+void flux_sums(Ctx& c, const double* flux, double* part, double* out3);
 
 // flow (fsb_flow.cu)
 void fill_sweep(Ctx& c);            // hwater along the stack (SFD lake fill / MFD h0)

@@ -622,6 +622,7 @@ bool local_minima(Ctx& c) {
   inclusive_scan_int(c, c.s_flag, c.s_scan2, nn);
   k_basins<<<grid1d(nn), kBlock, 0, st>>>(nn, c.stack, c.s_scan2, c.basins);
   c.count_launch();
+  catchment(c);  // find_stack's catch: labels of the forest before re-routing
   fetch_counters(c, 10);
   const int nroots = c.h_cnt[C_NBASINS];
   k_roots_scan<<<grid1d(nroots), kBlock, 0, st>>>(c.bd, nroots, c.s_roots, c.d_cnt);

@@ -49,8 +49,8 @@ _lib = ctypes.CDLL(LIB_PATH)
 
 FSB_HOST, FSB_DEVICE = 0, 1
 FIELDS = {"h": 0, "basement": 1, "total_erosion": 2, "drainage_area": 3, "erosion_rate": 4,
-          "lake_depth": 5, "length": 6, "hwater": 7, "sedflux": 8, "u": 10, "precip": 11,
-          "kf": 12, "kd": 13}
+          "lake_depth": 5, "length": 6, "hwater": 7, "sedflux": 8, "catchment": 9, "u": 10,
+          "precip": 11, "kf": 12, "kd": 13}
 INT_FIELDS = {"rec": 0, "ndon": 1, "stack": 2, "mnrec": 3, "mstack": 4, "basins": 5,
               "rec_pre": 6, "stack_pre": 7}
 SLOT_FIELDS = {"don": 0, "mrec": 1, "mwrec": 2, "mlrec": 3}
@@ -93,6 +93,12 @@ _sig("fsb_set_capture", _vp, _i)
 _sig("fsb_locmin_counts", _vp, _vp)
 _sig("fsb_copy_locmin", _vp, *([_vp] * 11))
 _sig("fsb_synchronize", _vp)
+for _n in ("fsb_copy_chi", "fsb_copy_slope", "fsb_copy_curvature"):
+    _sig(_n, _vp, _vp, _i)
+_sig("fsb_get_fluxes", _vp, ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_d))
+_sig("fsb_set_all_layers", _vp, _vp, _i)
+_sig("fsb_view", _vp)
+_sig("fsb_debug", _vp)
 _sig("fsb_launch_count", _vp, res=ctypes.c_longlong)
 _sig("fsb_set_profile", _vp, _i)
 _sig("fsb_stage_times", _vp, _vp, _vp, _i, _i)
@@ -286,6 +292,41 @@ class FastScape:
         ptr, where = self._out(buf)
         _check(_lib.fsb_copy_field(self._h, FIELDS[name], ptr, where))
         self._sync_if_device(where)
+
+    def _derived(self, fn, buf) -> None:
+        dst, where = self._out(buf)
+        _check(fn(self._h, dst, where))
+        self._sync_if_device(where)
+
+    def copy_chi(self, buf) -> None:
+        """FastScape_Copy_Chi (api:379): chi along the last step's stack."""
+        self._derived(_lib.fsb_copy_chi, buf)
+
+    def copy_slope(self, buf) -> None:
+        """FastScape_Copy_Slope (api:395): slope in degrees."""
+        self._derived(_lib.fsb_copy_slope, buf)
+
+    def copy_curvature(self, buf) -> None:
+        """FastScape_Copy_Curvature (api:411)."""
+        self._derived(_lib.fsb_copy_curvature, buf)
+
+    def get_fluxes(self):
+        """FastScape_Get_Fluxes (api:762): (tectonic, erosion, boundary) fluxes."""
+        t, e, b = _d(), _d(), _d()
+        _check(_lib.fsb_get_fluxes(self._h, ctypes.byref(t), ctypes.byref(e), ctypes.byref(b)))
+        return t.value, e.value, b.value
+
+    def set_all_layers(self, dh) -> None:
+        """FastScape_Set_All_Layers (api:680): h and basement += dh."""
+        self._set(_lib.fsb_set_all_layers, dh)
+
+    def view(self) -> None:
+        """FastScape_View (api:188): prints a summary of the instance."""
+        _check(_lib.fsb_view(self._h))
+
+    def debug(self) -> None:
+        """FastScape_Debug (api:588): prints routing counts and stage times."""
+        _check(_lib.fsb_debug(self._h))
 
     def field(self, name: str) -> torch.Tensor:
         """Zero-copy float64 view of a device field (shape (ny, nx))."""
@@ -568,6 +609,39 @@ def fastscape_copy_erosion_rate(eratep):
 
 def fastscape_copy_lake_depth(lp):
     _inst().copy("lake_depth", lp)
+
+
+def fastscape_copy_chi(chip):
+    _inst().copy_chi(chip)
+
+
+def fastscape_copy_slope(slopep):
+    _inst().copy_slope(slopep)
+
+
+def fastscape_copy_curvature(curvaturep):
+    _inst().copy_curvature(curvaturep)
+
+
+def fastscape_copy_catchment(catchp):
+    _inst().copy("catchment", catchp)
+
+
+def fastscape_get_fluxes():
+    """FastScape_Get_Fluxes (api:762); f2py returns the intent(out) scalars."""
+    return _inst().get_fluxes()
+
+
+def fastscape_set_all_layers(dhp):
+    _inst().set_all_layers(dhp)
+
+
+def fastscape_view():
+    _inst().view()
+
+
+def fastscape_debug():
+    _inst().debug()
 
 
 __all__ = [n for n in dir() if n.startswith("fastscape_")] + ["FastScape", "Job", "Batch", "LIB_PATH"]

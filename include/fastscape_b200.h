@@ -45,6 +45,8 @@ enum {
   FSB_LENGTH = 6,         /* receiver distance (internal array length, ctx:17)           */
   FSB_HWATER = 7,         /* filled surface (internal array hwater, ctx:33)              */
   FSB_SEDFLUX = 8,        /* Sedflux (ctx:18)                                            */
+  FSB_CATCHMENT = 9,      /* catch: catch0 of the node's root before LocalMinima
+                             FastScape_Copy_Catchment api:427 (ctx:297-307, FlowRouting.f90:393-443) */
   FSB_U = 10, FSB_PRECIP = 11, FSB_KF = 12, FSB_KD = 13
 };
 
@@ -135,6 +137,21 @@ int fsb_locmin_counts(fsb_ctx* c, int* out6);
 int fsb_copy_locmin(fsb_ctx* c, int* b1, int* b2, int* n1, int* n2, double* w, int* sort_id,
                     int* tree, int* ob1, int* ob2, int* on1, int* on2);
 /* Blocks until the instance's stream is idle; reports device-side errors */
+/* FastScape_Copy_Chi (api:379 -> ctx:228-251): chi along the stack of the last
+   step, a0 = 10*dx*dy; zeros before the first step that routed flow. */
+int fsb_copy_chi(fsb_ctx* c, double* dst, int where);
+/* FastScape_Copy_Slope (api:395 -> ctx:255-272, TerrainDerivatives.f90:3-35), degrees */
+int fsb_copy_slope(fsb_ctx* c, double* dst, int where);
+/* FastScape_Copy_Curvature (api:411 -> ctx:276-293, TerrainDerivatives.f90:39-74) */
+int fsb_copy_curvature(fsb_ctx* c, double* dst, int where);
+/* FastScape_Get_Fluxes (api:762 -> ctx:843-886): tectonic, erosion and boundary fluxes */
+int fsb_get_fluxes(fsb_ctx* c, double* tectonic, double* erosion, double* boundary);
+/* FastScape_Set_All_Layers (api:680 -> ctx:660-676): h and b += dh (no stratigraphy) */
+int fsb_set_all_layers(fsb_ctx* c, const double* dh, int where);
+/* FastScape_View (api:188 -> ctx:378-393) and FastScape_Debug (api:588 -> ctx:513-561):
+   summaries printed to stdout */
+int fsb_view(fsb_ctx* c);
+int fsb_debug(fsb_ctx* c);
 int fsb_synchronize(fsb_ctx* c);
 /* Kernels this instance has launched so far (for throughput accounting) */
 long long fsb_launch_count(fsb_ctx* c);
@@ -238,6 +255,15 @@ void fastscape_reset_cumulative_erosion_(void);                    /* api:650 */
 void fastscape_set_h_(double* hp);                                 /* api:664 */
 void fastscape_set_basement_(double* bp);                          /* api:696 */
 void fastscape_set_precip_(double* precipp);                       /* api:712 */
+void fastscape_copy_chi_(double* chip);                            /* api:379 */
+void fastscape_copy_slope_(double* slopep);                        /* api:395 */
+void fastscape_copy_curvature_(double* curvaturep);                /* api:411 */
+void fastscape_copy_catchment_(double* catchp);                    /* api:427 */
+void fastscape_get_fluxes_(double* ttectonic_flux, double* eerosion_flux,
+                           double* bboundary_flux);                /* api:762 */
+void fastscape_set_all_layers_(double* dhp);                       /* api:680 */
+void fastscape_view_(void);                                        /* api:188 */
+void fastscape_debug_(void);                                       /* api:588 */
 
 #ifdef __cplusplus
 }

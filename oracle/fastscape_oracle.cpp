@@ -1144,4 +1144,117 @@ int fso_indexx(int n, const double* arr, int* indx) {
   return rc;
 }
 
+// ---- derived fields and diagnostics of the API ----------------------------
+
+// CopyChi -- FastScape_ctx.f90:228-251: along the stack, chi(k) = chi(rec(k))
+// + (a0/a(k))**(m/n) * length(k) where a(k) > a0 = dx*dy*10, else 0.
+int fso_copy_chi(double* out) {
+  Ctx& c = *C;
+  if (!c.setup_done) return fail("CopyChi - You need to run SetUp first");
+  dvec chi(c.nn + 1, 0.0);
+  const double dx = c.xl / (c.nx - 1), dy = c.yl / (c.ny - 1);
+  const double a0 = dx * dy * 10.0;
+  for (int ij = 1; ij <= c.nn; ++ij) {
+    const int ijk = c.stack[ij];
+    if (ijk < 1) continue;  // stack not built yet (no step run)
+    if (c.a[ijk] > a0) chi[ijk] = chi[c.rec[ijk]] + std::pow(a0 / c.a[ijk], c.m / c.n) * c.length[ijk];
+  }
+  for (int i = 0; i < c.nn; ++i) out[i] = chi[i + 1];
+  return 0;
+}
+
+// slope -- TerrainDerivatives.f90:3-35 (degrees; 0 on the grid's edges)
+int fso_copy_slope(double* out) {
+  Ctx& c = *C;
+  if (!c.setup_done) return fail("CopySlope - You need to run SetUp first");
+  const int nx = c.nx, ny = c.ny;
+  const double dx = c.xl / (nx - 1), dy = c.yl / (ny - 1);
+  const double con = 45.0 / std::atan(1.0);
+  const dvec& h = c.h;
+  dvec s(c.nn + 1, 0.0);
+  for (int j = 2; j <= ny - 1; ++j)
+    for (int i = 2; i <= nx - 1; ++i) {
+      const int ij = i + (j - 1) * nx;
+      const int ia = ij + nx - 1, ib = ia + 1, ic = ib + 1, id = ij - 1, iff = ij + 1;
+      const int ig = ij - nx - 1, ih = ig + 1, ii = ih + 1;
+      const double dzdx = ((h[ic] + 2.0 * h[iff] + h[ii]) - (h[ia] + 2.0 * h[id] + h[ig])) / 8.0 / dx;
+      const double dzdy = ((h[ig] + 2.0 * h[ih] + h[ii]) - (h[ia] + 2.0 * h[ib] + h[ic])) / 8.0 / dy;
+      s[ij] = dzdx * dzdx + dzdy * dzdy;
+      if (s[ij] > DBL_MIN) s[ij] = std::atan(std::sqrt(s[ij])) * con;
+    }
+  for (int i = 0; i < c.nn; ++i) out[i] = s[i + 1];
+  return 0;
+}
+
+// curvature -- TerrainDerivatives.f90:39-74 (0 on the grid's edges)
+int fso_copy_curvature(double* out) {
+  Ctx& c = *C;
+  if (!c.setup_done) return fail("CopyCurvature - You need to run SetUp first");
+  const int nx = c.nx, ny = c.ny;
+  const double dx = c.xl / (nx - 1), dy = c.yl / (ny - 1);
+  const dvec& h = c.h;
+  dvec cv(c.nn + 1, 0.0);
+  for (int j = 2; j <= ny - 1; ++j)
+    for (int i = 2; i <= nx - 1; ++i) {
+      const int ij = i + (j - 1) * nx;
+      const int i1 = ij + nx - 1, i2 = i1 + 1, i3 = i2 + 1, i4 = ij - 1, i5 = ij, i6 = ij + 1;
+      const int i7 = ij - nx - 1, i8 = i7 + 1, i9 = i8 + 1;
+      const double a = (h[i1] + h[i3] + h[i4] + h[i6] + h[i7] + h[i9]) / dx / dx / 12.0 -
+                       (h[i2] + h[i5] + h[i8]) / dx / dx / 6.0;
+      const double b = (h[i1] + h[i2] + h[i3] + h[i7] + h[i8] + h[i9]) / dy / dy / 12.0 -
+                       (h[i4] + h[i5] + h[i6]) / dy / dy / 6.0;
+      const double cc = (h[i3] + h[i7] - h[i1] - h[i9]) / dx / dy / 4.0;
+      const double d = (h[i3] + h[i6] + h[i9] - h[i1] - h[i4] - h[i7]) / dx / 6.0;
+      const double e = (h[i1] + h[i2] + h[i3] - h[i7] - h[i8] - h[i9]) / dy / 6.0;
+      cv[ij] = 1.0 + d * d + e * e;
+      if (cv[ij] > DBL_MIN)
+        cv[ij] = (a * (1.0 + e * e) + b * (1.0 + d * d) - cc * d * e) / std::pow(cv[ij], 3.0 / 2.0);
+    }
+  for (int i = 0; i < c.nn; ++i) out[i] = cv[i + 1];
+  return 0;
+}
+
+// compute_fluxes -- FastScape_ctx.f90:843-886: out3 = tectonic, erosion and
+// boundary fluxes (erate accumulated downstream with max(0, .) at each node).
+int fso_get_fluxes(double* out3) {
+  Ctx& c = *C;
+  if (!c.setup_done) return fail("GetFluxes - You need to run SetUp first");
+  const double surf = c.xl * c.yl / (c.nx - 1) / (c.ny - 1);
+  double su = 0.0, se = 0.0;
+  for (int i = 1; i <= c.nn; ++i) { su += c.u[i]; se += c.erate[i]; }
+  dvec flux = c.erate;
+  if (c.step > 0) {
+    if (c.sfd) {
+      for (int ij = c.nn; ij >= 1; --ij) {
+        const int ijk = c.stack[ij];
+        flux[ijk] = std::max(0.0, flux[ijk]);
+        flux[c.rec[ijk]] = flux[c.rec[ijk]] + flux[ijk];
+      }
+    } else {
+      for (int ij = 1; ij <= c.nn; ++ij) {
+        const int ijk = c.mstack[ij];
+        flux[ijk] = std::max(0.0, flux[ijk]);
+        for (int k = 1; k <= c.mnrec[ijk]; ++k) {
+          const size_t o = (size_t)(ijk - 1) * 8 + (k - 1);
+          flux[c.mrec[o]] = flux[c.mrec[o]] + flux[ijk] * c.mwrec[o];
+        }
+      }
+    }
+  }
+  double sb = 0.0;
+  for (int i = 1; i <= c.nn; ++i) if (c.bc[i]) sb += flux[i];
+  out3[0] = su * surf;
+  out3[1] = se * surf;
+  out3[2] = sb * surf;
+  return 0;
+}
+
+// SetAllLayers -- FastScape_ctx.f90:660-676 (no stratigraphy): h, b += dh
+int fso_set_all_layers(const double* dh) {
+  Ctx& c = *C;
+  if (!c.setup_done) return fail("SetAllLayers - You need to run SetUp first");
+  for (int i = 1; i <= c.nn; ++i) { c.h[i] = c.h[i] + dh[i - 1]; c.b[i] = c.b[i] + dh[i - 1]; }
+  return 0;
+}
+
 }  // extern "C"

@@ -62,6 +62,9 @@ def lib():
         L.fso_locmin_arrays.argtypes = [_I32P, _I32P, _I32P, _I32P, _F64P, _I32P, _I32P,
                                         _I32P, _I32P, _I32P, _I32P]
         L.fso_indexx.argtypes = [ctypes.c_int, _F64P, _I32P]
+        for name in ("fso_copy_chi", "fso_copy_slope", "fso_copy_curvature", "fso_get_fluxes",
+                     "fso_set_all_layers"):
+            getattr(L, name).argtypes = [_F64P]
         _lib = L
     return _lib
 
@@ -209,3 +212,40 @@ def indexx(arr) -> np.ndarray:
 
 def get_ngs() -> int:
     return lib().fso_get_ngs()
+
+
+def _derived(fn) -> np.ndarray:
+    out = np.empty(_nn(), dtype=np.float64)
+    _check(fn(out))
+    return out
+
+
+def fastscape_copy_chi(buf):
+    """CopyChi (FastScape_ctx.f90:228-251)."""
+    buf[...] = _derived(lib().fso_copy_chi).reshape(buf.shape)
+
+
+def fastscape_copy_slope(buf):
+    """slope (TerrainDerivatives.f90:3-35), in degrees."""
+    buf[...] = _derived(lib().fso_copy_slope).reshape(buf.shape)
+
+
+def fastscape_copy_curvature(buf):
+    """curvature (TerrainDerivatives.f90:39-74)."""
+    buf[...] = _derived(lib().fso_copy_curvature).reshape(buf.shape)
+
+
+def fastscape_copy_catchment(buf):
+    buf[...] = copy_double("catchment").reshape(buf.shape)
+
+
+def fastscape_get_fluxes():
+    """compute_fluxes (FastScape_ctx.f90:843-886): (tectonic, erosion, boundary)."""
+    out = np.zeros(3, dtype=np.float64)
+    _check(lib().fso_get_fluxes(out))
+    return float(out[0]), float(out[1]), float(out[2])
+
+
+def fastscape_set_all_layers(dh):
+    """SetAllLayers (FastScape_ctx.f90:660-676) without stratigraphy."""
+    _check(lib().fso_set_all_layers(_f64(dh, _nn())))

@@ -149,3 +149,100 @@ def test_setup_errors():
     O.fastscape_init()
     with pytest.raises(RuntimeError, match="SetUp"):
         O.fastscape_execute_step()
+
+
+def _literal_chi(stack, rec, a, length, a0, mn):
+    """CopyChi (FastScape_ctx.f90:228-251), loop for loop (0-based ids)."""
+    chi = np.zeros(a.size)
+    for ijk in stack:
+        if a[ijk] > a0:
+            chi[ijk] = chi[rec[ijk]] + (a0 / a[ijk]) ** mn * length[ijk]
+    return chi
+
+
+def _literal_slope_curv(h, nx, ny, dx, dy):
+    """slope and curvature (TerrainDerivatives.f90:3-74) in plain Python."""
+    con = 45.0 / np.arctan(1.0)
+    s = np.zeros(nx * ny)
+    cv = np.zeros(nx * ny)
+    for j in range(1, ny - 1):
+        for i in range(1, nx - 1):
+            ij = i + j * nx
+            ia, id_, ig = ij + nx - 1, ij - 1, ij - nx - 1
+            ib, ic, if_, ih, ii = ia + 1, ia + 2, ij + 1, ig + 1, ig + 2
+            dzdx = ((h[ic] + 2.0 * h[if_] + h[ii]) - (h[ia] + 2.0 * h[id_] + h[ig])) / 8.0 / dx
+            dzdy = ((h[ig] + 2.0 * h[ih] + h[ii]) - (h[ia] + 2.0 * h[ib] + h[ic])) / 8.0 / dy
+            v = dzdx * dzdx + dzdy * dzdy
+            s[ij] = np.arctan(np.sqrt(v)) * con if v > np.finfo(float).tiny else v
+            i1, i2, i3, i4, i5, i6, i7, i8, i9 = ia, ib, ic, id_, ij, if_, ig, ih, ii
+            a = (h[i1] + h[i3] + h[i4] + h[i6] + h[i7] + h[i9]) / dx / dx / 12.0 - \
+                (h[i2] + h[i5] + h[i8]) / dx / dx / 6.0
+            b = (h[i1] + h[i2] + h[i3] + h[i7] + h[i8] + h[i9]) / dy / dy / 12.0 - \
+                (h[i4] + h[i5] + h[i6]) / dy / dy / 6.0
+            c = (h[i3] + h[i7] - h[i1] - h[i9]) / dx / dy / 4.0
+            d = (h[i3] + h[i6] + h[i9] - h[i1] - h[i4] - h[i7]) / dx / 6.0
+            e = (h[i1] + h[i2] + h[i3] - h[i7] - h[i8] - h[i9]) / dy / 6.0
+            v = 1.0 + d * d + e * e
+            cv[ij] = (a * (1.0 + e * e) + b * (1.0 + d * d) - c * d * e) / v ** 1.5
+    return s, cv
+
+
+@pytest.mark.parametrize("maker", [lambda: W.plain_d8(23, 19, seed=31, nsteps=3),
+                                   lambda: W.mfd(21, 25, seed=32, nsteps=3, bc=1010)])
+def test_derived_fields_match_literal(maker):
+    """chi, slope, curvature, fluxes and set_all_layers of the oracle against
+    plain-Python transliterations of the reference routines."""
+    wl = maker()
+    wl.apply(O)
+    for _ in range(wl.nsteps):
+        O.fastscape_execute_step()
+    nn = wl.nn
+    dx, dy = wl.xl / (wl.nx - 1), wl.yl / (wl.ny - 1)
+    buf = np.empty(nn)
+    O.fastscape_copy_chi(buf)
+    ref = _literal_chi(O.copy_int("stack"), O.copy_int("rec"), O.copy_double("drainage_area"),
+                       O.copy_double("length"), dx * dy * 10.0, wl.m / wl.n)
+    assert np.array_equal(buf, ref)
+    s, cv = _literal_slope_curv(O.copy_double("h"), wl.nx, wl.ny, dx, dy)
+    O.fastscape_copy_slope(buf)
+    assert np.allclose(buf, s, rtol=1e-14, atol=0)
+    O.fastscape_copy_curvature(buf)
+    assert np.allclose(buf, cv, rtol=1e-12, atol=1e-12 * np.abs(cv).max())
+    # compute_fluxes (FastScape_ctx.f90:843-886)
+    erate, u = O.copy_double("erosion_rate"), O.copy_double("u")
+    flux = erate.copy()
+    if wl.p < -1.5:
+        stack, rec = O.copy_int("stack"), O.copy_int("rec")
+        for ijk in stack[::-1]:
+            flux[ijk] = max(0.0, flux[ijk])
+            flux[rec[ijk]] += flux[ijk]
+    else:
+        mrec, mwrec, mnrec = O.copy_slots("mrec"), O.copy_slots("mwrec"), O.copy_int("mnrec")
+        for ijk in O.copy_int("mstack"):
+            flux[ijk] = max(0.0, flux[ijk])
+            for k in range(mnrec[ijk]):
+                flux[mrec[ijk, k]] += flux[ijk] * mwrec[ijk, k]
+    bcmask = np.zeros((wl.ny, wl.nx), bool)
+    bcmask[0, :] = bcmask[-1, :] = True  # bc 1111 / 1010: bottom and top fixed
+    if wl.bc == 1111:
+        bcmask[:, 0] = bcmask[:, -1] = True
+    surf = wl.xl * wl.yl / (wl.nx - 1) / (wl.ny - 1)
+    t, e, b = O.fastscape_get_fluxes()
+    assert np.isclose(t, u.sum() * surf, rtol=1e-13)
+    assert np.isclose(e, erate.sum() * surf, rtol=1e-13)
+    assert np.isclose(b, flux[bcmask.ravel()].sum() * surf, rtol=1e-13)
+    # catchment: catch0 of each node's root in the forest before LocalMinima
+    catch = O.copy_double("catchment")
+    rec_pre = O.copy_int("rec_pre")
+    root = np.arange(nn)
+    for _ in range(nn):
+        nxt = rec_pre[root]
+        if np.array_equal(nxt, root):
+            break
+        root = nxt
+    assert np.array_equal(catch, catch[root])  # constant along each pre-LocalMinima tree
+    dh = np.linspace(-1.0, 1.0, nn)
+    h0, b0 = O.copy_double("h"), O.copy_double("basement")
+    O.fastscape_set_all_layers(dh)
+    assert np.array_equal(O.copy_double("h"), h0 + dh)
+    assert np.array_equal(O.copy_double("basement"), b0 + dh)
