@@ -159,6 +159,7 @@ size_t layout(fsb::Ctx& c, char* base) {
   c.done = L.take<unsigned>(N); c.ticket = L.take<unsigned>(4);
   c.water = L.take<double>(N); c.hnew = L.take<double>(N);
   c.catch0 = L.take<double>(N); c.catchv = L.take<double>(N); c.red = L.take<double>(3 * 512 + 8);
+  c.g = L.take<double>(N);
   c.dK = L.take<double>(N); c.dA = L.take<double>(N); c.dB = L.take<double>(N); c.dC = L.take<double>(N);
   c.dF = L.take<double>(N); c.dG = L.take<double>(N); c.dZ = L.take<double>(N);
   c.d_err = L.take<int>(4); c.d_cnt = L.take<int>(32);
@@ -256,8 +257,6 @@ void collect_stage_times(fsb::Ctx& c) {
 }
 
 int step_once(fsb::Ctx& c) {
-  if (c.runSPL && (c.g1 > 0.0 || c.g2 > 0.0))
-    return fail("set_erosional_parameters: g1/g2 > 0 (sediment deposition) is not supported by this build");
   if (c.runUplift) {
     stage_begin(c, ST_UPLIFT);
     fsb::launch_uplift(c);
@@ -296,7 +295,12 @@ int step_once(fsb::Ctx& c) {
     fsb::accumulate(c);
     stage_end(c, ST_ACCUM);
     stage_begin(c, ST_SPL);
-    fsb::stream_power(c);
+    if (fsb::gs_active(c)) {
+      if (fsb::stream_power_gs(c)) return 1;
+    } else {
+      fsb::stream_power(c);
+      c.ngs = 1;
+    }
     stage_end(c, ST_SPL);
   }
   if (c.runDiffusion) {
@@ -428,6 +432,8 @@ int fsb_setup(fsb_ctx* h, void* arena, size_t bytes) {
   c.p = 1.0;
   c.step = 0;
   c.routed = false;
+  c.g_positive = false;
+  c.ngs = 0;
   c.setup_done = true;
   return 0;
 }
@@ -628,6 +634,12 @@ void min_mean_max(const std::vector<double>& v, double& lo, double& mean, double
 }  // namespace
 }  // extern "C++"
 
+int fsb_get_gs_iterations(fsb_ctx* h, int* n) {
+  if (!h || !n) return fail("null argument");
+  *n = h->c.ngs;
+  return 0;
+}
+
 int fsb_view(fsb_ctx* h) {
   if (need_setup(h, "View")) return 1;
   fsb::Ctx& c = h->c;
@@ -669,7 +681,7 @@ int fsb_debug(fsb_ctx* h) {
   std::printf(" Number of nil elements in stack %lld\n", c.routed ? nil : 0LL);
   std::printf(" Total number of donors %lld\n Total number of self donors %lld\n", sdon, self);
   std::printf(" Total number of local minima %lld\n", minima);
-  std::printf(" Number of Gauss-Siedel iterations (SPL) %d\n", c.routed ? 1 : 0);
+  std::printf(" Number of Gauss-Siedel iterations (SPL) %d\n", c.ngs);
   std::printf(" Timing (device milliseconds, accumulated while profiling is on):\n");
   static const char* names[] = {"Uplift", "Receivers", "Stack", "LocalMinima", "LakeFill", "MFDReceivers",
                                 "DrainageArea", "SPL", "Diffusion"};

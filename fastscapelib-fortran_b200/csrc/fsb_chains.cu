@@ -269,15 +269,59 @@ __global__ void __launch_bounds__(128) k_fill_chains(ChainView cv, const int* __
 // their done flags at once, fences once and reads all their areas at once;
 // the chain recurrence then runs in registers in the original summation order.
 constexpr int kLight = 16;  // light donors fetched together per chunk
-// With CLAMP the same recurrence gives compute_fluxes' sediment flux
-// (FastScape_ctx.f90:864-869): base erate, max(0, .) before the node's value
-// goes downstream (and before a root adds itself).
-template <bool CLAMP>
+// Finishers of the bottom-up recurrence v(k) = fin(k, base(k) + v(d_m) + ... + v(d_1)):
+//   AreaFin  drainage area; a root adds itself (FlowRouting.f90:136-139)
+//   FluxFin  compute_fluxes' sediment flux: base erate, max(0, .) before the
+//            value goes downstream, a root adds itself (FastScape_ctx.f90:864-869)
+//   GsFin    the erosion sum of a Gauss-Seidel iteration with g > 0
+//            (StreamPowerLaw.f90:262-280): base ht-hp; a lake sill's own
+//            share is taken out and kept as lake_sediment
+//   VolFin   lake water volume: a flooded node passes its contribution
+//            (w_rcv - h) and its flooded donors' up to its receiver; every
+//            node records what its donors pass as its volume (a sill's volume)
+struct AreaFin {
+  const double* precip;
+  double dxdy;
+  __device__ double base(int k) const { return dxdy * precip[k]; }
+  __device__ double finish(int, double acc, bool root) const { return root ? acc + acc : acc; }
+};
+struct FluxFin {
+  const double* erate;
+  __device__ double base(int k) const { return erate[k]; }
+  __device__ double finish(int, double acc, bool root) const {
+    acc = fmax(0.0, acc);
+    return root ? acc + acc : acc;
+  }
+};
+struct GsFin {
+  const double *ht, *hp;
+  const int* sill;
+  double* lsed;
+  __device__ double base(int k) const { return ht[k] - hp[k]; }
+  __device__ double finish(int k, double acc, bool root) const {
+    if (root) { lsed[k] = acc; return acc; }
+    const double e = ht[k] - hp[k];
+    const double t = acc - e;
+    if (sill[k] == k) lsed[k] = t <= 0.0 ? 0.0 : t;
+    return t + e;
+  }
+};
+struct VolFin {
+  const int* sill;
+  const double* contrib;
+  double* vol;
+  __device__ double base(int) const { return 0.0; }
+  __device__ double finish(int k, double acc, bool root) const {
+    vol[k] = acc;
+    return (!root && sill[k] != k) ? contrib[k] + acc : 0.0;
+  }
+};
+
+template <class Fin>
 __global__ void __launch_bounds__(128) k_area_chains(ChainView cv, const int* __restrict__ rec,
                                                      const int* __restrict__ ndon, const int* __restrict__ don,
-                                                     const double* __restrict__ precip, double dxdy,
-                                                     double* __restrict__ a, unsigned* ticket, unsigned* done,
-                                                     unsigned epoch, int* err) {
+                                                     Fin fin, double* __restrict__ a, unsigned* ticket,
+                                                     unsigned* done, unsigned epoch, int* err) {
   const int lane = threadIdx.x & 31;
   for (;;) {
     unsigned w = 0;
@@ -301,7 +345,7 @@ __global__ void __launch_bounds__(128) k_area_chains(ChainView cv, const int* __
 #pragma unroll
       for (int i = 0; i < kCF; ++i) if (i < n) {
         nd[i] = ndon[kk[i]];
-        base[i] = dxdy * precip[kk[i]];
+        base[i] = fin.base(kk[i]);
         if (rec[kk[i]] == kk[i]) nd[i] |= 1 << 8;
       }
       // light donors of the chunk in processing order (i descending, q descending);
@@ -342,8 +386,7 @@ __global__ void __launch_bounds__(128) k_area_chains(ChainView cv, const int* __
           }
           acc = acc + v;
         }
-        if (CLAMP) acc = fmax(0.0, acc);
-        if (nd[i] >> 8) acc = acc + acc;
+        acc = fin.finish(k, acc, (nd[i] >> 8) != 0);
         a[k] = acc;
         ac = acc;
         child = k;
@@ -409,14 +452,27 @@ __global__ void __launch_bounds__(128) k_chi_chains(ChainView cv, const int* __r
 // Top-down single-flow stream power law with g == 0 (StreamPowerLaw.f90:291-373):
 // writes hnew and water; h keeps ht.  The per-node factor kf*dt*a^m/l(^n)
 // does not depend on the recurrence and is computed for a whole chunk first.
+// With GS (a Gauss-Seidel iteration of the g > 0 solve, StreamPowerLaw.f90:285-373)
+// the deposition-corrected surface comes from `elev`, Newton starts from the
+// current iterate `hstart`, and the lake bookkeeping is written: sill(k) = k
+// for a node above its receiver's water, else sill(rec) with its volume
+// contribution w_rcv - h(k) in contrib(k).  Without GS, elev = hstart = ht.
+struct GsIo {
+  const double* elev;
+  const double* hstart;
+  int* sill;
+  double* contrib;
+};
+
+template <bool GS>
 __global__ void __launch_bounds__(128) k_spl_chains(ChainView cv, const int* __restrict__ rec,
                                                     const int* __restrict__ ndon, const double* __restrict__ h,
                                                     const double* __restrict__ b, const double* __restrict__ kf,
                                                     const double* __restrict__ a, const double* __restrict__ length,
                                                     double kfsed, double dt, double m, double n, double omega,
                                                     int n_is_one, double* __restrict__ hnew,
-                                                    double* __restrict__ water, unsigned* ticket, unsigned* done,
-                                                    unsigned epoch, int* err) {
+                                                    double* __restrict__ water, GsIo gs, unsigned* ticket,
+                                                    unsigned* done, unsigned epoch, int* err) {
   const int lane = threadIdx.x & 31;
   for (;;) {
     unsigned w = 0;
@@ -432,22 +488,26 @@ __global__ void __launch_bounds__(128) k_spl_chains(ChainView cv, const int* __r
     const int r0 = rec[k0];
     bool root = r0 == k0;
     double hr = 0.0, wr = 0.0, htr = 0.0;
+    int sr = 0;
     if (!root) {
       wait_flag(done, r0, epoch, err);
       hr = __ldcg(&hnew[r0]);
       wr = __ldcg(&water[r0]);
       htr = h[r0];
+      if (GS) sr = __ldcg(&gs.sill[r0]);
     }
     for (int p = s; p < e; p += kCS) {
       const int cn = min(kCS, e - p);
-      int kk[kCS], nd[kCS];
-      double ht[kCS], fact[kCS], ho[kCS], wo[kCS];
+      int kk[kCS], nd[kCS], so[kCS];
+      double ht[kCS], fact[kCS], ho[kCS], wo[kCS], el[kCS], h0[kCS], co[kCS];
 #pragma unroll
       for (int i = 0; i < kCS; ++i) if (i < cn) kk[i] = cv.ord[p + i];
 #pragma unroll
       for (int i = 0; i < kCS; ++i) if (i < cn) {
         const int k = kk[i];
         ht[i] = h[k];
+        el[i] = GS ? gs.elev[k] : ht[i];
+        h0[i] = GS ? gs.hstart[k] : ht[i];
         nd[i] = ndon[k];
         const double kfint = (kfsed > 0.0 && (ht[i] - b[k]) > 1.0) ? kfsed : kf[k];
         const double l = length[k];
@@ -456,11 +516,14 @@ __global__ void __launch_bounds__(128) k_spl_chains(ChainView cv, const int* __r
 #pragma unroll
       for (int i = 0; i < kCS; ++i) if (i < cn) {
         double hk = ht[i], wk;
+        int sk = kk[i];
+        double ck = 0.0;
         if (root) {
           wk = ht[i];
           root = false;
         } else {
-          const double elev = ht[i];
+          const double elev = el[i];
+          hk = h0[i];
           if (elev > wr) {
             if (n_is_one) {
               double f = elev, df = 1.0;
@@ -494,17 +557,26 @@ __global__ void __launch_bounds__(128) k_spl_chains(ChainView cv, const int* __r
             if (hk < wr) hk = wr;
           } else {
             hk = elev;
+            sk = sr;
+            ck = wr - hk;
           }
           wk = fmax(wr, hk);
         }
         ho[i] = hk;
         wo[i] = wk;
+        so[i] = sk;
+        co[i] = ck;
         hr = hk;
         wr = wk;
         htr = ht[i];
+        sr = sk;
       }
 #pragma unroll
-      for (int i = 0; i < kCS; ++i) if (i < cn) { hnew[kk[i]] = ho[i]; water[kk[i]] = wo[i]; }
+      for (int i = 0; i < kCS; ++i) if (i < cn) {
+        hnew[kk[i]] = ho[i];
+        water[kk[i]] = wo[i];
+        if (GS) { gs.sill[kk[i]] = so[i]; gs.contrib[kk[i]] = co[i]; }
+      }
       fence_acq_rel();
 #pragma unroll
       for (int i = 0; i < kCS; ++i) if (i < cn && nd[i] > 1) *(volatile unsigned*)&done[kk[i]] = epoch;
@@ -603,16 +675,17 @@ void fill_chains(Ctx& c) {
 void area_chains(Ctx& c) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_bu, c.nchains, c.ntickets_bu, c.nn};
-  k_area_chains<false><<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, c.precip, c.dx * c.dy,
-                                                                        c.a, c.ticket, c.done, c.epoch, c.d_err);
+  k_area_chains<<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don,
+                                                                 AreaFin{c.precip, c.dx * c.dy}, c.a, c.ticket,
+                                                                 c.done, c.epoch, c.d_err);
   c.count_launch();
 }
 
 void flux_chains(Ctx& c, double* flux) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_bu, c.nchains, c.ntickets_bu, c.nn};
-  k_area_chains<true><<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, c.erate, 1.0, flux,
-                                                                       c.ticket, c.done, c.epoch, c.d_err);
+  k_area_chains<<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, FluxFin{c.erate}, flux,
+                                                                 c.ticket, c.done, c.epoch, c.d_err);
   c.count_launch();
 }
 
@@ -628,9 +701,35 @@ void spl_chains(Ctx& c, double* hnew) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_td, c.nchains, c.ntickets_td, c.nn};
   const int n1 = fabs(c.n - 1.0) < 2.2250738585072014e-308;
-  k_spl_chains<<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.h, c.b, c.kf, c.a, c.length, c.kfsed, c.dt,
-                                                   c.m, c.n, 0.875 / c.n, n1, hnew, c.water, c.ticket, c.done,
-                                                   c.epoch, c.d_err);
+  k_spl_chains<false><<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(
+      cv, c.rec, c.ndon, c.h, c.b, c.kf, c.a, c.length, c.kfsed, c.dt, c.m, c.n, 0.875 / c.n, n1, hnew, c.water,
+      GsIo{nullptr, nullptr, nullptr, nullptr}, c.ticket, c.done, c.epoch, c.d_err);
+  c.count_launch();
+}
+
+void spl_chains_gs(Ctx& c, const double* elev, const double* hstart, double* hnew, int* sill, double* contrib) {
+  next_epoch(c);
+  ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_td, c.nchains, c.ntickets_td, c.nn};
+  const int n1 = fabs(c.n - 1.0) < 2.2250738585072014e-308;
+  k_spl_chains<true><<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(
+      cv, c.rec, c.ndon, c.h, c.b, c.kf, c.a, c.length, c.kfsed, c.dt, c.m, c.n, 0.875 / c.n, n1, hnew, c.water,
+      GsIo{elev, hstart, sill, contrib}, c.ticket, c.done, c.epoch, c.d_err);
+  c.count_launch();
+}
+
+void gs_erosion_chains(Ctx& c, const double* hp, const int* sill, double* lsed, double* dh) {
+  next_epoch(c);
+  ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_bu, c.nchains, c.ntickets_bu, c.nn};
+  k_area_chains<<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, GsFin{c.h, hp, sill, lsed},
+                                                                 dh, c.ticket, c.done, c.epoch, c.d_err);
+  c.count_launch();
+}
+
+void lake_volume_chains(Ctx& c, const int* sill, const double* contrib, double* vol, double* up) {
+  next_epoch(c);
+  ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_bu, c.nchains, c.ntickets_bu, c.nn};
+  k_area_chains<<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, VolFin{sill, contrib, vol},
+                                                                 up, c.ticket, c.done, c.epoch, c.d_err);
   c.count_launch();
 }
 

@@ -282,11 +282,18 @@ union LineWords {
 // k's dependents are its distinct receivers.  With `clamp` set and lines
 // built on erate it is compute_fluxes' sediment flux (FastScape_ctx.f90:871-877):
 // max(0, .) before the node's value goes downstream.
+// With `gs` set (lines built on e = ht - hp) it is the erosion sum of a
+// Gauss-Seidel iteration with g > 0 (StreamPowerLaw.f90:59-80): a sill's own
+// share is taken out and kept as lake_sediment; a root keeps its whole sum.
 struct AccMfdOp {
   const AccLine* line;
   int nx, ny;
   double* a;
   int clamp;
+  int gs = 0;
+  const int* rec = nullptr;
+  const int* sill = nullptr;
+  double* lsed = nullptr;
   __device__ void prefetch(int k) const { prefetch_l1(line + k); }
   __device__ int run(int k, int* dep, unsigned* pr, const Loc& loc) const {
     const LineWords<6> L(line + k);  // aw[0..7] = d[0..7], base = d[8], don = u[18], rcv = u[19], pr = s[40..47]
@@ -313,6 +320,16 @@ struct AccMfdOp {
     for (int t = 0; t < 8; ++t)
       if ((dc >> (4 * t)) & 15u) acc = acc + av[t] * L.d[t];
     if (clamp) acc = fmax(0.0, acc);
+    if (gs) {
+      if (rec[k] == k) {
+        lsed[k] = acc;
+      } else {
+        const double e = L.d[8];
+        const double t = acc - e;
+        if (sill[k] == k) lsed[k] = t <= 0.0 ? 0.0 : t;
+        acc = t + e;
+      }
+    }
     a[k] = acc;
     return nd;
   }
@@ -321,6 +338,10 @@ struct AccMfdOp {
 // implicit stream power law over the multiple receivers with g == 0
 // (StreamPowerLaw.f90:92-177): the new elevation and the water surface go to
 // hw[k] = (h, water); h keeps ht.  k's dependents are the donors that read it.
+// With GS (g > 0, StreamPowerLaw.f90:89-177 in a Gauss-Seidel iteration) the
+// surface comes from `elev`, Newton starts from the current iterate `hstart`,
+// and sill / contrib record the lake bookkeeping (as in k_spl_chains).
+template <bool GS>
 struct SplMfdOp {
   const SplLine* line;
   int nx, ny;
@@ -329,6 +350,10 @@ struct SplMfdOp {
   double omega;
   int n_is_one;
   double2* hw;
+  const double* elev = nullptr;
+  const double* hstart = nullptr;
+  int* sill = nullptr;
+  double* contrib = nullptr;
   __device__ int run(int k, int* dep, unsigned* pr, const Loc& loc) const {
     // fact = d[0..7], ht = d[8], q = u[18], dep = u[19], pr = s[40..47], meta = u[24]
     const LineWords<7> L(line + k);
@@ -346,17 +371,20 @@ struct SplMfdOp {
       }
     }
     double hk = ht, wk = ht;
+    int sk = k;
+    double ck = 0.0;
     const unsigned rcode = meta & 15u;
     if (rcode) {
       const int r = nb.at(rcode);
       double hq[8];
       const double wr = loc.ld(&hw[r].y, r);
+      if (GS) hk = hstart[k];
 #pragma unroll
       for (int t = 0; t < 8; ++t) {
         const unsigned c = (qc >> (4 * t)) & 15u;
         if (c) { const int q = nb.at(c); hq[t] = loc.ld(&hw[q].x, q); }
       }
-      const double elev = ht;
+      const double elev = GS ? this->elev[k] : ht;
       if (elev > wr) {
         if (meta & 16u) {  // mnrec(k) > 0
           if (n_is_one) {
@@ -392,10 +420,18 @@ struct SplMfdOp {
         if (hk < wr) hk = wr;
       } else {
         hk = elev;
+        if (GS) {
+          sk = __ldcg(&sill[r]);
+          ck = wr - hk;
+        }
       }
       wk = fmax(wr, hk);
     }
     hw[k] = make_double2(hk, wk);
+    if (GS) {
+      sill[k] = sk;
+      contrib[k] = ck;
+    }
     return nd;
   }
 };
@@ -904,6 +940,34 @@ void accumulate(Ctx& c) {
   run_sweep<FSB_LANES_ACC, FSB_SIDE_DIV_ACC>(c, AccMfdOp{line, c.nx, c.ny, c.a, 0}, c.cnt_acc);
 }
 
+void gs_erosion_mfd(Ctx& c, const double* e, const int* sill, double* lsed, double* dh) {
+  AccLine* line = static_cast<AccLine*>(c.mfd_line);
+  k_acc_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, 1.0, c.mrec, c.mnrec, c.mwrec, e, c.size, line,
+                                                     c.cnt_acc, c.d_err);
+  c.count_launch();
+  AccMfdOp op{line, c.nx, c.ny, dh, 0};
+  op.gs = 1;
+  op.rec = c.rec;
+  op.sill = sill;
+  op.lsed = lsed;
+  run_sweep<FSB_LANES_ACC, FSB_SIDE_DIV_ACC>(c, op, c.cnt_acc);
+}
+
+void spl_mfd_gs(Ctx& c, const double* elev, const double* hstart, int* sill, double* contrib) {
+  const int n1 = fabs(c.n - 1.0) < DBL_MIN;
+  SplLine* line = static_cast<SplLine*>(c.mfd_line);
+  k_spl_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec, c.mnrec, c.mwrec,
+                                                     c.mlrec, c.h, c.b, c.kf, c.a, c.size, line, c.cnt_spl, c.d_err);
+  c.count_launch();
+  SplMfdOp<true> op{line, c.nx, c.ny, NewtonPow{c.n, c.n == 1.5}, 0.875 / c.n, n1,
+                    reinterpret_cast<double2*>(c.hw)};
+  op.elev = elev;
+  op.hstart = hstart;
+  op.sill = sill;
+  op.contrib = contrib;
+  run_sweep<FSB_LANES_SPL, FSB_SIDE_DIV_SPL>(c, op, c.cnt_spl);
+}
+
 void flux_mfd(Ctx& c, double* flux) {
   AccLine* line = static_cast<AccLine*>(c.mfd_line);
   k_acc_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, 1.0, c.mrec, c.mnrec, c.mwrec, c.erate, c.size, line,
@@ -927,7 +991,8 @@ void stream_power(Ctx& c) {
                                                      c.mlrec, c.h, c.b, c.kf, c.a, c.size, line, c.cnt_spl, c.d_err);
   c.count_launch();
   double2* hw = reinterpret_cast<double2*>(c.hw);
-  run_sweep<FSB_LANES_SPL, FSB_SIDE_DIV_SPL>(c, SplMfdOp{line, c.nx, c.ny, NewtonPow{c.n, c.n == 1.5}, omega, n1, hw}, c.cnt_spl);
+  run_sweep<FSB_LANES_SPL, FSB_SIDE_DIV_SPL>(c, SplMfdOp<false>{line, c.nx, c.ny, NewtonPow{c.n, c.n == 1.5}, omega, n1, hw},
+                                             c.cnt_spl);
   k_spl_finish<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nn, c.dt, c.hw, 2, c.h, c.b, c.etot, c.erate, c.sedflux);
   c.count_launch();
 }

@@ -48,7 +48,10 @@ struct Ctx {
   double *etot = nullptr, *erate = nullptr, *a = nullptr, *length = nullptr, *lake_depth = nullptr;
   double *hwater = nullptr, *sedflux = nullptr;
   double *catch0 = nullptr, *catchv = nullptr;  // catchment seeds (SetUp) and labels (ctx:17,94)
-  double* red = nullptr;                         // 3*512 partial sums + 3 results (get_fluxes)
+  double* red = nullptr;                         // 3*512 partial sums + 3 results (reductions)
+  double* g = nullptr;                           // sediment parameter per node (ctx:17), kept across steps
+  bool g_positive = false;                       // max(g) > 0 at the last stream-power call
+  int ngs = 0;                                   // Gauss-Seidel iterations of the last call
   int *rec = nullptr, *ndon = nullptr, *don = nullptr /*8*nn*/, *stack = nullptr;
   int *pos = nullptr, *size = nullptr;
   int *mrec = nullptr /*8*nn*/, *mnrec = nullptr, *mstack = nullptr, *mdmask = nullptr;
@@ -158,6 +161,14 @@ void spl_chains(Ctx& c, double* hnew);
 void flux_chains(Ctx& c, double* flux);               // compute_fluxes' flux, single flow
 void chi_chains(Ctx& c, double a0, double mn, double* chi);
 void flux_mfd(Ctx& c, double* flux);                  // compute_fluxes' flux, multiple flow
+// the stream power law with the sediment term g > 0 (fsb_sediment.cu)
+bool gs_active(const Ctx& c);
+int stream_power_gs(Ctx& c);
+void spl_chains_gs(Ctx& c, const double* elev, const double* hstart, double* hnew, int* sill, double* contrib);
+void gs_erosion_chains(Ctx& c, const double* hp, const int* sill, double* lsed, double* dh);
+void lake_volume_chains(Ctx& c, const int* sill, const double* contrib, double* vol, double* up);
+void gs_erosion_mfd(Ctx& c, const double* e, const int* sill, double* lsed, double* dh);
+void spl_mfd_gs(Ctx& c, const double* elev, const double* hstart, int* sill, double* contrib);
 // derived fields (fsb_derived.cu)
 void catchment(Ctx& c);                               // catch = catch0 of the root, before LocalMinima
 void slope_field(Ctx& c, double* out);

@@ -97,6 +97,7 @@ for _n in ("fsb_copy_chi", "fsb_copy_slope", "fsb_copy_curvature"):
     _sig(_n, _vp, _vp, _i)
 _sig("fsb_get_fluxes", _vp, ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_d))
 _sig("fsb_set_all_layers", _vp, _vp, _i)
+_sig("fsb_get_gs_iterations", _vp, ctypes.POINTER(_i))
 _sig("fsb_view", _vp)
 _sig("fsb_debug", _vp)
 _sig("fsb_launch_count", _vp, res=ctypes.c_longlong)
@@ -319,6 +320,12 @@ class FastScape:
     def set_all_layers(self, dh) -> None:
         """FastScape_Set_All_Layers (api:680): h and basement += dh."""
         self._set(_lib.fsb_set_all_layers, dh)
+
+    def gs_iterations(self) -> int:
+        """Gauss-Seidel iterations of the last stream-power call (nGSStreamPowerLaw)."""
+        n = _i()
+        _check(_lib.fsb_get_gs_iterations(self._h, ctypes.byref(n)))
+        return n.value
 
     def view(self) -> None:
         """FastScape_View (api:188): prints a summary of the instance."""

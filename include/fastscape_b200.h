@@ -150,6 +150,9 @@ int fsb_get_fluxes(fsb_ctx* c, double* tectonic, double* erosion, double* bounda
 int fsb_set_all_layers(fsb_ctx* c, const double* dh, int where);
 /* FastScape_View (api:188 -> ctx:378-393) and FastScape_Debug (api:588 -> ctx:513-561):
    summaries printed to stdout */
+/* Gauss-Seidel iterations of the last stream-power call: the reference's
+   nGSStreamPowerLaw (ctx:15, StreamPowerLaw.f90:250-378); 1 when g = 0. */
+int fsb_get_gs_iterations(fsb_ctx* c, int* n);
 int fsb_view(fsb_ctx* c);
 int fsb_debug(fsb_ctx* c);
 int fsb_synchronize(fsb_ctx* c);

@@ -100,7 +100,7 @@ def test_failing_job_is_isolated():
     import fastscapelib_fortran as fs
     good = W.plain_d8(33, 33, seed=9, nsteps=2)
     bad = W.plain_d8(33, 33, seed=9, nsteps=2)
-    bad.g1 = 1.0  # the sediment term is not supported: the job must fail
+    bad.bc = 0  # no fixed boundary: LocalMinima has no outlet, the job must fail
     with fs.Batch(workers=2) as b:
         ids = [b.submit(good.job()), b.submit(bad.job()), b.submit(good.job())]
         j0 = b.wait(ids[0])

@@ -246,3 +246,126 @@ def test_derived_fields_match_literal(maker):
     O.fastscape_set_all_layers(dh)
     assert np.array_equal(O.copy_double("h"), h0 + dh)
     assert np.array_equal(O.copy_double("basement"), b0 + dh)
+
+
+def _literal_spl(sfd, h, b, ht_bc, rec, stack, mstack, a, length, mrec, mnrec, mwrec, mlrec, kf, kfsed,
+                 m, n, g1, g2, dt, dx, dy):
+    """StreamPowerLaw / StreamPowerLawSingleFlowDirection (StreamPowerLaw.f90:3-400)
+    with g > 0, statement for statement (0-based ids; lake_sill starts at -1)."""
+    nn = h.size
+    g = np.full(nn, g1)
+    if g2 > 0:
+        g[(h - b) > 1.0] = g2
+    kfint = kf.copy()
+    if kfsed > 0:
+        kfint[(h - b) > 1.0] = kfsed
+    tol = 1e-4 * (np.max(np.abs(h)) + 1.0)
+    err = 2.0 * tol
+    ht = h.copy()
+    h = h.copy()
+    ngs = 0
+    lsed = np.zeros(nn)
+    lsill = np.full(nn, -1)
+    water = np.zeros(nn)
+    lwv = np.zeros(nn)
+    elev = np.zeros(nn)
+    while err > tol and ngs < 99:
+        ngs += 1
+        hp = h.copy()
+        dh = ht - hp
+        order = stack[::-1] if sfd else mstack
+        for ijk in order:
+            if rec[ijk] != ijk:
+                dh[ijk] = dh[ijk] - (ht[ijk] - hp[ijk])
+                if lsill[ijk] == ijk:
+                    lsed[ijk] = 0.0 if dh[ijk] <= 0.0 else dh[ijk]
+                dh[ijk] = dh[ijk] + (ht[ijk] - hp[ijk])
+                if sfd:
+                    dh[rec[ijk]] = dh[rec[ijk]] + dh[ijk]
+                else:
+                    for k in range(mnrec[ijk]):
+                        dh[mrec[ijk, k]] = dh[mrec[ijk, k]] + dh[ijk] * mwrec[ijk, k]
+            else:
+                lsed[ijk] = dh[ijk]
+        for i in range(nn):
+            elev[i] = ht[i] if ht_bc[i] else ht[i] + (dh[i] - (ht[i] - hp[i])) * g[i] * dx * dy / a[i]
+        omega = 0.875 / n
+        for ijk in (stack if sfd else mstack[::-1]):
+            ijr = rec[ijk]
+            if ijr == ijk:
+                water[ijk] = ht[ijk]
+                lsill[ijk] = ijk
+                lwv[ijk] = 0.0
+                continue
+            w_rcv = water[ijr]
+            if elev[ijk] > w_rcv:
+                slots = [(ijr, length[ijk], 1.0)] if sfd else \
+                    [(mrec[ijk, k], mlrec[ijk, k], mwrec[ijk, k]) for k in range(mnrec[ijk])]
+                if slots:
+                    if abs(n - 1.0) < np.finfo(float).tiny:
+                        f, df = elev[ijk], 1.0
+                        for q, l, w in slots:
+                            if sfd or ht[ijk] >= ht[q]:
+                                fact = kfint[ijk] * dt * (a[ijk] * w) ** m / l if not sfd else \
+                                    kfint[ijk] * dt * a[ijk] ** m / l
+                                f = f + fact * h[q]
+                                df = df + fact
+                        h[ijk] = f / df
+                    else:
+                        errp, h0 = 2e-3, elev[ijk]
+                        while errp > 1e-3:
+                            f, df = h[ijk] - h0, 1.0
+                            for q, l, w in slots:
+                                if ht[ijk] > ht[q]:
+                                    fact = kfint[ijk] * dt * a[ijk] ** m / l ** n if sfd else \
+                                        kfint[ijk] * dt * (a[ijk] * w) ** m / l ** n
+                                    x = max(0.0, h[ijk] - h[q])
+                                    f = f + fact * x ** n
+                                    df = df + fact * n * x ** (n - 1.0)
+                            hn = h[ijk] - f / df
+                            errp = abs(hn - h[ijk])
+                            h[ijk] = h[ijk] * (1.0 - omega) + hn * omega
+                lsill[ijk] = ijk
+                lwv[ijk] = 0.0
+                if h[ijk] < w_rcv:
+                    h[ijk] = w_rcv
+            else:
+                h[ijk] = elev[ijk]
+                lsill[ijk] = lsill[ijr]
+                if lsill[ijk] != -1:
+                    lwv[lsill[ijk]] = lwv[lsill[ijk]] + (w_rcv - h[ijk])
+            water[ijk] = max(w_rcv, h[ijk])
+        err = np.sqrt(np.sum((h - hp) ** 2) / nn)
+        if np.max(g) < np.finfo(float).tiny:
+            err = 0.0
+    for ij in range(nn):
+        s = lsill[ij]
+        if s != -1 and lwv[s] > 0.0:
+            h[ij] = h[ij] + max(0.0, min(lsed[s], lwv[s])) / lwv[s] * (water[ij] - h[ij])
+    return h, ngs
+
+
+@pytest.mark.parametrize("sfd,n", [(True, 1.0), (True, 1.5), (False, 1.0), (False, 1.5)])
+def test_sediment_spl_matches_literal(sfd, n):
+    """The oracle's g > 0 stream power law against a literal transliteration:
+    with no uplift and no diffusion a step's change of h is the SPL alone."""
+    wl = W.plain_d8(19, 17, seed=51) if sfd else W.mfd(19, 17, seed=52, p=1.1, bc=1111)
+    wl.n, wl.g1, wl.g2 = n, 1.2, 0.0
+    wl.kf = np.full(wl.nn, (1e-4 if n == 1.0 else 2e-3) if sfd else 2e-5)
+    wl.u = np.zeros(wl.nn)
+    wl.kd = np.zeros(wl.nn)
+    wl.apply(O)
+    for _ in range(2):
+        O.fastscape_execute_step()
+    h0, b0 = O.copy_double("h"), O.copy_double("basement")
+    O.fastscape_execute_step()
+    bc = np.zeros((wl.ny, wl.nx), bool)
+    bc[0, :] = bc[-1, :] = bc[:, 0] = bc[:, -1] = True
+    dx, dy = wl.xl / (wl.nx - 1), wl.yl / (wl.ny - 1)
+    h_lit, ngs = _literal_spl(sfd, h0, b0, bc.ravel(), O.copy_int("rec"), O.copy_int("stack"),
+                              O.copy_int("mstack"), O.copy_double("drainage_area"),
+                              O.copy_double("length"), O.copy_slots("mrec"), O.copy_int("mnrec"),
+                              O.copy_slots("mwrec"), O.copy_slots("mlrec"), wl.kf, wl.kfsed, wl.m, n,
+                              wl.g1, wl.g2, wl.dt, dx, dy)
+    assert ngs == O.get_ngs() and ngs > 1
+    assert np.max(np.abs(O.copy_double("h") - h_lit)) <= 1e-12 * (np.abs(h_lit).max() + 1.0)
