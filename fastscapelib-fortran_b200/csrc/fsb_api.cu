@@ -159,7 +159,7 @@ size_t layout(fsb::Ctx& c, char* base) {
   c.done = L.take<unsigned>(N); c.ticket = L.take<unsigned>(4);
   c.water = L.take<double>(N); c.hnew = L.take<double>(N);
   c.catch0 = L.take<double>(N); c.catchv = L.take<double>(N); c.red = L.take<double>(3 * 512 + 8);
-  c.g = L.take<double>(N);
+  c.g = L.take<double>(N); c.vx = L.take<double>(N); c.vy = L.take<double>(N);
   c.dK = L.take<double>(N); c.dA = L.take<double>(N); c.dB = L.take<double>(N); c.dC = L.take<double>(N);
   c.dF = L.take<double>(N); c.dG = L.take<double>(N); c.dZ = L.take<double>(N);
   c.d_err = L.take<int>(4); c.d_cnt = L.take<int>(32);
@@ -226,7 +226,7 @@ int check_device_error(fsb::Ctx& c) {
   return 0;
 }
 
-enum { ST_UPLIFT, ST_RECEIVERS, ST_STACK, ST_LOCMIN, ST_FILL, ST_MFD, ST_ACCUM, ST_SPL, ST_DIFFUSION };
+enum { ST_UPLIFT, ST_RECEIVERS, ST_STACK, ST_LOCMIN, ST_FILL, ST_MFD, ST_ACCUM, ST_SPL, ST_DIFFUSION, ST_ADVECT };
 
 void stage_begin(fsb::Ctx& c, int s) {
   if (!c.profile) return;
@@ -257,6 +257,11 @@ void collect_stage_times(fsb::Ctx& c) {
 }
 
 int step_once(fsb::Ctx& c) {
+  if (c.runAdvect) {  // Advect first (FastScape_api.f90:209-214)
+    stage_begin(c, ST_ADVECT);
+    fsb::advect(c);
+    stage_end(c, ST_ADVECT);
+  }
   if (c.runUplift) {
     stage_begin(c, ST_UPLIFT);
     fsb::launch_uplift(c);
@@ -434,6 +439,7 @@ int fsb_setup(fsb_ctx* h, void* arena, size_t bytes) {
   c.routed = false;
   c.g_positive = false;
   c.ngs = 0;
+  c.runAdvect = false;
   c.setup_done = true;
   return 0;
 }
@@ -474,6 +480,13 @@ int fsb_set_erosional_parameters(fsb_ctx* h, const double* kf, double kfsed, dou
 int fsb_set_bc(fsb_ctx* h, int bc) {
   if (need_setup(h, "set_bc")) return 1;
   decode_bc(h->c, bc);
+  return 0;
+}
+
+int fsb_set_v(fsb_ctx* h, const double* vx, const double* vy, int where) {
+  if (need_setup(h, "SetV")) return 1;
+  if (upload(h->c, h->c.vx, vx, where) || upload(h->c, h->c.vy, vy, where)) return 1;
+  h->c.runAdvect = true;
   return 0;
 }
 
@@ -684,8 +697,8 @@ int fsb_debug(fsb_ctx* h) {
   std::printf(" Number of Gauss-Siedel iterations (SPL) %d\n", c.ngs);
   std::printf(" Timing (device milliseconds, accumulated while profiling is on):\n");
   static const char* names[] = {"Uplift", "Receivers", "Stack", "LocalMinima", "LakeFill", "MFDReceivers",
-                                "DrainageArea", "SPL", "Diffusion"};
-  for (int s = 0; s < fsb::Ctx::kStages && s < 9; ++s)
+                                "DrainageArea", "SPL", "Diffusion", "Advection"};
+  for (int s = 0; s < fsb::Ctx::kStages && s < 10; ++s)
     if (c.stage_calls[s]) std::printf(" %s: %.6g\n", names[s], c.stage_ms[s]);
   std::fflush(stdout);
   return 0;
@@ -842,6 +855,7 @@ void fastscape_get_sizes_(int* nnx, int* nny) { die_on(fsb_get_sizes(g_single, n
 void fastscape_get_step_(int* sstep) { die_on(fsb_get_step(g_single, sstep)); }
 void fastscape_set_bc_(const int* jbc) { die_on(fsb_set_bc(g_single, *jbc)); }
 void fastscape_set_u_(const double* up) { die_on(fsb_set_u(g_single, up, FSB_HOST)); }
+void fastscape_set_v_(const double* ux, const double* uy) { die_on(fsb_set_v(g_single, ux, uy, FSB_HOST)); }
 void fastscape_reset_cumulative_erosion_(void) { die_on(fsb_reset_cumulative_erosion(g_single)); }
 void fastscape_set_h_(double* hp) { die_on(fsb_set_h(g_single, hp, FSB_HOST)); }
 void fastscape_set_basement_(double* bp) { die_on(fsb_set_basement(g_single, bp, FSB_HOST)); }

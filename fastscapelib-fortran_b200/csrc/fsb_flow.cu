@@ -997,6 +997,13 @@ void stream_power(Ctx& c) {
   c.count_launch();
 }
 
+void thomas_lines(Ctx& c, int N, int L, int s0, int s1, const double* A, const double* B, const double* C, double* F,
+                  double* G) {
+  if (s1 <= s0) return;
+  k_thomas<<<(s1 - s0 + 31) / 32, 32, 0, c.stream>>>(N, L, s0, s1, A, B, C, F, G, c.d_err);
+  c.count_launch();
+}
+
 void diffusion(Ctx& c) {
   const int nx = c.nx, ny = c.ny, nn = c.nn;
   const double dt2 = c.dt / 2.0, dx2 = c.dx * c.dx, dy2 = c.dy * c.dy;

@@ -50,6 +50,8 @@ struct Ctx {
   double *catch0 = nullptr, *catchv = nullptr;  // catchment seeds (SetUp) and labels (ctx:17,94)
   double* red = nullptr;                         // 3*512 partial sums + 3 results (reductions)
   double* g = nullptr;                           // sediment parameter per node (ctx:17), kept across steps
+  double *vx = nullptr, *vy = nullptr;           // advection velocities (ctx:17, SetV)
+  bool runAdvect = false;
   bool g_positive = false;                       // max(g) > 0 at the last stream-power call
   int ngs = 0;                                   // Gauss-Seidel iterations of the last call
   int *rec = nullptr, *ndon = nullptr, *don = nullptr /*8*nn*/, *stack = nullptr;
@@ -121,7 +123,7 @@ struct Ctx {
   int nbasins = 0, basin0 = 0, nconn = 0, tree_size = 0, nlocmin_before = 0, nlocmin_after = 0;
 
   // per-stage device timing (CUDA events on the instance's stream)
-  static constexpr int kStages = 9;  // uplift receivers stack locmin fill mfd accum spl diffusion
+  static constexpr int kStages = 10;  // uplift receivers stack locmin fill mfd accum spl diffusion advection
   bool profile = false;
   cudaEvent_t ev_begin[kStages] = {}, ev_end[kStages] = {};
   bool ev_pending[kStages] = {};
@@ -161,6 +163,10 @@ void spl_chains(Ctx& c, double* hnew);
 void flux_chains(Ctx& c, double* flux);               // compute_fluxes' flux, single flow
 void chi_chains(Ctx& c, double a0, double mn, double* chi);
 void flux_mfd(Ctx& c, double* flux);                  // compute_fluxes' flux, multiple flow
+// tridiagonal systems s0..s1-1, element t of system s at [t*L + s], F solved in place
+void thomas_lines(Ctx& c, int N, int L, int s0, int s1, const double* A, const double* B, const double* C, double* F,
+                  double* G);
+void advect(Ctx& c);  // fsb_advect.cu
 // the stream power law with the sediment term g > 0 (fsb_sediment.cu)
 bool gs_active(const Ctx& c);
 int stream_power_gs(Ctx& c);

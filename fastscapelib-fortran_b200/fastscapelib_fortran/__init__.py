@@ -78,6 +78,7 @@ _sig("fsb_set_xl_yl", _vp, _d, _d)
 _sig("fsb_set_dt", _vp, _d)
 _sig("fsb_set_erosional_parameters", _vp, _vp, _d, _d, _d, _vp, _d, _d, _d, _d, _i)
 _sig("fsb_set_bc", _vp, _i)
+_sig("fsb_set_v", _vp, _vp, _vp, _i)
 for _n in ("fsb_set_u", "fsb_init_h", "fsb_set_h", "fsb_set_basement", "fsb_set_precip"):
     _sig(_n, _vp, _vp, _i)
 _sig("fsb_reset_cumulative_erosion", _vp)
@@ -113,7 +114,7 @@ _sig("fsb_batch_memory", _vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ct
 _sig("fsb_batch_destroy", _vp)
 
 STAGES = ("uplift", "receivers", "stack", "local_minima", "lake_fill", "mfd_receivers",
-          "drainage_area", "stream_power", "diffusion")
+          "drainage_area", "stream_power", "diffusion", "advection")
 
 
 def _check(rc: int) -> None:
@@ -242,6 +243,16 @@ class FastScape:
 
     def set_u(self, u) -> None:
         self._set(_lib.fsb_set_u, u)
+
+    def set_v(self, vx, vy) -> None:
+        """FastScape_Set_V (api:634): advection velocities; switches advection on."""
+        px, wx, kx = self._in(vx)
+        py, wy, ky = self._in(vy)
+        if wx != wy:
+            raise ValueError("vx and vy must both be host or both be device arrays")
+        _check(_lib.fsb_set_v(self._h, px, py, wx))
+        self._sync_if_device(wx)
+        del kx, ky
 
     def init_h(self, h) -> None:
         self._set(_lib.fsb_init_h, h)
@@ -637,6 +648,10 @@ def fastscape_copy_catchment(catchp):
 def fastscape_get_fluxes():
     """FastScape_Get_Fluxes (api:762); f2py returns the intent(out) scalars."""
     return _inst().get_fluxes()
+
+
+def fastscape_set_v(ux, uy):
+    _inst().set_v(ux, uy)
 
 
 def fastscape_set_all_layers(dhp):

@@ -95,6 +95,9 @@ int fsb_set_erosional_parameters(fsb_ctx* c, const double* kf, double kfsed, dou
 int fsb_set_bc(fsb_ctx* c, int bc);
 /* FastScape_Set_U (api:618 -> ctx:597-612) */
 int fsb_set_u(fsb_ctx* c, const double* u, int where);
+/* FastScape_Set_V (api:634 -> ctx:616-632): advection velocities vx, vy;
+   switches advection on (Advect.f90, run first in each step) */
+int fsb_set_v(fsb_ctx* c, const double* vx, const double* vy, int where);
 /* FastScape_Init_H (api:267 -> ctx:339-350): h and basement b */
 int fsb_init_h(fsb_ctx* c, const double* h, int where);
 /* FastScape_Set_H (api:664 -> ctx:636-644) */
@@ -162,7 +165,7 @@ long long fsb_launch_count(fsb_ctx* c);
    counterpart of the reference's cpu_time accumulators (api:209-257,
    ctx:27).  Stages: 0 uplift, 1 receivers, 2 stack, 3 LocalMinima, 4 lake
    fill, 5 multiple-flow receivers, 6 drainage area, 7 stream power law,
-   8 diffusion.  fsb_stage_times returns accumulated milliseconds and call
+   8 diffusion, 9 advection.  fsb_stage_times returns accumulated milliseconds and call
    counts for the first n stages and optionally resets them. */
 int fsb_set_profile(fsb_ctx* c, int on);
 int fsb_stage_times(fsb_ctx* c, double* ms, long long* calls, int n, int reset);
@@ -254,6 +257,7 @@ void fastscape_get_sizes_(int* nnx, int* nny);                     /* api:556 */
 void fastscape_get_step_(int* sstep);                              /* api:572 */
 void fastscape_set_bc_(const int* jbc);                            /* api:602 */
 void fastscape_set_u_(const double* up);                           /* api:618 */
+void fastscape_set_v_(const double* ux, const double* uy);         /* api:634 */
 void fastscape_reset_cumulative_erosion_(void);                    /* api:650 */
 void fastscape_set_h_(double* hp);                                 /* api:664 */
 void fastscape_set_basement_(double* bp);                          /* api:696 */

@@ -65,6 +65,8 @@ struct Ctx {
   int nGS = 0;
   dvec h, u, length, a, erate, etot, catchv, catch0, b, precip, kf, kd, sedflux, g, pmfd;
   dvec lake_depth, hwater;
+  dvec vx, vy;  // advection velocities (SetV, ctx:616-632)
+  bool runAdvect = false;
   ivec stack, ndon, rec, don;  // don(8,nn): don[(ij-1)*8 + k-1]
   ivec mnrec, mstack, mrec;
   dvec mwrec, mlrec;
@@ -873,7 +875,8 @@ bool diffusion(Ctx& c) {
 void alloc_all(Ctx& c) {
   const size_t n1 = (size_t)c.nn + 1, n8 = (size_t)c.nn * 8;
   for (dvec* v : {&c.h, &c.u, &c.length, &c.a, &c.erate, &c.etot, &c.catchv, &c.catch0, &c.b,
-                  &c.precip, &c.kf, &c.kd, &c.sedflux, &c.g, &c.pmfd, &c.lake_depth, &c.hwater})
+                  &c.precip, &c.kf, &c.kd, &c.sedflux, &c.g, &c.pmfd, &c.lake_depth, &c.hwater,
+                  &c.vx, &c.vy})
     v->assign(n1, 0.0);
   for (ivec* v : {&c.stack, &c.ndon, &c.rec, &c.mnrec, &c.mstack}) v->assign(n1, 0);
   c.don.assign(n8, 0);
@@ -881,6 +884,41 @@ void alloc_all(Ctx& c) {
   c.mwrec.assign(n8, 0.0);
   c.mlrec.assign(n8, 0.0);
   c.bc.assign(n1, 0);
+}
+
+// Advect -- Advect.f90:1-103: implicit upwind x-pass over every row, then
+// y-pass over every column, tridag for h, b and etot; then b = min(b, h).
+bool advect(Ctx& c) {
+  const int nx = c.nx, ny = c.ny;
+  const double dx = c.xl / (nx - 1), dy = c.yl / (ny - 1);
+  auto I = [nx](int i, int j) { return (size_t)(j - 1) * nx + i; };
+  auto pass = [&](int n, int lines, double d, const dvec& v, auto idx) {
+    dvec diag(n + 1), sup(n + 1), inf(n + 1), rhs(n + 1), res(n + 1), gam(n + 1);
+    for (int l = 1; l <= lines; ++l) {
+      for (int t = 1; t <= n; ++t) {
+        diag[t] = 1.0; sup[t] = 0.0; inf[t] = 0.0;
+        const double vv = v[idx(t, l)];
+        if (vv > 0.0) {
+          diag[t] = 1.0 + vv * c.dt / d;
+          inf[t] = -(vv * c.dt / d);
+        } else if (vv < 0.0) {
+          diag[t] = 1.0 - vv * c.dt / d;
+          sup[t] = vv * c.dt / d;
+        }
+      }
+      sup[1] = 0.0; diag[1] = 1.0; diag[n] = 1.0; inf[n] = 0.0;
+      for (dvec* f : {&c.h, &c.b, &c.etot}) {
+        for (int t = 1; t <= n; ++t) rhs[t] = (*f)[idx(t, l)];
+        if (!tridag(inf.data(), diag.data(), sup.data(), rhs.data(), res.data(), n, gam.data())) return false;
+        for (int t = 1; t <= n; ++t) (*f)[idx(t, l)] = res[t];
+      }
+    }
+    return true;
+  };
+  if (!pass(nx, ny, dx, c.vx, [&](int t, int l) { return I(t, l); })) return false;
+  if (!pass(ny, nx, dy, c.vy, [&](int t, int l) { return I(l, t); })) return false;
+  for (int i = 1; i <= c.nn; ++i) c.b[i] = std::min(c.b[i], c.h[i]);
+  return true;
 }
 
 // Stand-in for gfortran's random_number in SetUp (FastScape_ctx.f90:82,94): a
@@ -968,6 +1006,15 @@ int fso_set_bc(int jbc) {
 }
 
 // FastScape_Set_U -- api:618 -> ctx:597-612
+// FastScape_Set_V -- api:634 -> ctx:616-632
+int fso_set_v(const double* ux, const double* uy) {
+  Ctx& c = *C;
+  if (!c.setup_done) return fail("SetV - You need to run SetUp first");
+  for (int i = 1; i <= c.nn; ++i) { c.vx[i] = ux[i - 1]; c.vy[i] = uy[i - 1]; }
+  c.runAdvect = true;
+  return 0;
+}
+
 int fso_set_u(const double* up) {
   if (!C->setup_done) return fail("set_u - You need to run SetUp first");
   C->runUplift = true;
@@ -1008,6 +1055,7 @@ int fso_execute_step() {
   Ctx& c = *C;
   if (!c.setup_done) return fail("Execute_Step - You need to run SetUp first");
   c.err.clear();
+  if (c.runAdvect && !advect(c)) return fail("tridag failed");  // Advect first (api:209-214)
   if (c.runUplift) {  // Uplift.f90:9-10
     for (int i = 1; i <= c.nn; ++i) {
       const double du = c.u[i] * c.dt;

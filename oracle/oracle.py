@@ -62,6 +62,7 @@ def lib():
         L.fso_locmin_arrays.argtypes = [_I32P, _I32P, _I32P, _I32P, _F64P, _I32P, _I32P,
                                         _I32P, _I32P, _I32P, _I32P]
         L.fso_indexx.argtypes = [ctypes.c_int, _F64P, _I32P]
+        L.fso_set_v.argtypes = [_F64P, _F64P]
         for name in ("fso_copy_chi", "fso_copy_slope", "fso_copy_curvature", "fso_get_fluxes",
                      "fso_set_all_layers"):
             getattr(L, name).argtypes = [_F64P]
@@ -249,3 +250,8 @@ def fastscape_get_fluxes():
 def fastscape_set_all_layers(dh):
     """SetAllLayers (FastScape_ctx.f90:660-676) without stratigraphy."""
     _check(lib().fso_set_all_layers(_f64(dh, _nn())))
+
+
+def fastscape_set_v(ux, uy):
+    """FastScape_Set_V (api:634 -> ctx:616-632)."""
+    _check(lib().fso_set_v(_f64(ux, _nn()), _f64(uy, _nn())))

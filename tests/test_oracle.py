@@ -369,3 +369,75 @@ def test_sediment_spl_matches_literal(sfd, n):
                               wl.g1, wl.g2, wl.dt, dx, dy)
     assert ngs == O.get_ngs() and ngs > 1
     assert np.max(np.abs(O.copy_double("h") - h_lit)) <= 1e-12 * (np.abs(h_lit).max() + 1.0)
+
+
+def _tridag(a, b, c, r):
+    """tridag (Diffusion.f90:164-202), 0-based."""
+    n = len(b)
+    u, gam = np.zeros(n), np.zeros(n)
+    bet = b[0]
+    u[0] = r[0] / bet
+    for j in range(1, n):
+        gam[j] = c[j - 1] / bet
+        bet = b[j] - a[j] * gam[j]
+        u[j] = (r[j] - a[j] * u[j - 1]) / bet
+    for j in range(n - 2, -1, -1):
+        u[j] = u[j] - gam[j + 1] * u[j + 1]
+    return u
+
+
+def _literal_advect(h, b, etot, vx, vy, nx, ny, dx, dy, dt):
+    """Advect (Advect.f90:1-103) on (ny, nx) arrays."""
+    h, b, etot = h.reshape(ny, nx).copy(), b.reshape(ny, nx).copy(), etot.reshape(ny, nx).copy()
+    vx, vy = vx.reshape(ny, nx), vy.reshape(ny, nx)
+
+    def coefs(v, d):
+        n = v.size
+        diag, sup, inf = np.ones(n), np.zeros(n), np.zeros(n)
+        for i in range(n):
+            if v[i] > 0.0:
+                diag[i] = 1.0 + v[i] * dt / d
+                inf[i] = -(v[i] * dt / d)
+            elif v[i] < 0.0:
+                diag[i] = 1.0 - v[i] * dt / d
+                sup[i] = v[i] * dt / d
+        sup[0], diag[0], diag[-1], inf[-1] = 0.0, 1.0, 1.0, 0.0
+        return inf, diag, sup
+
+    for j in range(ny):
+        inf, diag, sup = coefs(vx[j, :], dx)
+        for f in (h, b, etot):
+            f[j, :] = _tridag(inf, diag, sup, f[j, :])
+    for i in range(nx):
+        inf, diag, sup = coefs(vy[:, i], dy)
+        for f in (h, b, etot):
+            f[:, i] = _tridag(inf, diag, sup, f[:, i])
+    return h.ravel(), np.minimum(b, h).ravel(), etot.ravel()
+
+
+def velocity_field(nx, ny, seed):
+    rng = np.random.default_rng(seed)
+    j, i = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    vx = 0.02 * np.sin(2 * np.pi * j / ny) + 0.005 * rng.standard_normal((ny, nx))
+    vy = 0.015 * np.cos(2 * np.pi * i / nx) + 0.005 * rng.standard_normal((ny, nx))
+    vx[:, nx // 3] = 0.0  # zero velocities take the diag = 1 branch
+    return vx.ravel(), vy.ravel()
+
+
+def test_advect_matches_literal():
+    """The oracle's Advect against a literal transliteration (no uplift, no
+    erosion, no diffusion: a step is the advection alone)."""
+    wl = W.plain_d8(23, 19, seed=61)
+    wl.kf = np.zeros(wl.nn)
+    wl.kd = np.zeros(wl.nn)
+    wl.u = np.zeros(wl.nn)
+    wl.apply(O)
+    vx, vy = velocity_field(wl.nx, wl.ny, 7)
+    O.fastscape_set_v(vx, vy)
+    h0, b0, e0 = O.copy_double("h"), O.copy_double("basement"), O.copy_double("total_erosion")
+    O.fastscape_execute_step()
+    dx, dy = wl.xl / (wl.nx - 1), wl.yl / (wl.ny - 1)
+    h, b, e = _literal_advect(h0, b0, e0, vx, vy, wl.nx, wl.ny, dx, dy, wl.dt)
+    assert np.array_equal(O.copy_double("h"), h)
+    assert np.array_equal(O.copy_double("basement"), b)
+    assert np.array_equal(O.copy_double("total_erosion"), e)
