@@ -647,6 +647,17 @@ void min_mean_max(const std::vector<double>& v, double& lo, double& mean, double
 }  // namespace
 }  // extern "C++"
 
+int fsb_vtk(fsb_ctx* h, const double* f, int where, double vex, const char* dir) {
+  if (need_setup(h, "VTK")) return 1;
+  fsb::Ctx& c = h->c;
+  const double* fd = f;
+  if (where != FSB_DEVICE) {
+    if (upload(c, c.dK, f, where)) return 1;
+    fd = c.dK;
+  }
+  return fsb::write_vtk(c, fd, vex, dir);
+}
+
 int fsb_get_gs_iterations(fsb_ctx* h, int* n) {
   if (!h || !n) return fail("null argument");
   *n = h->c.ngs;
@@ -867,6 +878,7 @@ void fastscape_copy_catchment_(double* p) { die_on(fsb_copy_field(g_single, FSB_
 void fastscape_get_fluxes_(double* t, double* e, double* b) { die_on(fsb_get_fluxes(g_single, t, e, b)); }
 void fastscape_set_all_layers_(double* dh) { die_on(fsb_set_all_layers(g_single, dh, FSB_HOST)); }
 void fastscape_view_(void) { die_on(fsb_view(g_single)); }
+void fastscape_vtk_(double* fp, double* vexp) { die_on(fsb_vtk(g_single, fp, FSB_HOST, *vexp, nullptr)); }
 void fastscape_debug_(void) { die_on(fsb_debug(g_single)); }
 
 }  // extern "C"

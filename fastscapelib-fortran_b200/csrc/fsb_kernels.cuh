@@ -167,6 +167,7 @@ void flux_mfd(Ctx& c, double* flux);                  // compute_fluxes' flux, m
 void thomas_lines(Ctx& c, int N, int L, int s0, int s1, const double* A, const double* B, const double* C, double* F,
                   double* G);
 void advect(Ctx& c);  // fsb_advect.cu
+int write_vtk(Ctx& c, const double* f_dev, double vex, const char* dir);  // fsb_vtk.cu
 // the stream power law with the sediment term g > 0 (fsb_sediment.cu)
 bool gs_active(const Ctx& c);
 int stream_power_gs(Ctx& c);

@@ -100,6 +100,7 @@ _sig("fsb_get_fluxes", _vp, ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINT
 _sig("fsb_set_all_layers", _vp, _vp, _i)
 _sig("fsb_get_gs_iterations", _vp, ctypes.POINTER(_i))
 _sig("fsb_view", _vp)
+_sig("fsb_vtk", _vp, _vp, _i, _d, ctypes.c_char_p)
 _sig("fsb_debug", _vp)
 _sig("fsb_launch_count", _vp, res=ctypes.c_longlong)
 _sig("fsb_set_profile", _vp, _i)
@@ -337,6 +338,14 @@ class FastScape:
         n = _i()
         _check(_lib.fsb_get_gs_iterations(self._h, ctypes.byref(n)))
         return n.value
+
+    def vtk(self, f, vex: float, directory: str | None = None) -> None:
+        """FastScape_VTK (api:728): legacy binary VTK files of the surface with
+        the scalar field f, in `directory` (default "VTK", as the reference)."""
+        ptr, where, keep = self._in(f)
+        _check(_lib.fsb_vtk(self._h, ptr, where, float(vex),
+                            None if directory is None else os.fsencode(directory)))
+        del keep
 
     def view(self) -> None:
         """FastScape_View (api:188): prints a summary of the instance."""
@@ -656,6 +665,11 @@ def fastscape_set_v(ux, uy):
 
 def fastscape_set_all_layers(dhp):
     _inst().set_all_layers(dhp)
+
+
+def fastscape_vtk(fp, vexp):
+    """FastScape_VTK (api:728); vexp may be a float or a 0-d array."""
+    _inst().vtk(fp, float(np.asarray(vexp)))
 
 
 def fastscape_view():

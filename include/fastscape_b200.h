@@ -153,6 +153,12 @@ int fsb_get_fluxes(fsb_ctx* c, double* tectonic, double* erosion, double* bounda
 int fsb_set_all_layers(fsb_ctx* c, const double* dh, int where);
 /* FastScape_View (api:188 -> ctx:378-393) and FastScape_Debug (api:588 -> ctx:513-561):
    summaries printed to stdout */
+/* FastScape_VTK (api:728 -> ctx:692-777): writes <dir>/Topography<step>.vtk
+   (and, for vex < 0, Basement<step>.vtk and SeaLevel<step>.vtk) in the legacy
+   binary VTK format with big-endian float32 data, exactly as the reference
+   built with -fconvert=big-endian; `f` is the extra scalar field (HHHHH),
+   `dir` NULL means "VTK" in the current directory, created if missing. */
+int fsb_vtk(fsb_ctx* c, const double* f, int where, double vex, const char* dir);
 /* Gauss-Seidel iterations of the last stream-power call: the reference's
    nGSStreamPowerLaw (ctx:15, StreamPowerLaw.f90:250-378); 1 when g = 0. */
 int fsb_get_gs_iterations(fsb_ctx* c, int* n);
@@ -270,6 +276,7 @@ void fastscape_get_fluxes_(double* ttectonic_flux, double* eerosion_flux,
                            double* bboundary_flux);                /* api:762 */
 void fastscape_set_all_layers_(double* dhp);                       /* api:680 */
 void fastscape_view_(void);                                        /* api:188 */
+void fastscape_vtk_(double* fp, double* vexp);                     /* api:728 */
 void fastscape_debug_(void);                                       /* api:588 */
 
 #ifdef __cplusplus

@@ -1297,6 +1297,58 @@ int fso_get_fluxes(double* out3) {
   return 0;
 }
 
+// Make_VTK -- FastScape_ctx.f90:692-777 with -fconvert=big-endian
+// (CMakeLists.txt:49): legacy binary VTK, big-endian float32.
+static void put_be(FILE* fp, double v) {
+  const float f = (float)v;
+  unsigned u;
+  std::memcpy(&u, &f, 4);
+  const unsigned char b[4] = {(unsigned char)(u >> 24), (unsigned char)(u >> 16), (unsigned char)(u >> 8),
+                              (unsigned char)u};
+  std::fwrite(b, 1, 4, fp);
+}
+static bool vtk_one(const Ctx& c, const std::string& path, const dvec* z, double zc, const char* name,
+                    const dvec* s1, double s1c, const double* f, double vex) {
+  FILE* fp = std::fopen(path.c_str(), "wb");
+  if (!fp) return false;
+  const double dx = c.xl / (c.nx - 1), dy = c.yl / (c.ny - 1);
+  char nxc[16], nyc[16], nnc[32];
+  std::snprintf(nxc, sizeof nxc, "%6d", c.nx);
+  std::snprintf(nyc, sizeof nyc, "%6d", c.ny);
+  std::snprintf(nnc, sizeof nnc, "%12d", c.nn);
+  std::fprintf(fp, "# vtk DataFile Version 3.0\nFastScape\nBINARY\nDATASET STRUCTURED_GRID\nDIMENSIONS %s %s 1\n"
+                   "POINTS%s float\n", nxc, nyc, nnc);
+  for (int j = 1; j <= c.ny; ++j)
+    for (int i = 1; i <= c.nx; ++i) {
+      put_be(fp, dx * (i - 1));
+      put_be(fp, dy * (j - 1));
+      put_be(fp, (z ? (*z)[i + (j - 1) * c.nx] : zc) * std::fabs(vex));
+    }
+  std::fprintf(fp, "POINT_DATA%s\n", nnc);
+  std::fprintf(fp, "SCALARS %s float 1\nLOOKUP_TABLE default\n", name);
+  for (int k = 1; k <= c.nn; ++k) put_be(fp, s1 ? (*s1)[k] : s1c);
+  if (f) {
+    std::fprintf(fp, "SCALARS HHHHH float 1\nLOOKUP_TABLE default\n");
+    for (int k = 0; k < c.nn; ++k) put_be(fp, f[k]);
+  }
+  return std::fclose(fp) == 0;
+}
+
+int fso_vtk(const double* f, double vex, const char* dir) {
+  Ctx& c = *C;
+  if (!c.setup_done) return fail("VTK - You need to run SetUp first");
+  const std::string d = dir;
+  char cstep[16];
+  std::snprintf(cstep, sizeof cstep, "%07d", c.step);
+  if (!vtk_one(c, d + "/Topography" + cstep + ".vtk", &c.h, 0.0, "H", &c.h, 0.0, f, vex)) return fail("VTK write");
+  if (vex < 0.0) {
+    if (!vtk_one(c, d + "/Basement" + cstep + ".vtk", &c.b, 0.0, "B", &c.b, 0.0, f, vex)) return fail("VTK write");
+    if (!vtk_one(c, d + "/SeaLevel" + cstep + ".vtk", nullptr, c.sealevel, "SL", nullptr, c.sealevel, nullptr, vex))
+      return fail("VTK write");
+  }
+  return 0;
+}
+
 // SetAllLayers -- FastScape_ctx.f90:660-676 (no stratigraphy): h, b += dh
 int fso_set_all_layers(const double* dh) {
   Ctx& c = *C;

@@ -63,6 +63,7 @@ def lib():
                                         _I32P, _I32P, _I32P, _I32P]
         L.fso_indexx.argtypes = [ctypes.c_int, _F64P, _I32P]
         L.fso_set_v.argtypes = [_F64P, _F64P]
+        L.fso_vtk.argtypes = [_F64P, ctypes.c_double, ctypes.c_char_p]
         for name in ("fso_copy_chi", "fso_copy_slope", "fso_copy_curvature", "fso_get_fluxes",
                      "fso_set_all_layers"):
             getattr(L, name).argtypes = [_F64P]
@@ -255,3 +256,8 @@ def fastscape_set_all_layers(dh):
 def fastscape_set_v(ux, uy):
     """FastScape_Set_V (api:634 -> ctx:616-632)."""
     _check(lib().fso_set_v(_f64(ux, _nn()), _f64(uy, _nn())))
+
+
+def fastscape_vtk(fp, vexp, directory="VTK"):
+    """Make_VTK (FastScape_ctx.f90:692-777); the directory must exist."""
+    _check(lib().fso_vtk(_f64(fp, _nn()), float(vexp), os.fsencode(directory)))

@@ -441,3 +441,42 @@ def test_advect_matches_literal():
     assert np.array_equal(O.copy_double("h"), h)
     assert np.array_equal(O.copy_double("basement"), b)
     assert np.array_equal(O.copy_double("total_erosion"), e)
+
+
+def literal_vtk_bytes(nx, ny, xl, yl, step, z, scal_name, scal, f, vex):
+    """The bytes of one Make_VTK file (FastScape_ctx.f90:692-777), gfortran
+    with -fconvert=big-endian (CMakeLists.txt:49)."""
+    import struct
+    nn = nx * ny
+    dx, dy = xl / (nx - 1), yl / (ny - 1)
+    nnc = "%12d" % nn
+    out = bytearray(("# vtk DataFile Version 3.0\nFastScape\nBINARY\nDATASET STRUCTURED_GRID\n"
+                     "DIMENSIONS %6d %6d 1\nPOINTS%s float\n" % (nx, ny, nnc)).encode())
+    pts = np.empty((nn, 3), dtype=np.float64)
+    ii, jj = np.meshgrid(np.arange(nx), np.arange(ny))
+    pts[:, 0] = dx * ii.ravel()
+    pts[:, 1] = dy * jj.ravel()
+    pts[:, 2] = z * abs(vex)
+    out += pts.astype(">f4").tobytes()
+    out += ("POINT_DATA%s\n" % nnc).encode()
+    out += ("SCALARS %s float 1\nLOOKUP_TABLE default\n" % scal_name).encode()
+    out += np.asarray(scal, dtype=np.float64).astype(">f4").tobytes()
+    if f is not None:
+        out += b"SCALARS HHHHH float 1\nLOOKUP_TABLE default\n"
+        out += np.asarray(f, dtype=np.float64).astype(">f4").tobytes()
+    assert struct.calcsize(">f") == 4
+    return bytes(out)
+
+
+def test_vtk_matches_literal(tmp_path):
+    wl = W.plain_d8(13, 11, seed=81)
+    wl.apply(O)
+    O.fastscape_execute_step()
+    f = np.random.default_rng(3).standard_normal(wl.nn) * 1e3
+    O.fastscape_vtk(f, -2.0, str(tmp_path))
+    h, b = O.copy_double("h"), O.copy_double("basement")
+    args = (wl.nx, wl.ny, wl.xl, wl.yl, 1)
+    assert (tmp_path / "Topography0000001.vtk").read_bytes() == literal_vtk_bytes(*args, h, "H", h, f, -2.0)
+    assert (tmp_path / "Basement0000001.vtk").read_bytes() == literal_vtk_bytes(*args, b, "B", b, f, -2.0)
+    zero = np.zeros(wl.nn)
+    assert (tmp_path / "SeaLevel0000001.vtk").read_bytes() == literal_vtk_bytes(*args, zero, "SL", zero, None, -2.0)
