@@ -134,6 +134,26 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+# ranks: independent replicas, one per GPU, timed as the slowest rank
+
+def max_over_ranks(times_ms, device, world):
+    """Every rank's times, reduced with MAX over the process group (world > 1)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x) for x in times_ms], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    return [float(x) for x in t]
+
+
+def replica_throughput(nn, steps, world, ms_max):
+    """Whole-job node-steps/s: every rank stepped its own nn-node grid `steps`
+    times; the job took as long as the slowest rank."""
+    return nn * steps * world / (ms_max / 1e3)
+
+
+# ---------------------------------------------------------------------------
 # GPU arm
 
 class ClockSampler:
@@ -269,14 +289,9 @@ def run_gpu(args):
     torch.cuda.synchronize()
     e2e_ms = max(f0.elapsed_time(f1), 1e3 * (time.perf_counter() - t0))
 
-    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.barrier()
-    ms_max, e2e_max = float(t[0]), float(t[1])
-    nodes = wl.nn * args.steps * world
-    value = nodes / (ms_max / 1e3)
-    e2e_val = nodes / (e2e_max / 1e3)
+    ms_max, e2e_max = max_over_ranks([ms, e2e_ms], dev, world)
+    value = replica_throughput(wl.nn, args.steps, world, ms_max)
+    e2e_val = replica_throughput(wl.nn, args.steps, world, e2e_max)
 
     if rank == 0:
         mnrec = g.copy_int("mnrec")
