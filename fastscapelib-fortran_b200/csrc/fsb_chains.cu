@@ -157,9 +157,14 @@ __global__ void k_chain_list(int nn, const int* __restrict__ flag, const int* __
   }
 }
 
+// The light-depth histogram is counted per block in shared memory (few
+// distinct depths: one global atomic per block and depth, not per chain).
 __global__ void k_chain_keys(int nn, int nchains, const int* __restrict__ cstart, const int* __restrict__ ord,
                              const int* __restrict__ ldep, unsigned* __restrict__ key_td,
                              unsigned* __restrict__ key_bu, int* __restrict__ hist_td, int* __restrict__ hist_bu) {
+  __shared__ int sh[64];
+  for (int t = threadIdx.x; t < 64; t += blockDim.x) sh[t] = 0;
+  __syncthreads();
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nchains; c += gridDim.x * blockDim.x) {
     const int s = cstart[c];
     const int e = (c + 1 < nchains) ? cstart[c + 1] : nn;
@@ -169,9 +174,14 @@ __global__ void k_chain_keys(int nn, int nchains, const int* __restrict__ cstart
     const unsigned inv = 0x3ffffffu - (len > 0x3ffffffu ? 0x3ffffffu : len);
     key_td[c] = ((unsigned)ld << 26) | inv;
     key_bu[c] = ((unsigned)(63 - ld) << 26) | inv;
-    atomicAdd(&hist_td[ld], 1);
-    atomicAdd(&hist_bu[63 - ld], 1);
+    atomicAdd(&sh[ld], 1);
   }
+  __syncthreads();
+  for (int t = threadIdx.x; t < 64; t += blockDim.x)
+    if (sh[t]) {
+      atomicAdd(&hist_td[t], sh[t]);
+      atomicAdd(&hist_bu[63 - t], sh[t]);
+    }
 }
 
 // per-group offsets, padded to multiples of 32 (one thread)
@@ -604,15 +614,16 @@ void build_chains(Ctx& c) {
   c.count_launch();
   unsigned long long *va = c.ch_val, *vb = c.ch_val2;
   int *na = c.ch_nxt, *nb = c.ch_nxt2;
-  for (int round = 0; round < 40; ++round) {
+  // pointer jumping; the flag read back every 4 rounds says whether any
+  // pointer moved in them (rounds after convergence change nothing)
+  for (int round = 0; round < 20; ++round) {
     cudaMemsetAsync(c.d_cnt + 16, 0, sizeof(int), st);
-    k_path_jump<<<grid1d(nn), kBlock, 0, st>>>(nn, va, na, vb, nb, c.d_cnt + 16);
-    std::swap(va, vb);
-    std::swap(na, nb);
-    k_path_jump<<<grid1d(nn), kBlock, 0, st>>>(nn, va, na, vb, nb, c.d_cnt + 16);
-    std::swap(va, vb);
-    std::swap(na, nb);
-    c.count_launch(2);
+    for (int r = 0; r < 4; ++r) {
+      k_path_jump<<<grid1d(nn), kBlock, 0, st>>>(nn, va, na, vb, nb, c.d_cnt + 16);
+      std::swap(va, vb);
+      std::swap(na, nb);
+    }
+    c.count_launch(4);
     fetch_counters(c, 20);
     if (!c.h_cnt[16]) break;
   }

@@ -686,17 +686,22 @@ bool local_minima(Ctx& c) {
                                                    c.mst_next, c.e_inmst, c.d_cnt);
     k_mst_apply<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_next, c.mst_comp);
     c.count_launch(4);
-    fetch_counters(c, 12);
-    if (!c.h_cnt[C_CHANGED]) break;
-    // flatten the hook forest: comp[c] <- root of c
-    for (int jr = 0; jr < 40; ++jr) {
+    // flatten the hook forest: comp[c] <- root of c, four jumps per read-back
+    // (jumps on a flat forest change nothing); the first read-back also
+    // brings the round's "changed" flag
+    bool changed = true;
+    for (int jr = 0; jr < 20; ++jr) {
       cudaMemsetAsync(c.d_cnt + C_NOTFLAT, 0, sizeof(int), st);
-      k_mst_jump<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_comp, c.mst_next, c.d_cnt);
-      k_mst_jump<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_next, c.mst_comp, c.d_cnt);
-      c.count_launch(2);
+      for (int r = 0; r < 2; ++r) {
+        k_mst_jump<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_comp, c.mst_next, c.d_cnt);
+        k_mst_jump<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_next, c.mst_comp, c.d_cnt);
+      }
+      c.count_launch(4);
       fetch_counters(c, 12);
+      if (jr == 0 && !c.h_cnt[C_CHANGED]) { changed = false; break; }
       if (!c.h_cnt[C_NOTFLAT]) break;
     }
+    if (!changed) break;
   }
   k_tree_flags<<<grid1d(ne + 1), kBlock, 0, st>>>(ne, c.nr_idx, c.e_inmst, c.nr_lf);
   c.count_launch();
