@@ -31,7 +31,7 @@ namespace {
 
 enum {
   C_NBASINS = 0, C_NLOCMIN = 1, C_BASIN0 = 2, C_NEDGE = 3, C_NSEG = 4, C_NSMALL = 5,
-  C_CHANGED = 6, C_NTREE = 7, C_NLOCMIN_AFTER = 8, C_OVERFLOW = 9, C_NOTFLAT = 10
+  C_CHANGED = 6, C_NTREE = 7, C_NLOCMIN_AFTER = 8, C_OVERFLOW = 9, C_NOTFLAT = 10, C_NSEG2 = 11
 };
 
 __constant__ int c_ii[8] = {-1, 1, 0, 0, -1, 1, -1, 1};
@@ -214,8 +214,9 @@ __global__ void k_nr_init(int n, int* __restrict__ idx, int* __restrict__ segof,
 __device__ inline void iswap(int* v, int a, int b) { const int t = v[a]; v[a] = v[b]; v[b] = t; }
 
 // median of three (LocalMinima.f90:985-1006)
-__global__ void k_nr_median(int nseg, const int* __restrict__ seg, const double* __restrict__ arr,
+__global__ void k_nr_median(const int* __restrict__ nsegp, const int* __restrict__ seg, const double* __restrict__ arr,
                             int* __restrict__ idx, double* __restrict__ piv, int* __restrict__ meta) {
+  const int nseg = *nsegp;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
     const int l = seg[2 * s], ir = seg[2 * s + 1];
     const int k = (l + ir) / 2;
@@ -262,9 +263,10 @@ __global__ void k_nr_scatter(int n, const int* __restrict__ lf, const int* __res
 // partition swaps (L_t, R_t) for every t < T, T = min{t : L_t >= R_t}.  If
 // L_T == R_T = P the scans stop at i=P+1, j=P-1; otherwise at
 // i = min(L_T, R_{T-1}), j = max(R_T, L_{T-1}) (R_0 = +inf, L_0 = -inf).
-__global__ void k_nr_cross(int nseg, const int* __restrict__ seg, const int* __restrict__ ls,
+__global__ void k_nr_cross(const int* __restrict__ nsegp, const int* __restrict__ seg, const int* __restrict__ ls,
                            const int* __restrict__ rs, const int* __restrict__ lpos,
                            const int* __restrict__ rpos, int* __restrict__ meta) {
+  const int nseg = *nsegp;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
     const int l = seg[2 * s], ir = seg[2 * s + 1];
     const int lb = ls[l + 2], nL = ls[ir + 1] - ls[l + 2];
@@ -323,9 +325,12 @@ __global__ void k_nr_apply(int n, const int* __restrict__ segof, const int* __re
 
 // children segments [l, j-1] and [i, ir]: partitioned further when they hold
 // at least M+1=8 elements, insertion-sorted otherwise
-__global__ void k_nr_newsegs(int nseg, const int* __restrict__ seg, int* __restrict__ meta,
+// reads the level's segment count from cnt[in_slot] and counts the next
+// level's segments in cnt[out_slot] (zeroed before the launch)
+__global__ void k_nr_newsegs(int in_slot, int out_slot, const int* __restrict__ seg, int* __restrict__ meta,
                              int* __restrict__ seg2, int* __restrict__ small, int* __restrict__ cnt,
                              int small_cap) {
+  const int nseg = cnt[in_slot];
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
     const int l = seg[2 * s], ir = seg[2 * s + 1];
     const int i = meta[4 * s + 1], j = meta[4 * s + 2];
@@ -333,7 +338,7 @@ __global__ void k_nr_newsegs(int nseg, const int* __restrict__ seg, int* __restr
     const int lo[2] = {l, i}, hi[2] = {j - 1, ir};
     for (int c = 0; c < 2; ++c) {
       if (hi[c] - lo[c] >= 7) {
-        const int id = atomicAdd(&cnt[C_NSEG], 1);
+        const int id = atomicAdd(&cnt[out_slot], 1);
         seg2[2 * id] = lo[c];
         seg2[2 * id + 1] = hi[c];
         ids[c] = id;
@@ -576,25 +581,35 @@ static bool nr_indexx(Ctx& c, int n, const double* w) {
   c.count_launch();
   fetch_counters(c, 10);
   int nseg = c.h_cnt[C_NSEG];
+  // Levels run with the segment count on the device (slot `in` of d_cnt), a
+  // few levels per read-back: a level with no segment left changes nothing.
+  // Every segment holds at least 8 elements, so a level has at most n/8.
+  const unsigned gseg = grid1d((size_t)n / 8 + 1);
+  int in = C_NSEG, out = C_NSEG2;
   int levels = 0;
   while (nseg > 0) {
-    if (++levels > 200) { c.err = "NR sort emulation: too many levels"; return false; }
-    k_nr_median<<<grid1d(nseg), kBlock, 0, c.stream>>>(nseg, seg, arr, idx, c.nr_piv, c.nr_segmeta);
-    k_nr_flags<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, c.nr_segof, seg, c.nr_piv, arr, idx, c.nr_lf, c.nr_rf);
-    exclusive_scan_int(c, c.nr_lf, c.nr_ls, n + 2);
-    exclusive_scan_int(c, c.nr_rf, c.nr_rs, n + 2);
-    k_nr_scatter<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, c.nr_lf, c.nr_rf, c.nr_ls, c.nr_rs, c.nr_lpos, c.nr_rpos);
-    k_nr_cross<<<grid1d(nseg), kBlock, 0, c.stream>>>(nseg, seg, c.nr_ls, c.nr_rs, c.nr_lpos, c.nr_rpos, c.nr_segmeta);
-    k_nr_apply<<<grid1d(n + 1), kBlock, 0, c.stream>>>(n, c.nr_segof, seg, c.nr_segmeta, idx, c.nr_lf, c.nr_rf,
-                                                        c.nr_ls, c.nr_rs, c.nr_lpos, c.nr_rpos, idx2);
-    std::swap(idx, idx2);
-    cudaMemsetAsync(c.d_cnt + C_NSEG, 0, sizeof(int), c.stream);
-    k_nr_newsegs<<<grid1d(nseg), kBlock, 0, c.stream>>>(nseg, seg, c.nr_segmeta, seg2, c.nr_small, c.d_cnt, small_cap);
-    k_nr_segof<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, seg, c.nr_segmeta, c.nr_segof);
-    c.count_launch(7);
-    std::swap(seg, seg2);
-    fetch_counters(c, 10);
-    nseg = c.h_cnt[C_NSEG];
+    for (int b = 0; b < 4; ++b) {
+      if (++levels > 200) { c.err = "NR sort emulation: too many levels"; return false; }
+      const int* nsegp = c.d_cnt + in;
+      k_nr_median<<<gseg, kBlock, 0, c.stream>>>(nsegp, seg, arr, idx, c.nr_piv, c.nr_segmeta);
+      k_nr_flags<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, c.nr_segof, seg, c.nr_piv, arr, idx, c.nr_lf, c.nr_rf);
+      exclusive_scan_int(c, c.nr_lf, c.nr_ls, n + 2);
+      exclusive_scan_int(c, c.nr_rf, c.nr_rs, n + 2);
+      k_nr_scatter<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, c.nr_lf, c.nr_rf, c.nr_ls, c.nr_rs, c.nr_lpos,
+                                                            c.nr_rpos);
+      k_nr_cross<<<gseg, kBlock, 0, c.stream>>>(nsegp, seg, c.nr_ls, c.nr_rs, c.nr_lpos, c.nr_rpos, c.nr_segmeta);
+      k_nr_apply<<<grid1d(n + 1), kBlock, 0, c.stream>>>(n, c.nr_segof, seg, c.nr_segmeta, idx, c.nr_lf, c.nr_rf,
+                                                          c.nr_ls, c.nr_rs, c.nr_lpos, c.nr_rpos, idx2);
+      std::swap(idx, idx2);
+      cudaMemsetAsync(c.d_cnt + out, 0, sizeof(int), c.stream);
+      k_nr_newsegs<<<gseg, kBlock, 0, c.stream>>>(in, out, seg, c.nr_segmeta, seg2, c.nr_small, c.d_cnt, small_cap);
+      k_nr_segof<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, seg, c.nr_segmeta, c.nr_segof);
+      c.count_launch(7);
+      std::swap(seg, seg2);
+      std::swap(in, out);
+    }
+    fetch_counters(c, 12);
+    nseg = c.h_cnt[in];
     if (c.h_cnt[C_OVERFLOW]) { c.err = "NR sort emulation: small-segment buffer overflow"; return false; }
   }
   const int nsmall = c.h_cnt[C_NSMALL];
