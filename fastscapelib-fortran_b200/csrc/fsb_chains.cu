@@ -552,6 +552,9 @@ __global__ void __launch_bounds__(128) k_spl_chains(ChainView cv, const int* __r
                   if (n == 1.5) {  // x^1.5 = x*sqrt(x), x^0.5 = sqrt(x)
                     pn1 = sqrt(x);
                     pn = x * pn1;
+                  } else if (x > 0.0) {  // one pow: x^n = x * x^(n-1)
+                    pn1 = pow(x, n - 1.0);
+                    pn = x * pn1;
                   } else {
                     pn = pow(x, n);
                     pn1 = pow(x, n - 1.0);

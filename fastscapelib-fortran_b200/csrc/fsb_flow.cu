@@ -246,8 +246,10 @@ struct NbrDecoder {
   }
 };
 
-// x^n and n*x^(n-1) for the Newton update.  For n = 1.5 they are evaluated
-// as x*sqrt(x) and 1.5*sqrt(x) (sqrt is correctly rounded); otherwise with pow.
+// x^n and x^(n-1) for the Newton update.  For n = 1.5 they are evaluated as
+// x*sqrt(x) and sqrt(x) (sqrt is correctly rounded); otherwise as x*x^(n-1)
+// and x^(n-1) with one pow for x > 0 (within an ulp or two of pow(x, n)), and
+// with two pows at x = 0.
 struct NewtonPow {
   double n;
   int half3;  // n == 1.5
@@ -256,6 +258,9 @@ struct NewtonPow {
       const double r = sqrt(x);
       pn = x * r;
       pn1 = r;
+    } else if (x > 0.0) {
+      pn1 = pow(x, n - 1.0);
+      pn = x * pn1;
     } else {
       pn = pow(x, n);
       pn1 = pow(x, n - 1.0);
