@@ -437,6 +437,8 @@ int fsb_setup(fsb_ctx* h, void* arena, size_t bytes) {
   c.p = 1.0;
   c.step = 0;
   c.routed = false;
+  c.precip_uniform = true;
+  c.precip_value = 1.0;
   c.g_positive = false;
   c.ngs = 0;
   c.runAdvect = false;
@@ -515,7 +517,18 @@ int fsb_set_basement(fsb_ctx* h, const double* bp, int where) {
 
 int fsb_set_precip(fsb_ctx* h, const double* pp, int where) {
   if (need_setup(h, "SetPrecip")) return 1;
-  return upload(h->c, h->c.precip, pp, where);
+  fsb::Ctx& c = h->c;
+  if (upload(c, c.precip, pp, where)) return 1;
+  // remember whether the field is uniform (the single-flow area then has an
+  // exact closed form, see fsb::accumulate)
+  std::vector<double> v(c.nn);
+  FSB_CUDA(cudaMemcpyAsync(v.data(), c.precip, sizeof(double) * c.nn, cudaMemcpyDeviceToHost, c.stream));
+  FSB_CUDA(cudaStreamSynchronize(c.stream));
+  bool uni = true;
+  for (int k = 1; k < c.nn && uni; ++k) uni = std::memcmp(&v[k], &v[0], sizeof(double)) == 0;
+  c.precip_uniform = uni;
+  c.precip_value = v.empty() ? 1.0 : v[0];
+  return 0;
 }
 
 int fsb_reset_cumulative_erosion(fsb_ctx* h) {

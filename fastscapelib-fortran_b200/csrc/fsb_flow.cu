@@ -933,9 +933,40 @@ static void run_sweep(Ctx& c, Op op, const int* cnt0) {
 
 void fill_sweep(Ctx& c) { fill_chains(c); }
 
+// Single-flow area with uniform precipitation P: the reference's loop
+// (FlowRouting.f90:133-139) adds multiples m*v of v = dx*dy*P, m <= 2*nn.  When
+// v's odd significand M has M*2*nn <= 2^53, every such partial sum is exact,
+// so a(k) = v*size(k) (doubled at a root) bit for bit, whatever the order.
+static bool exact_size_area(const Ctx& c, double& v) {
+  if (!c.precip_uniform) return false;
+  v = c.dx * c.dy * c.precip_value;
+  if (!std::isfinite(v)) return false;
+  if (v == 0.0) return true;
+  int e = 0;
+  const double f = std::frexp(std::fabs(v), &e);               // v = f * 2^e, f in [0.5, 1)
+  unsigned long long M = (unsigned long long)std::ldexp(f, 53);  // exact: f has at most 53 bits
+  while (!(M & 1ull)) M >>= 1;
+  return (double)M * 2.0 * (double)c.nn <= 9007199254740992.0;
+}
+
+__global__ void k_area_from_size(int nn, double v, const int* __restrict__ size, const int* __restrict__ rec,
+                                 double* __restrict__ a) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    double x = v * (double)size[k];
+    if (rec[k] == k) x = x + x;
+    a[k] = x;
+  }
+}
+
 void accumulate(Ctx& c) {
   if (c.sfd) {
-    area_chains(c);
+    double v = 0.0;
+    if (exact_size_area(c, v)) {
+      k_area_from_size<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nn, v, c.size, c.rec, c.a);
+      c.count_launch();
+    } else {
+      area_chains(c);
+    }
     return;
   }
   AccLine* line = static_cast<AccLine*>(c.mfd_line);

@@ -33,6 +33,8 @@ struct Ctx {
   bool setup_done = false;
   bool capture = false;  // keep LocalMinima intermediates of the last step
   bool routed = false;   // a step has built receivers, stack, chains and area
+  bool precip_uniform = true;  // every node has precipitation precip_value (SetUp: 1)
+  double precip_value = 1.0;
   int step = 0;
   cudaStream_t stream = 0;
   long long launches = 0;  // kernels launched by this instance

@@ -178,3 +178,23 @@ def test_reference_api_drop_in():
     fs.fastscape_copy_h(ht)
     assert np.array_equal(ht.cpu().numpy(), hg)  # device copy-out equals host copy-out
     fs.fastscape_destroy()
+
+
+@pytest.mark.parametrize("precip", ["uniform", "random", "uniform_long_significand"])
+def test_sfd_area_is_bit_exact(precip):
+    """Single-flow drainage area equals the oracle's bit for bit on both of its
+    paths: the closed form v*subtree_size (uniform precipitation, v = dx*dy*P
+    with a short significand) and the bottom-up chain sweep (otherwise)."""
+    wl = W.plain_d8(83, 71, seed=17)
+    wl.apply(O)
+    g = make_gpu(wl)
+    if precip != "uniform":
+        p = (np.random.default_rng(4).random(wl.nn) + 0.5 if precip == "random"
+             else np.full(wl.nn, 1.0 / 3.0))
+        O.fastscape_set_precip(p)
+        g.set_precip(p)
+    for _ in range(3):
+        resync(g)
+        O.fastscape_execute_step()
+        g.execute_step()
+        assert np.array_equal(gpu_float(g, "drainage_area"), O.copy_double("drainage_area"))
