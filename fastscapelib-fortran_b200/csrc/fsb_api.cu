@@ -139,6 +139,7 @@ size_t layout(fsb::Ctx& c, char* base) {
   c.nr_segof = L.take<int>(E + 2);
   c.nr_seg = L.take<int>(E + 8); c.nr_seg2 = L.take<int>(E + 8); c.nr_small = L.take<int>(E + 16);
   c.nr_piv = L.take<double>(E / 2 + 8); c.nr_segmeta = L.take<int>(2 * E + 32);
+  c.nr_bsum_cap = 2 * 4096; c.nr_bsum = L.take<int>(c.nr_bsum_cap);
   c.e_rank = L.take<int>(E); c.e_inmst = L.take<int>(E); c.tree = L.take<int>(N);
   c.mst_comp = L.take<int>(N); c.mst_min = L.take<int>(N); c.mst_next = L.take<int>(N);
   c.arc_deg = L.take<int>(N + 1); c.arc_start = L.take<int>(N + 1); c.arc_slot = L.take<int>(2 * N);

@@ -81,6 +81,8 @@ struct Ctx {
   int *o_b1 = nullptr, *o_b2 = nullptr, *o_n1 = nullptr, *o_n2 = nullptr;  // oriented copies
   int *r_b1 = nullptr, *r_b2 = nullptr, *r_n1 = nullptr, *r_n2 = nullptr;  // unsorted edges
   double* r_w = nullptr;
+  int* nr_bsum = nullptr;  // per-block stopper totals of the cooperative NR sort
+  int nr_bsum_cap = 0;
   int *nr_idx = nullptr, *nr_idx2 = nullptr, *nr_lf = nullptr, *nr_rf = nullptr, *nr_ls = nullptr,
       *nr_rs = nullptr, *nr_lpos = nullptr, *nr_rpos = nullptr, *nr_segof = nullptr;
   int *nr_seg = nullptr, *nr_seg2 = nullptr;  // segments: pairs (l, ir), 1-based

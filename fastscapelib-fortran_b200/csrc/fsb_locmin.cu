@@ -23,6 +23,8 @@
 #include <cfloat>
 #include <climits>
 
+#include <cooperative_groups.h>
+
 #include "fsb_kernels.cuh"
 
 namespace fsb {
@@ -31,7 +33,8 @@ namespace {
 
 enum {
   C_NBASINS = 0, C_NLOCMIN = 1, C_BASIN0 = 2, C_NEDGE = 3, C_NSEG = 4, C_NSMALL = 5,
-  C_CHANGED = 6, C_NTREE = 7, C_NLOCMIN_AFTER = 8, C_OVERFLOW = 9, C_NOTFLAT = 10, C_NSEG2 = 11
+  C_CHANGED = 6, C_NTREE = 7, C_NLOCMIN_AFTER = 8, C_OVERFLOW = 9, C_NOTFLAT = 10, C_NSEG2 = 11,
+  C_NRIDX = 12, C_NRLEVELS = 13
 };
 
 __constant__ int c_ii[8] = {-1, 1, 0, 0, -1, 1, -1, 1};
@@ -213,48 +216,39 @@ __global__ void k_nr_init(int n, int* __restrict__ idx, int* __restrict__ segof,
 
 __device__ inline void iswap(int* v, int a, int b) { const int t = v[a]; v[a] = v[b]; v[b] = t; }
 
+// ---- one NR level, per segment s / per position q (shared by the level
+// kernels below and the cooperative kernel k_nr_levels) ----------------------
+// No pointer here is __restrict__ but the weights: in k_nr_levels the same
+// arrays are written in one phase and read in the next, so their loads must
+// not take the non-coherent read-only path.
+
 // median of three (LocalMinima.f90:985-1006)
-__global__ void k_nr_median(const int* __restrict__ nsegp, const int* __restrict__ seg, const double* __restrict__ arr,
-                            int* __restrict__ idx, double* __restrict__ piv, int* __restrict__ meta) {
-  const int nseg = *nsegp;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
+__device__ inline void nr_median_one(int s, const int* seg, const double* __restrict__ arr,
+                                     int* idx, double* piv, int* meta) {
+  const int l = seg[2 * s], ir = seg[2 * s + 1];
+  const int k = (l + ir) / 2;
+  iswap(idx, k, l + 1);
+  if (arr[idx[l + 1]] > arr[idx[ir]]) iswap(idx, l + 1, ir);
+  if (arr[idx[l]] > arr[idx[ir]]) iswap(idx, l, ir);
+  if (arr[idx[l + 1]] > arr[idx[l]]) iswap(idx, l + 1, l);
+  piv[s] = arr[idx[l]];
+  meta[4 * s] = idx[l];
+}
+
+// stopper flags of position q: the left scan stops where arr >= a (positions
+// l+2..ir), the right scan where arr <= a (positions l+1..ir-1)
+__device__ inline void nr_flags_one(int q, const int* segof, const int* seg,
+                                    const double* piv, const double* __restrict__ arr,
+                                    const int* idx, int& a, int& b) {
+  a = 0;
+  b = 0;
+  const int s = segof[q];
+  if (s >= 0) {
     const int l = seg[2 * s], ir = seg[2 * s + 1];
-    const int k = (l + ir) / 2;
-    iswap(idx, k, l + 1);
-    if (arr[idx[l + 1]] > arr[idx[ir]]) iswap(idx, l + 1, ir);
-    if (arr[idx[l]] > arr[idx[ir]]) iswap(idx, l, ir);
-    if (arr[idx[l + 1]] > arr[idx[l]]) iswap(idx, l + 1, l);
-    piv[s] = arr[idx[l]];
-    meta[4 * s] = idx[l];
-  }
-}
-
-// stopper flags: left scan stops where arr >= a (positions l+2..ir),
-// right scan stops where arr <= a (positions l+1..ir-1)
-__global__ void k_nr_flags(int n, const int* __restrict__ segof, const int* __restrict__ seg,
-                           const double* __restrict__ piv, const double* __restrict__ arr,
-                           const int* __restrict__ idx, int* __restrict__ lf, int* __restrict__ rf) {
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= n + 1; q += gridDim.x * blockDim.x) {
-    int a = 0, b = 0;
-    const int s = segof[q];
-    if (s >= 0) {
-      const int l = seg[2 * s], ir = seg[2 * s + 1];
-      const double pv = piv[s];
-      const double v = arr[idx[q]];
-      a = (q >= l + 2 && q <= ir && v >= pv) ? 1 : 0;
-      b = (q >= l + 1 && q <= ir - 1 && v <= pv) ? 1 : 0;
-    }
-    lf[q] = a;
-    rf[q] = b;
-  }
-}
-
-__global__ void k_nr_scatter(int n, const int* __restrict__ lf, const int* __restrict__ rf,
-                             const int* __restrict__ ls, const int* __restrict__ rs, int* __restrict__ lpos,
-                             int* __restrict__ rpos) {
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= n + 1; q += gridDim.x * blockDim.x) {
-    if (lf[q]) lpos[ls[q]] = q;
-    if (rf[q]) rpos[rs[q]] = q;
+    const double pv = piv[s];
+    const double v = arr[idx[q]];
+    a = (q >= l + 2 && q <= ir && v >= pv) ? 1 : 0;
+    b = (q >= l + 1 && q <= ir - 1 && v <= pv) ? 1 : 0;
   }
 }
 
@@ -263,34 +257,31 @@ __global__ void k_nr_scatter(int n, const int* __restrict__ lf, const int* __res
 // partition swaps (L_t, R_t) for every t < T, T = min{t : L_t >= R_t}.  If
 // L_T == R_T = P the scans stop at i=P+1, j=P-1; otherwise at
 // i = min(L_T, R_{T-1}), j = max(R_T, L_{T-1}) (R_0 = +inf, L_0 = -inf).
-__global__ void k_nr_cross(const int* __restrict__ nsegp, const int* __restrict__ seg, const int* __restrict__ ls,
-                           const int* __restrict__ rs, const int* __restrict__ lpos,
-                           const int* __restrict__ rpos, int* __restrict__ meta) {
-  const int nseg = *nsegp;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
-    const int l = seg[2 * s], ir = seg[2 * s + 1];
-    const int lb = ls[l + 2], nL = ls[ir + 1] - ls[l + 2];
-    const int rtop = rs[ir], nR = rs[ir] - rs[l + 1];
-    auto L = [&](int t) { return lpos[lb + t - 1]; };
-    auto R = [&](int t) { return rpos[rtop - t]; };
-    int lo = 1, hi = min(nL, nR);
-    while (lo < hi) {
-      const int mid = (lo + hi) / 2;
-      if (L(mid) >= R(mid)) hi = mid; else lo = mid + 1;
-    }
-    const int T = lo;
-    int i, j;
-    if (L(T) == R(T)) {
-      i = L(T) + 1;
-      j = L(T) - 1;
-    } else {
-      i = (T == 1) ? L(1) : min(L(T), R(T - 1));
-      j = (T == 1) ? R(1) : max(R(T), L(T - 1));
-    }
-    meta[4 * s + 1] = i;
-    meta[4 * s + 2] = j;
-    meta[4 * s + 3] = T;
+__device__ inline void nr_cross_one(int s, const int* seg, const int* ls,
+                                    const int* rs, const int* lpos,
+                                    const int* rpos, int* meta) {
+  const int l = seg[2 * s], ir = seg[2 * s + 1];
+  const int lb = ls[l + 2], nL = ls[ir + 1] - ls[l + 2];
+  const int rtop = rs[ir], nR = rs[ir] - rs[l + 1];
+  auto L = [&](int t) { return lpos[lb + t - 1]; };
+  auto R = [&](int t) { return rpos[rtop - t]; };
+  int lo = 1, hi = min(nL, nR);
+  while (lo < hi) {
+    const int mid = (lo + hi) / 2;
+    if (L(mid) >= R(mid)) hi = mid; else lo = mid + 1;
   }
+  const int T = lo;
+  int i, j;
+  if (L(T) == R(T)) {
+    i = L(T) + 1;
+    j = L(T) - 1;
+  } else {
+    i = (T == 1) ? L(1) : min(L(T), R(T - 1));
+    j = (T == 1) ? R(1) : max(R(T), L(T - 1));
+  }
+  meta[4 * s + 1] = i;
+  meta[4 * s + 2] = j;
+  meta[4 * s + 3] = T;
 }
 
 __device__ inline int nr_newval(int x, int l, int ir, int T, const int* idx, const int* lf,
@@ -307,66 +298,249 @@ __device__ inline int nr_newval(int x, int l, int ir, int T, const int* idx, con
   return idx[x];
 }
 
+// the partitioned permutation at position q (1..n)
+__device__ inline int nr_apply_one(int q, const int* segof, const int* seg,
+                                   const int* meta, const int* idx,
+                                   const int* lf, const int* rf, const int* ls,
+                                   const int* rs, const int* lpos,
+                                   const int* rpos) {
+  const int s = segof[q];
+  if (s < 0) return idx[q];
+  const int l = seg[2 * s], ir = seg[2 * s + 1];
+  const int pv = meta[4 * s], j = meta[4 * s + 2], T = meta[4 * s + 3];
+  if (q == l) return nr_newval(j, l, ir, T, idx, lf, rf, ls, rs, lpos, rpos);
+  if (q == j) return pv;
+  return nr_newval(q, l, ir, T, idx, lf, rf, ls, rs, lpos, rpos);
+}
+
+// children segments [l, j-1] and [i, ir]: partitioned further when they hold
+// at least M+1=8 elements (counted in cnt[out_slot]), insertion-sorted otherwise
+__device__ inline void nr_newsegs_one(int s, int out_slot, const int* seg, int* meta,
+                                      int* seg2, int* small, int* cnt,
+                                      int small_cap) {
+  const int l = seg[2 * s], ir = seg[2 * s + 1];
+  const int i = meta[4 * s + 1], j = meta[4 * s + 2];
+  int ids[2] = {-1, -1};
+  const int lo[2] = {l, i}, hi[2] = {j - 1, ir};
+  for (int c = 0; c < 2; ++c) {
+    if (hi[c] - lo[c] >= 7) {
+      const int id = atomicAdd(&cnt[out_slot], 1);
+      seg2[2 * id] = lo[c];
+      seg2[2 * id + 1] = hi[c];
+      ids[c] = id;
+    } else if (hi[c] - lo[c] >= 1) {
+      const int id = atomicAdd(&cnt[C_NSMALL], 1);
+      if (id < small_cap) { small[2 * id] = lo[c]; small[2 * id + 1] = hi[c]; }
+      else atomicExch(&cnt[C_OVERFLOW], 1);
+    }
+  }
+  // reuse meta slots for the children ids (i, j no longer needed after this)
+  meta[4 * s + 1] = ids[0];
+  meta[4 * s + 2] = ids[1];
+  meta[4 * s + 3] = j;  // boundary of the left child
+  meta[4 * s] = i;      // start of the right child
+}
+
+__device__ inline void nr_segof_one(int q, const int* seg, const int* meta,
+                                    int* segof) {
+  const int s = segof[q];
+  if (s < 0) return;
+  const int l = seg[2 * s], ir = seg[2 * s + 1];
+  const int i = meta[4 * s], j = meta[4 * s + 3];
+  int ns = -1;
+  if (q >= l && q <= j - 1) ns = meta[4 * s + 1];
+  else if (q >= i && q <= ir) ns = meta[4 * s + 2];
+  segof[q] = ns;
+}
+
+// ---- one level per kernel -------------------------------------------------
+__global__ void k_nr_median(const int* __restrict__ nsegp, const int* __restrict__ seg, const double* __restrict__ arr,
+                            int* __restrict__ idx, double* __restrict__ piv, int* __restrict__ meta) {
+  const int nseg = *nsegp;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x)
+    nr_median_one(s, seg, arr, idx, piv, meta);
+}
+
+__global__ void k_nr_flags(int n, const int* __restrict__ segof, const int* __restrict__ seg,
+                           const double* __restrict__ piv, const double* __restrict__ arr,
+                           const int* __restrict__ idx, int* __restrict__ lf, int* __restrict__ rf) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= n + 1; q += gridDim.x * blockDim.x) {
+    int a, b;
+    nr_flags_one(q, segof, seg, piv, arr, idx, a, b);
+    lf[q] = a;
+    rf[q] = b;
+  }
+}
+
+__global__ void k_nr_scatter(int n, const int* __restrict__ lf, const int* __restrict__ rf,
+                             const int* __restrict__ ls, const int* __restrict__ rs, int* __restrict__ lpos,
+                             int* __restrict__ rpos) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= n + 1; q += gridDim.x * blockDim.x) {
+    if (lf[q]) lpos[ls[q]] = q;
+    if (rf[q]) rpos[rs[q]] = q;
+  }
+}
+
+__global__ void k_nr_cross(const int* __restrict__ nsegp, const int* __restrict__ seg, const int* __restrict__ ls,
+                           const int* __restrict__ rs, const int* __restrict__ lpos,
+                           const int* __restrict__ rpos, int* __restrict__ meta) {
+  const int nseg = *nsegp;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x)
+    nr_cross_one(s, seg, ls, rs, lpos, rpos, meta);
+}
+
 __global__ void k_nr_apply(int n, const int* __restrict__ segof, const int* __restrict__ seg,
                            const int* __restrict__ meta, const int* __restrict__ idx, const int* __restrict__ lf,
                            const int* __restrict__ rf, const int* __restrict__ ls, const int* __restrict__ rs,
                            const int* __restrict__ lpos, const int* __restrict__ rpos, int* __restrict__ out) {
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= n; q += gridDim.x * blockDim.x) {
-    if (q == 0) continue;
-    const int s = segof[q];
-    if (s < 0) { out[q] = idx[q]; continue; }
-    const int l = seg[2 * s], ir = seg[2 * s + 1];
-    const int pv = meta[4 * s], j = meta[4 * s + 2], T = meta[4 * s + 3];
-    if (q == l) out[q] = nr_newval(j, l, ir, T, idx, lf, rf, ls, rs, lpos, rpos);
-    else if (q == j) out[q] = pv;
-    else out[q] = nr_newval(q, l, ir, T, idx, lf, rf, ls, rs, lpos, rpos);
-  }
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= n; q += gridDim.x * blockDim.x)
+    if (q > 0) out[q] = nr_apply_one(q, segof, seg, meta, idx, lf, rf, ls, rs, lpos, rpos);
 }
 
-// children segments [l, j-1] and [i, ir]: partitioned further when they hold
-// at least M+1=8 elements, insertion-sorted otherwise
 // reads the level's segment count from cnt[in_slot] and counts the next
 // level's segments in cnt[out_slot] (zeroed before the launch)
 __global__ void k_nr_newsegs(int in_slot, int out_slot, const int* __restrict__ seg, int* __restrict__ meta,
                              int* __restrict__ seg2, int* __restrict__ small, int* __restrict__ cnt,
                              int small_cap) {
   const int nseg = cnt[in_slot];
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
-    const int l = seg[2 * s], ir = seg[2 * s + 1];
-    const int i = meta[4 * s + 1], j = meta[4 * s + 2];
-    int ids[2] = {-1, -1};
-    const int lo[2] = {l, i}, hi[2] = {j - 1, ir};
-    for (int c = 0; c < 2; ++c) {
-      if (hi[c] - lo[c] >= 7) {
-        const int id = atomicAdd(&cnt[out_slot], 1);
-        seg2[2 * id] = lo[c];
-        seg2[2 * id + 1] = hi[c];
-        ids[c] = id;
-      } else if (hi[c] - lo[c] >= 1) {
-        const int id = atomicAdd(&cnt[C_NSMALL], 1);
-        if (id < small_cap) { small[2 * id] = lo[c]; small[2 * id + 1] = hi[c]; }
-        else atomicExch(&cnt[C_OVERFLOW], 1);
-      }
-    }
-    // reuse meta slots 1,2 for the children ids (i, j no longer needed after this)
-    meta[4 * s + 1] = ids[0];
-    meta[4 * s + 2] = ids[1];
-    meta[4 * s + 3] = j;  // boundary of the left child
-    meta[4 * s] = i;      // start of the right child
-  }
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x)
+    nr_newsegs_one(s, out_slot, seg, meta, seg2, small, cnt, small_cap);
 }
 
 __global__ void k_nr_segof(int n, const int* __restrict__ seg, const int* __restrict__ meta,
                            int* __restrict__ segof) {
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= n + 1; q += gridDim.x * blockDim.x) {
-    const int s = segof[q];
-    if (s < 0) continue;
-    const int l = seg[2 * s], ir = seg[2 * s + 1];
-    const int i = meta[4 * s], j = meta[4 * s + 3];
-    int ns = -1;
-    if (q >= l && q <= j - 1) ns = meta[4 * s + 1];
-    else if (q >= i && q <= ir) ns = meta[4 * s + 2];
-    segof[q] = ns;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= n + 1; q += gridDim.x * blockDim.x)
+    nr_segof_one(q, seg, meta, segof);
+}
+
+// ---- all levels in one cooperative kernel ----------------------------------
+// The phases of a level (medians; stopper flags and their prefix sums with
+// the stopper positions; crossings; the partitioned permutation; the next
+// level's segments; segment ids) are separated by grid-wide barriers, so the
+// whole sort is one launch instead of about eleven per level.  The prefix
+// sums run over contiguous chunks of positions, one chunk per block: block
+// totals, then each block's offset, then a tiled scan of the chunk (the two
+// flags packed into one int, 16 bits each, per 256-position tile).
+struct NrCoop {
+  int n;
+  const double* arr;
+  int *idx, *idx2, *seg, *seg2, *segof, *lf, *rf, *ls, *rs, *lpos, *rpos, *meta, *small, *cnt, *bsum;
+  double* piv;
+  int small_cap;
+};
+
+constexpr int kCoopThreads = 256;
+
+__device__ inline int block_sum(int v, int* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  int t = 0;
+  if (threadIdx.x < kCoopThreads / 32) t = sh[threadIdx.x];
+  if (w == 0)
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  __syncthreads();
+  if (threadIdx.x == 0) sh[0] = t;
+  __syncthreads();
+  const int r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kCoopThreads) k_nr_levels(NrCoop A) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  __shared__ int sh[kCoopThreads / 32];
+  __shared__ int wsc[kCoopThreads / 32];
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nthreads = gridDim.x * blockDim.x;
+  const int n = A.n, np = n + 2;  // positions 0..n+1
+  const int chunk = (np + gridDim.x - 1) / gridDim.x;
+  const int q0 = min(np, blockIdx.x * chunk), q1 = min(np, q0 + chunk);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int *idx = A.idx, *idx2 = A.idx2, *seg = A.seg, *seg2 = A.seg2;
+  int in = C_NSEG, out = C_NSEG2;
+  int level = 0;
+  for (; level < 200; ++level) {
+    const int nseg = __ldcg(&A.cnt[in]);
+    if (nseg == 0) break;
+    if (tid == 0) A.cnt[out] = 0;
+    for (int s = tid; s < nseg; s += nthreads) nr_median_one(s, seg, A.arr, idx, A.piv, A.meta);
+    grid.sync();
+    // stopper flags and the block's totals
+    int tl = 0, tr = 0;
+    for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+      int a, b;
+      nr_flags_one(q, A.segof, seg, A.piv, A.arr, idx, a, b);
+      A.lf[q] = a;
+      A.rf[q] = b;
+      tl += a;
+      tr += b;
+    }
+    tl = block_sum(tl, sh);
+    tr = block_sum(tr, sh);
+    if (threadIdx.x == 0) { A.bsum[2 * blockIdx.x] = tl; A.bsum[2 * blockIdx.x + 1] = tr; }
+    grid.sync();
+    // this block's offsets, then the tiled exclusive scan of its chunk
+    int ol = 0, orr = 0;
+    for (int b = threadIdx.x; b < (int)blockIdx.x; b += blockDim.x) {
+      ol += __ldcg(&A.bsum[2 * b]);
+      orr += __ldcg(&A.bsum[2 * b + 1]);
+    }
+    ol = block_sum(ol, sh);
+    orr = block_sum(orr, sh);
+    for (int base = q0; base < q1; base += blockDim.x) {
+      const int q = base + threadIdx.x;
+      const int a = q < q1 ? A.lf[q] : 0, b = q < q1 ? A.rf[q] : 0;
+      const int v = a | (b << 16);
+      int x = v;  // inclusive warp scan of the packed pair
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (lane == 31) wsc[wid] = x;
+      __syncthreads();
+      if (wid == 0) {
+        int w = lane < kCoopThreads / 32 ? wsc[lane] : 0;
+        for (int o = 1; o < kCoopThreads / 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, w, o);
+          if (lane >= o) w += y;
+        }
+        if (lane < kCoopThreads / 32) wsc[lane] = w;  // inclusive warp totals
+      }
+      __syncthreads();
+      const int excl = x - v + (wid > 0 ? wsc[wid - 1] : 0);
+      const int tot = wsc[kCoopThreads / 32 - 1];
+      if (q < q1) {
+        const int L = ol + (excl & 0xffff), R = orr + (excl >> 16);
+        A.ls[q] = L;
+        A.rs[q] = R;
+        if (a) A.lpos[L] = q;
+        if (b) A.rpos[R] = q;
+      }
+      ol += tot & 0xffff;
+      orr += tot >> 16;
+      __syncthreads();
+    }
+    grid.sync();
+    for (int s = tid; s < nseg; s += nthreads) nr_cross_one(s, seg, A.ls, A.rs, A.lpos, A.rpos, A.meta);
+    grid.sync();
+    for (int q = tid + 1; q <= n; q += nthreads)
+      idx2[q] = nr_apply_one(q, A.segof, seg, A.meta, idx, A.lf, A.rf, A.ls, A.rs, A.lpos, A.rpos);
+    grid.sync();
+    for (int s = tid; s < nseg; s += nthreads) nr_newsegs_one(s, out, seg, A.meta, seg2, A.small, A.cnt, A.small_cap);
+    grid.sync();
+    for (int q = tid; q <= n + 1; q += nthreads) nr_segof_one(q, seg, A.meta, A.segof);
+    grid.sync();
+    int* t = idx; idx = idx2; idx2 = t;
+    t = seg; seg = seg2; seg2 = t;
+    const int ti = in; in = out; out = ti;
+  }
+  if (tid == 0) {
+    A.cnt[C_NRIDX] = idx == A.idx ? 0 : 1;
+    A.cnt[C_NRLEVELS] = level;
   }
 }
 
@@ -570,6 +744,32 @@ __global__ void k_copy_nroots(const int* src, int* cnt) {
 
 // Runs the exact NR index sort on w[0..n-1]; result: c.nr_idx[1..n] holds the
 // 1-based ids in sorted order.  Returns false on buffer overflow.
+// All levels in one cooperative launch; false when the device cannot run it
+// (the caller then runs one launch per level).  Reads the counters back.
+static bool nr_levels_coop(Ctx& c, int n, const double* arr, int small_cap) {
+  int dev = 0, coop = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nr_levels, kCoopThreads, 0) != cudaSuccess ||
+      per_sm < 1)
+    return false;
+  // about 2048 positions per block, at most what is resident at once
+  const int want = (n + 2 + 2047) / 2048;
+  const int blocks = std::max(1, std::min(want, std::min(sms * per_sm, c.nr_bsum_cap / 2)));
+  NrCoop A{n, arr, c.nr_idx, c.nr_idx2, c.nr_seg, c.nr_seg2, c.nr_segof, c.nr_lf, c.nr_rf, c.nr_ls, c.nr_rs,
+           c.nr_lpos, c.nr_rpos, c.nr_segmeta, c.nr_small, c.d_cnt, c.nr_bsum, c.nr_piv, small_cap};
+  void* args[] = {&A};
+  if (cudaLaunchCooperativeKernel((const void*)k_nr_levels, dim3(blocks), dim3(kCoopThreads), args, 0, c.stream) !=
+      cudaSuccess) {
+    cudaGetLastError();  // clear the launch error; the per-level path runs instead
+    return false;
+  }
+  c.count_launch();
+  fetch_counters(c, 14);
+  return true;
+}
+
 static bool nr_indexx(Ctx& c, int n, const double* w) {
   const double* arr = w - 1;  // 1-based
   int* idx = c.nr_idx;
@@ -581,6 +781,12 @@ static bool nr_indexx(Ctx& c, int n, const double* w) {
   c.count_launch();
   fetch_counters(c, 10);
   int nseg = c.h_cnt[C_NSEG];
+  if (nseg > 0 && nr_levels_coop(c, n, arr, small_cap)) {
+    if (c.h_cnt[C_OVERFLOW]) { c.err = "NR sort emulation: small-segment buffer overflow"; return false; }
+    if (c.h_cnt[C_NRLEVELS] >= 200) { c.err = "NR sort emulation: too many levels"; return false; }
+    if (c.h_cnt[C_NRIDX]) std::swap(idx, idx2);
+    nseg = 0;  // all levels done
+  }
   // Levels run with the segment count on the device (slot `in` of d_cnt), a
   // few levels per read-back: a level with no segment left changes nothing.
   // Every segment holds at least 8 elements, so a level has at most n/8.
