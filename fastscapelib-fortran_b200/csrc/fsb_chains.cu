@@ -38,15 +38,16 @@ constexpr unsigned FULL = 0xffffffffu;
 
 // bounded wait for done[k] == epoch (relaxed polling, then an acquire
 // fence); gives up once any wait has failed
+// waits (bounded) until done[k] == epoch; the acquire load that sees it makes
+// the chain's values released before the flag visible
 __device__ inline void wait_flag(unsigned* done, int k, unsigned epoch, int* err) {
   int spins = 0, back = 32;
-  while (*(volatile unsigned*)&done[k] != epoch) {
+  while (ld_acquire_gpu(&done[k]) != epoch) {
     if (++spins > kSpinLimit) { atomicExch(err, DEV_SPIN_LIMIT); return; }
     if ((spins & 63) == 0 && *(volatile int*)err != 0) return;
     __nanosleep(back);
     if (back < 512) back <<= 1;
   }
-  fence_acq_rel();
 }
 
 // heavy child: donor with the largest subtree, first in ascending order on ties

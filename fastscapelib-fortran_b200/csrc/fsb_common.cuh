@@ -55,6 +55,20 @@ constexpr int kSpinLimit = 1 << 21;  // polls (~1 s) before a bounded wait gives
 // needs acquire-release ordering only -- not the sequentially consistent
 // fence that __threadfence() issues.
 __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// loads with acquire semantics at GPU scope: later memory operations of the
+// thread see everything released before the value read was written (cheaper
+// than a load followed by fence_acq_rel)
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 #endif
 
 }  // namespace fsb

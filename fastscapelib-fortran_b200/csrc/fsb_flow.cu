@@ -97,13 +97,13 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, i
       if (want) slot = (long long)base + __popc(m & lt);
     }
     if (cur < 0 && slot >= 0 && slot < nn) {
-      const int v = *(volatile int*)&queue[slot];
+      // acquire load: the pusher released the node (fence, then this slot)
+      const int v = ld_acquire_gpu(&queue[slot]);
       if (v >= 0) { cur = v; slot = -1; }
     }
     int dep[8];
     unsigned rdy = 0;  // bit t: dependent t became ready and goes to the queue
-    if (cur >= 0) {
-      fence_acq_rel();  // acquire: the node's inputs were published before it became ready
+    if (cur >= 0) {  // cur's inputs are visible: it was acquired from the queue or below
       unsigned pr[8];
       const int nd = op.run(cur, dep, pr, Loc{});
       int nxt = -1;
@@ -121,7 +121,15 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, i
             if (bi < 0 || pr[t] > bp) { bp = pr[t]; bi = t; nxt = dep[t]; }
           }
         if (bi >= 0) rdy &= ~(1u << bi);
-        if (nxt >= 0) op.prefetch(nxt);  // the continuation's record line into L1
+        if (nxt >= 0) {
+          op.prefetch(nxt);  // the continuation's record line into L1
+          // Acquire the continuation: each producer released (fence) before
+          // its decrement, our decrement continues their release sequences,
+          // and this acquire load reads our decrement's value.  It replaces a
+          // full fence (on B200 an acquire hand-off costs ~470 ns against
+          // ~800 ns with a fence; the 2049^2 step 66.6 against 72.9 ms).
+          (void)ld_acquire_gpu(&cnt[nxt]);
+        }
       }
       ++local_done;
       cur = nxt;
