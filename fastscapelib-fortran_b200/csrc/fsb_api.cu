@@ -156,6 +156,7 @@ size_t layout(fsb::Ctx& c, char* base) {
   c.la_queue = L.take<int>(N); c.la_cnt = L.take<int>(N); c.cnt_acc = L.take<int>(N); c.cnt_spl = L.take<int>(N);
   c.la_ctl = L.take<unsigned>(128);
   c.mfd_line = L.take<double>(16 * N); c.hw = L.take<double>(2 * N);
+  c.slots = L.take<double>(fsb::kSlotStride * N);
   c.s_scan2 = L.take<int>(N + 1);
   c.done = L.take<unsigned>(N); c.ticket = L.take<unsigned>(4);
   c.water = L.take<double>(N); c.hnew = L.take<double>(N);

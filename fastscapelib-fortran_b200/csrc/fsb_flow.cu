@@ -4,7 +4,8 @@
 // Reference routines restated here (fastscapelib-fortran file:line):
 //   find_mult_rec                 src/FlowRouting.f90:147-298
 //   FlowAccumulation (MFD)        src/FlowRouting.f90:97-119
-//   StreamPowerLaw (MFD, g == 0)  src/StreamPowerLaw.f90:3-206
+//   StreamPowerLaw (MFD)          src/StreamPowerLaw.f90:3-206 (the g > 0
+//                                 iterations are driven from fsb_sediment.cu)
 //   Diffusion + tridag            src/Diffusion.f90:1-202
 // The single-flow tree sweeps live in fsb_chains.cu.
 //
@@ -13,8 +14,10 @@
 // brings a counter to zero ("last arriver") continues with that node, and
 // further nodes it makes ready go to a work queue.  Nothing waits on work that
 // has not been scheduled, so the sweep needs no global order and cannot
-// deadlock; the counters' acquire/release ordering makes every dependency's
-// value visible before it is read.
+// deadlock.  A producer hands its value to each dependent by storing it into
+// one of the dependent's input slots before decrementing the dependent's
+// counter; the consumer reads its slots and waits (bounded) on any that still
+// hold the empty sentinel, so no fence is needed on either side.
 #include <algorithm>
 #include <cmath>
 #include <cuda/atomic>
@@ -33,14 +36,8 @@ __device__ inline unsigned long long ordered_key(double x) {
   return (u & 0x8000000000000000ull) ? ~u : (u | 0x8000000000000000ull);
 }
 
-// Reads a dependency's value produced by another thread: through L2
-// (__ldcg), after the acquire fence of the hand-off.
-struct Loc {
-  __device__ double ld(const double* p, int) const { return __ldcg(p); }
-};
-
 // ---- last-arriver sweep engine ----------------------------------------------
-// Op::run(k, dep[], pr[], loc) computes node k, stores its outputs and lists
+// Op::run(k, dep[], pr[]) computes node k, stores its outputs and lists
 // k's dependents with their priorities; the engine then decrements their
 // counters, continues with the ready dependent of largest priority (subtree
 // size), prefetching its record (Op::prefetch), and queues the other ready
@@ -97,19 +94,22 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, i
       if (want) slot = (long long)base + __popc(m & lt);
     }
     if (cur < 0 && slot >= 0 && slot < nn) {
-      // acquire load: the pusher released the node (fence, then this slot)
-      const int v = ld_acquire_gpu(&queue[slot]);
+      const int v = ld_relaxed_gpu(&queue[slot]);
       if (v >= 0) { cur = v; slot = -1; }
     }
     int dep[8];
     unsigned rdy = 0;  // bit t: dependent t became ready and goes to the queue
-    if (cur >= 0) {  // cur's inputs are visible: it was acquired from the queue or below
+    if (cur >= 0) {
+      // No fence or acquire anywhere: op.run reads cur's inputs from its
+      // slots, where each producer stored its value before its decrement,
+      // and waits on a slot that still holds the sentinel.  (On B200 this
+      // hand-off costs ~510 ns against ~860 ns with a release fence and an
+      // acquire load, ~1160 ns with two fences.)
       unsigned pr[8];
-      const int nd = op.run(cur, dep, pr, Loc{});
+      const int nd = op.run(cur, dep, pr);
       int nxt = -1;
       if (nd) {
         int old[8];
-        fence_acq_rel();  // release the node's outputs before its dependents' counters drop
 #pragma unroll
         for (int t = 0; t < 8; ++t) old[t] = t < nd ? atomicSub(&cnt[dep[t]], 1) : 0;
         unsigned bp = 0;
@@ -121,21 +121,12 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, i
             if (bi < 0 || pr[t] > bp) { bp = pr[t]; bi = t; nxt = dep[t]; }
           }
         if (bi >= 0) rdy &= ~(1u << bi);
-        if (nxt >= 0) {
-          op.prefetch(nxt);  // the continuation's record line into L1
-          // Acquire the continuation: each producer released (fence) before
-          // its decrement, our decrement continues their release sequences,
-          // and this acquire load reads our decrement's value.  It replaces a
-          // full fence (on B200 an acquire hand-off costs ~470 ns against
-          // ~800 ns with a fence; the 2049^2 step 66.6 against 72.9 ms).
-          (void)ld_acquire_gpu(&cnt[nxt]);
-        }
+        if (nxt >= 0) op.prefetch(nxt);  // the continuation's record line into L1
       }
       ++local_done;
       cur = nxt;
     }
     if (__ballot_sync(FULL, rdy != 0)) {  // queue the other ready nodes, one atomic per warp
-      bool fenced = false;
 #pragma unroll
       for (int t = 0; t < 8; ++t) {
         const bool has = (rdy >> t) & 1u;
@@ -147,7 +138,6 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, i
         base = __shfl_sync(FULL, base, leader);
         if (has) {
           const unsigned idx = base + __popc(mm & lt);
-          if (!fenced) { fence_acq_rel(); fenced = true; }
           if (idx < (unsigned)nn) *(volatile int*)&queue[idx] = dep[t];
           else atomicExch(err, DEV_OVERFLOW);
         }
@@ -209,12 +199,19 @@ __global__ void k_seed_queue(int nn, const int* __restrict__ cnt, int* __restric
 //               q       codes of those receiver slots
 //               dep     codes of the donors that wait for k (gated, or rec == k), pr[8]
 //               meta    code of rec(k) (0: k is a root); bit 4 set when mnrec(k) > 0
+// The values a sweep hands from node to node travel in slots: node k's inputs
+// are Ctx::slots[k*kSlotStride + s] (area: s = donor position; stream power:
+// s = gated-receiver position, 8 = rec's water, 9 = rec's lake sill as
+// integer bits), all ones until written.  rpos / qmask / wflag tell a
+// producer where its value goes in each dependent's slots; they are filled by
+// a second pass over the consumers (k_acc_slotpos, k_spl_slotpos).
 struct __align__(128) AccLine {
   double aw[8];
   double base;
   unsigned don, rcv;
   unsigned short pr[8];
-  int pad[8];
+  unsigned rpos;  // 4 bits per receiver t: this node's slot in that receiver's inputs
+  int pad[7];
 };
 struct __align__(128) SplLine {
   double fact[8];
@@ -222,7 +219,9 @@ struct __align__(128) SplLine {
   unsigned q, dep;
   unsigned short pr[8];
   int meta;
-  int pad[7];
+  unsigned qmask[2];  // 8 bits per dependent t (t < 4: qmask[0]): its gated slots that are this node
+  unsigned wflag;     // bit t: this node is rec of dependent t (water, and the lake sill with g > 0)
+  int pad[4];
 };
 static_assert(sizeof(AccLine) == 128 && sizeof(SplLine) == 128, "one line per node");
 
@@ -291,6 +290,19 @@ union LineWords {
   }
 };
 
+// A consumer's input slot: strong relaxed loads, then a bounded wait while a
+// slot still holds the all-ones sentinel (its producer's store is in flight).
+constexpr long long kSlotEmpty = -1ll;
+__device__ inline double slot_value(const double* p, double v, int* err) {
+  int spins = 0;
+  while (__double_as_longlong(v) == kSlotEmpty) {
+    if (++spins > kSpinLimit) { atomicExch(err, DEV_SPIN_LIMIT); return 0.0; }
+    __nanosleep(32);
+    v = ld_relaxed_gpu(p);
+  }
+  return v;
+}
+
 // a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115);
 // k's dependents are its distinct receivers.  With `clamp` set and lines
 // built on erate it is compute_fluxes' sediment flux (FastScape_ctx.f90:871-877):
@@ -303,21 +315,26 @@ struct AccMfdOp {
   int nx, ny;
   double* a;
   int clamp;
+  double* slots = nullptr;
+  int* err = nullptr;
   int gs = 0;
   const int* rec = nullptr;
   const int* sill = nullptr;
   double* lsed = nullptr;
   __device__ void prefetch(int k) const { prefetch_l1(line + k); }
-  __device__ int run(int k, int* dep, unsigned* pr, const Loc& loc) const {
-    const LineWords<6> L(line + k);  // aw[0..7] = d[0..7], base = d[8], don = u[18], rcv = u[19], pr = s[40..47]
+  __device__ int run(int k, int* dep, unsigned* pr) const {
+    // aw = d[0..7], base = d[8], don = u[18], rcv = u[19], pr = s[40..47], rpos = u[24]
+    const LineWords<7> L(line + k);
     const NbrDecoder nb(k, nx, ny);
-    const unsigned dc = L.u[18], rc = L.u[19];
+    const unsigned dc = L.u[18], rc = L.u[19], rpos = L.u[24];
+    const double* in = slots + (size_t)k * kSlotStride;
     double av[8];
 #pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      const unsigned c = (dc >> (4 * t)) & 15u;
-      if (c) { const int d = nb.at(c); av[t] = loc.ld(&a[d], d); }
-    }
+    for (int t = 0; t < 8; ++t)
+      if ((dc >> (4 * t)) & 15u) av[t] = ld_relaxed_gpu(&in[t]);
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if ((dc >> (4 * t)) & 15u) av[t] = slot_value(&in[t], av[t], err);
     int nd = 0;
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
@@ -344,6 +361,9 @@ struct AccMfdOp {
       }
     }
     a[k] = acc;
+#pragma unroll
+    for (int t = 0; t < 8; ++t)  // hand the value to the receivers
+      if (t < nd) st_relaxed_gpu(&slots[(size_t)dep[t] * kSlotStride + ((rpos >> (4 * t)) & 15u)], acc);
     return nd;
   }
 };
@@ -363,15 +383,18 @@ struct SplMfdOp {
   double omega;
   int n_is_one;
   double2* hw;
+  double* slots = nullptr;
+  int* err = nullptr;
   const double* elev = nullptr;
   const double* hstart = nullptr;
   int* sill = nullptr;
   double* contrib = nullptr;
-  __device__ int run(int k, int* dep, unsigned* pr, const Loc& loc) const {
-    // fact = d[0..7], ht = d[8], q = u[18], dep = u[19], pr = s[40..47], meta = u[24]
+  __device__ int run(int k, int* dep, unsigned* pr) const {
+    // fact = d[0..7], ht = d[8], q = u[18], dep = u[19], pr = s[40..47], meta = u[24],
+    // qmask = u[25..26], wflag = u[27]
     const LineWords<7> L(line + k);
     const NbrDecoder nb(k, nx, ny);
-    const unsigned qc = L.u[18], dc = L.u[19], meta = L.u[24];
+    const unsigned qc = L.u[18], dc = L.u[19], meta = L.u[24], wflag = L.u[27];
     const double ht = L.d[8];
     int nd = 0;
 #pragma unroll
@@ -388,15 +411,17 @@ struct SplMfdOp {
     double ck = 0.0;
     const unsigned rcode = meta & 15u;
     if (rcode) {
-      const int r = nb.at(rcode);
+      const double* in = slots + (size_t)k * kSlotStride;
       double hq[8];
-      const double wr = loc.ld(&hw[r].y, r);
-      if (GS) hk = hstart[k];
+      double wr = ld_relaxed_gpu(&in[8]);
 #pragma unroll
-      for (int t = 0; t < 8; ++t) {
-        const unsigned c = (qc >> (4 * t)) & 15u;
-        if (c) { const int q = nb.at(c); hq[t] = loc.ld(&hw[q].x, q); }
-      }
+      for (int t = 0; t < 8; ++t)
+        if ((qc >> (4 * t)) & 15u) hq[t] = ld_relaxed_gpu(&in[t]);
+      wr = slot_value(&in[8], wr, err);
+#pragma unroll
+      for (int t = 0; t < 8; ++t)
+        if ((qc >> (4 * t)) & 15u) hq[t] = slot_value(&in[t], hq[t], err);
+      if (GS) hk = hstart[k];
       const double elev = GS ? this->elev[k] : ht;
       if (elev > wr) {
         if (meta & 16u) {  // mnrec(k) > 0
@@ -434,7 +459,8 @@ struct SplMfdOp {
       } else {
         hk = elev;
         if (GS) {
-          sk = __ldcg(&sill[r]);
+          const double sv = ld_relaxed_gpu(&in[9]);
+          sk = (int)__double_as_longlong(slot_value(&in[9], sv, err));
           ck = wr - hk;
         }
       }
@@ -444,6 +470,21 @@ struct SplMfdOp {
     if (GS) {
       sill[k] = sk;
       contrib[k] = ck;
+    }
+    // hand h (to the gated slots that are this node), water and the sill (to
+    // the donors whose rec this node is) to the dependents
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      if (t >= nd) break;
+      double* out = slots + (size_t)dep[t] * kSlotStride;
+      const unsigned m = (L.u[25 + (t >> 2)] >> (8 * (t & 3))) & 0xffu;
+#pragma unroll
+      for (int p = 0; p < 8; ++p)
+        if ((m >> p) & 1u) st_relaxed_gpu(&out[p], hk);
+      if ((wflag >> t) & 1u) {
+        st_relaxed_gpu(&out[8], wk);
+        if (GS) st_relaxed_gpu(&out[9], __longlong_as_double((long long)sk));
+      }
     }
     return nd;
   }
@@ -549,7 +590,8 @@ __global__ void k_acc_lines(Bounds bd, double dxdy, const int* __restrict__ mrec
     L.base = dxdy * precip[k];
     L.don = don;
     L.rcv = rcv;
-    for (int t = 0; t < 8; ++t) L.pad[t] = 0;
+    L.rpos = 0;
+    for (int t = 0; t < 7; ++t) L.pad[t] = 0;
     line[k] = L;
     cnt_acc[k] = an;
   }
@@ -633,12 +675,70 @@ __global__ void k_spl_lines(Bounds bd, int n_is_one, double kfsed, double dt, do
     L.q = qc;
     L.dep = dc;
     L.meta = (int)((r != k ? nbr_code_of(i, j, r, nx, ny, err) : 0u) | (nr > 0 ? 16u : 0u));
-    for (int t = 0; t < 7; ++t) L.pad[t] = 0;
+    L.qmask[0] = L.qmask[1] = 0;
+    L.wflag = 0;
+    for (int t = 0; t < 4; ++t) L.pad[t] = 0;
     line[k] = L;
     cnt_spl[k] = cs;
   }
 }
 
+
+// Slot positions, area: consumer r's donor at position t (in r's donor list)
+// is told that its value goes to r's slot t, in the nibble of r in its own
+// receiver list.
+__global__ void k_acc_slotpos(int nx, int ny, AccLine* __restrict__ line) {
+  const int nn = nx * ny;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nn; r += gridDim.x * blockDim.x) {
+    const NbrDecoder nb(r, nx, ny);
+    const unsigned dc = line[r].don;
+    for (int t = 0; t < 8; ++t) {
+      const unsigned c = (dc >> (4 * t)) & 15u;
+      if (!c) break;
+      const int d = nb.at(c);
+      const NbrDecoder nd(d, nx, ny);
+      const unsigned rc = line[d].rcv;
+      for (int i = 0; i < 8; ++i) {
+        const unsigned ci = (rc >> (4 * i)) & 15u;
+        if (!ci) break;
+        if (nd.at(ci) == r) { atomicOr(&line[d].rpos, (unsigned)t << (4 * i)); break; }
+      }
+    }
+  }
+}
+
+// Slot positions, stream power: consumer d's gated receiver q at position p
+// sets bit p of q's mask for d; d's rec sets d's bit in its water flags.
+__global__ void k_spl_slotpos(int nx, int ny, SplLine* __restrict__ line) {
+  const int nn = nx * ny;
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nn; d += gridDim.x * blockDim.x) {
+    const NbrDecoder nb(d, nx, ny);
+    const unsigned qc = line[d].q;
+    auto index_in_deps = [&](int q) {
+      const NbrDecoder nq(q, nx, ny);
+      const unsigned dc = line[q].dep;
+      for (int i = 0; i < 8; ++i) {
+        const unsigned ci = (dc >> (4 * i)) & 15u;
+        if (!ci) break;
+        if (nq.at(ci) == d) return i;
+      }
+      return -1;
+    };
+    for (int p = 0; p < 8; ++p) {
+      const unsigned c = (qc >> (4 * p)) & 15u;
+      if (!c) break;
+      const int q = nb.at(c);
+      const int i = index_in_deps(q);
+      if (i >= 0) atomicOr(&line[q].qmask[i >> 2], 1u << (8 * (i & 3) + p));
+    }
+    const unsigned rcode = (unsigned)line[d].meta & 15u;
+    if (rcode) {
+      const int r = nb.at(rcode);
+      const int i = index_in_deps(r);
+      if (i >= 0) atomicOr(&line[r].wflag, 1u << i);
+    }
+  }
+}
 
 // topological order for the MFD sweeps: ascending h0, ties in stack order
 __global__ void k_order_keys(int nn, const int* __restrict__ stack, const double* __restrict__ h0,
@@ -930,6 +1030,9 @@ void mfd_receivers(Ctx& c) {
 template <int LANES, int SIDE_DIV, class Op>
 static void run_sweep(Ctx& c, Op op, const int* cnt0) {
   const int nn = c.nn;
+  op.slots = c.slots;
+  op.err = c.d_err;
+  cudaMemsetAsync(c.slots, 0xff, sizeof(double) * kSlotStride * (size_t)nn, c.stream);  // all slots empty
   cudaMemcpyAsync(c.la_cnt, cnt0, sizeof(int) * nn, cudaMemcpyDeviceToDevice, c.stream);
   cudaMemsetAsync(c.la_queue, 0xff, sizeof(int) * nn, c.stream);
   cudaMemsetAsync(c.la_ctl, 0, sizeof(unsigned) * 128, c.stream);
@@ -981,6 +1084,8 @@ void accumulate(Ctx& c) {
   k_acc_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, c.dx * c.dy, c.mrec, c.mnrec, c.mwrec, c.precip, c.size,
                                                      line, c.cnt_acc, c.d_err);
   c.count_launch();
+  k_acc_slotpos<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, line);
+  c.count_launch();
   run_sweep<FSB_LANES_ACC, FSB_SIDE_DIV_ACC>(c, AccMfdOp{line, c.nx, c.ny, c.a, 0}, c.cnt_acc);
 }
 
@@ -988,6 +1093,8 @@ void gs_erosion_mfd(Ctx& c, const double* e, const int* sill, double* lsed, doub
   AccLine* line = static_cast<AccLine*>(c.mfd_line);
   k_acc_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, 1.0, c.mrec, c.mnrec, c.mwrec, e, c.size, line,
                                                      c.cnt_acc, c.d_err);
+  c.count_launch();
+  k_acc_slotpos<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, line);
   c.count_launch();
   AccMfdOp op{line, c.nx, c.ny, dh, 0};
   op.gs = 1;
@@ -1003,6 +1110,8 @@ void spl_mfd_gs(Ctx& c, const double* elev, const double* hstart, int* sill, dou
   k_spl_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec, c.mnrec, c.mwrec,
                                                      c.mlrec, c.h, c.b, c.kf, c.a, c.size, line, c.cnt_spl, c.d_err);
   c.count_launch();
+  k_spl_slotpos<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, line);
+  c.count_launch();
   SplMfdOp<true> op{line, c.nx, c.ny, NewtonPow{c.n, c.n == 1.5}, 0.875 / c.n, n1,
                     reinterpret_cast<double2*>(c.hw)};
   op.elev = elev;
@@ -1016,6 +1125,8 @@ void flux_mfd(Ctx& c, double* flux) {
   AccLine* line = static_cast<AccLine*>(c.mfd_line);
   k_acc_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, 1.0, c.mrec, c.mnrec, c.mwrec, c.erate, c.size, line,
                                                      c.cnt_acc, c.d_err);
+  c.count_launch();
+  k_acc_slotpos<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, line);
   c.count_launch();
   run_sweep<FSB_LANES_ACC, FSB_SIDE_DIV_ACC>(c, AccMfdOp{line, c.nx, c.ny, flux, 1}, c.cnt_acc);
 }
@@ -1033,6 +1144,8 @@ void stream_power(Ctx& c) {
   SplLine* line = static_cast<SplLine*>(c.mfd_line);
   k_spl_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec, c.mnrec, c.mwrec,
                                                      c.mlrec, c.h, c.b, c.kf, c.a, c.size, line, c.cnt_spl, c.d_err);
+  c.count_launch();
+  k_spl_slotpos<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, line);
   c.count_launch();
   double2* hw = reinterpret_cast<double2*>(c.hw);
   run_sweep<FSB_LANES_SPL, FSB_SIDE_DIV_SPL>(c, SplMfdOp<false>{line, c.nx, c.ny, NewtonPow{c.n, c.n == 1.5}, omega, n1, hw},

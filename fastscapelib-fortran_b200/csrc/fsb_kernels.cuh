@@ -14,6 +14,7 @@
 namespace fsb {
 
 constexpr int kBlock = 256;
+constexpr int kSlotStride = 16;  // doubles per node in Ctx::slots
 
 inline unsigned grid1d(size_t n, int block = kBlock) {
   size_t g = (n + block - 1) / block;
@@ -106,6 +107,7 @@ struct Ctx {
   int *la_queue = nullptr, *la_cnt = nullptr, *cnt_acc = nullptr, *cnt_spl = nullptr;
   void* mfd_line = nullptr;  // one 128-byte record per node (area, then stream power)
   double* hw = nullptr;      // (elevation, water surface) pairs of the stream-power sweep
+  double* slots = nullptr;   // kSlotStride input slots per node of the multiple-flow sweeps
   unsigned* la_ctl = nullptr;  // head, tail, done count
   int* s_scan2 = nullptr;
   // sweeps
