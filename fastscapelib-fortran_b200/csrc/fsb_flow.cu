@@ -126,22 +126,25 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, i
       ++local_done;
       cur = nxt;
     }
-    if (__ballot_sync(FULL, rdy != 0)) {  // queue the other ready nodes, one atomic per warp
+    if (__ballot_sync(FULL, rdy != 0)) {  // queue the other ready nodes: one atomic per warp
+      const unsigned mine = __popc(rdy);
+      unsigned off = mine;  // inclusive prefix of the lanes' counts
 #pragma unroll
-      for (int t = 0; t < 8; ++t) {
-        const bool has = (rdy >> t) & 1u;
-        const unsigned mm = __ballot_sync(FULL, has);
-        if (!mm) continue;
-        const int leader = __ffs(mm) - 1;
-        unsigned base = 0;
-        if (lane == leader) base = atomicAdd(qtail, (unsigned)__popc(mm));
-        base = __shfl_sync(FULL, base, leader);
-        if (has) {
-          const unsigned idx = base + __popc(mm & lt);
-          if (idx < (unsigned)nn) *(volatile int*)&queue[idx] = dep[t];
-          else atomicExch(err, DEV_OVERFLOW);
-        }
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(FULL, off, o);
+        if (lane >= o) off += y;
       }
+      const unsigned total = __shfl_sync(FULL, off, 31);
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(qtail, total);
+      base = __shfl_sync(FULL, base, 0) + off - mine;
+#pragma unroll
+      for (int t = 0; t < 8; ++t)
+        if ((rdy >> t) & 1u) {
+          if (base < (unsigned)nn) *(volatile int*)&queue[base] = dep[t];
+          else atomicExch(err, DEV_OVERFLOW);
+          ++base;
+        }
     }
     const unsigned busy = __ballot_sync(FULL, cur >= 0);
     if (!busy) {
@@ -155,7 +158,7 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, i
       e = __shfl_sync(FULL, e, 0);
       if (d >= (unsigned)nn || e != 0) return;
       __nanosleep(back);
-      if (back < 256) back <<= 1;
+      if (back < 256) back <<= 1;  // longer caps were measured slower (4 us: +1.6 ms at 2049^2)
     } else {
       back = 32;
     }
@@ -323,15 +326,15 @@ struct AccMfdOp {
   double* lsed = nullptr;
   __device__ void prefetch(int k) const { prefetch_l1(line + k); }
   __device__ int run(int k, int* dep, unsigned* pr) const {
+    // the input slots do not depend on the line: load them together with it
+    const double* in = slots + (size_t)k * kSlotStride;
+    double av[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) av[t] = ld_relaxed_gpu(&in[t]);
     // aw = d[0..7], base = d[8], don = u[18], rcv = u[19], pr = s[40..47], rpos = u[24]
     const LineWords<7> L(line + k);
     const NbrDecoder nb(k, nx, ny);
     const unsigned dc = L.u[18], rc = L.u[19], rpos = L.u[24];
-    const double* in = slots + (size_t)k * kSlotStride;
-    double av[8];
-#pragma unroll
-    for (int t = 0; t < 8; ++t)
-      if ((dc >> (4 * t)) & 15u) av[t] = ld_relaxed_gpu(&in[t]);
 #pragma unroll
     for (int t = 0; t < 8; ++t)
       if ((dc >> (4 * t)) & 15u) av[t] = slot_value(&in[t], av[t], err);
@@ -390,6 +393,13 @@ struct SplMfdOp {
   int* sill = nullptr;
   double* contrib = nullptr;
   __device__ int run(int k, int* dep, unsigned* pr) const {
+    // the input slots do not depend on the line: load them together with it
+    const double* in = slots + (size_t)k * kSlotStride;
+    double hq[8], wr, sv = 0.0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) hq[t] = ld_relaxed_gpu(&in[t]);
+    wr = ld_relaxed_gpu(&in[8]);
+    if (GS) sv = ld_relaxed_gpu(&in[9]);
     // fact = d[0..7], ht = d[8], q = u[18], dep = u[19], pr = s[40..47], meta = u[24],
     // qmask = u[25..26], wflag = u[27]
     const LineWords<7> L(line + k);
@@ -411,12 +421,6 @@ struct SplMfdOp {
     double ck = 0.0;
     const unsigned rcode = meta & 15u;
     if (rcode) {
-      const double* in = slots + (size_t)k * kSlotStride;
-      double hq[8];
-      double wr = ld_relaxed_gpu(&in[8]);
-#pragma unroll
-      for (int t = 0; t < 8; ++t)
-        if ((qc >> (4 * t)) & 15u) hq[t] = ld_relaxed_gpu(&in[t]);
       wr = slot_value(&in[8], wr, err);
 #pragma unroll
       for (int t = 0; t < 8; ++t)
@@ -459,7 +463,6 @@ struct SplMfdOp {
       } else {
         hk = elev;
         if (GS) {
-          const double sv = ld_relaxed_gpu(&in[9]);
           sk = (int)__double_as_longlong(slot_value(&in[9], sv, err));
           ck = wr - hk;
         }
