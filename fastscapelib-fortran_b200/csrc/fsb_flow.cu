@@ -38,10 +38,9 @@ __device__ inline unsigned long long ordered_key(double x) {
 
 // ---- last-arriver sweep engine ----------------------------------------------
 // Op::run(k, dep[], pr[]) computes node k, stores its outputs and lists
-// k's dependents with their priorities; the engine then decrements their
-// counters, continues with the ready dependent of largest priority (subtree
-// size), prefetching its record (Op::prefetch), and queues the other ready
-// ones.  Idle lanes claim queue slots in
+// k's dependents with their priorities (prefetching their records); the
+// engine then decrements their counters, continues with the ready dependent
+// of largest priority (subtree size) and queues the other ready ones.  Idle lanes claim queue slots in
 // order (one atomic per warp) and keep a claim until a producer fills it.
 // The kernel ends when every node is done.
 // Control words: ctl[0] queue head, ctl[32] queue tail, ctl[64] nodes done
@@ -121,7 +120,6 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, i
             if (bi < 0 || pr[t] > bp) { bp = pr[t]; bi = t; nxt = dep[t]; }
           }
         if (bi >= 0) rdy &= ~(1u << bi);
-        if (nxt >= 0) op.prefetch(nxt);  // the continuation's record line into L1
       }
       ++local_done;
       cur = nxt;
@@ -279,6 +277,21 @@ struct NewtonPow {
 };
 
 __device__ inline void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+__device__ inline void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+// As soon as a node knows its dependents it prefetches their record lines
+// into L1 and their slot rows into L2, overlapping those fetches with its own
+// arithmetic and counter atomics (2049^2 step 60.5 -> 58.9 ms; prefetching
+// only the continuation's line after the atomics, or the lines into L2
+// only, measured slower).
+template <class Line>
+__device__ inline void prefetch_dependents(const Line* line, const double* slots, const int* dep, int nd) {
+#pragma unroll
+  for (int t = 0; t < 8; ++t)
+    if (t < nd) {
+      prefetch_l1(line + dep[t]);
+      prefetch_l2(slots + (size_t)dep[t] * kSlotStride);
+    }
+}
 
 // the first N 16-byte words of a record line (read-only during the sweep)
 template <int N>
@@ -324,7 +337,6 @@ struct AccMfdOp {
   const int* rec = nullptr;
   const int* sill = nullptr;
   double* lsed = nullptr;
-  __device__ void prefetch(int k) const { prefetch_l1(line + k); }
   __device__ int run(int k, int* dep, unsigned* pr) const {
     // the input slots do not depend on the line: load them together with it
     const double* in = slots + (size_t)k * kSlotStride;
@@ -348,6 +360,7 @@ struct AccMfdOp {
         nd = t + 1;
       }
     }
+    prefetch_dependents(line, slots, dep, nd);
     double acc = L.d[8];
 #pragma unroll
     for (int t = 0; t < 8; ++t)
@@ -381,7 +394,6 @@ template <bool GS>
 struct SplMfdOp {
   const SplLine* line;
   int nx, ny;
-  __device__ void prefetch(int k) const { prefetch_l1(line + k); }
   NewtonPow np;
   double omega;
   int n_is_one;
@@ -416,6 +428,7 @@ struct SplMfdOp {
         nd = t + 1;
       }
     }
+    prefetch_dependents(line, slots, dep, nd);
     double hk = ht, wk = ht;
     int sk = k;
     double ck = 0.0;
