@@ -126,13 +126,13 @@ __global__ void __launch_bounds__(128) k_last_arriver(Op op, int nn, int* cnt, i
     }
     if (__ballot_sync(FULL, rdy != 0)) {  // queue the other ready nodes: one atomic per warp
       const unsigned mine = __popc(rdy);
-      unsigned off = mine;  // inclusive prefix of the lanes' counts
+      unsigned off = mine;  // inclusive prefix of the lanes' counts (only lanes < LANES have any)
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
+      for (int o = 1; o < LANES; o <<= 1) {
         const unsigned y = __shfl_up_sync(FULL, off, o);
         if (lane >= o) off += y;
       }
-      const unsigned total = __shfl_sync(FULL, off, 31);
+      const unsigned total = __shfl_sync(FULL, off, LANES - 1);
       unsigned base = 0;
       if (lane == 0) base = atomicAdd(qtail, total);
       base = __shfl_sync(FULL, base, 0) + off - mine;
@@ -335,6 +335,15 @@ __device__ inline double slot_value(const double* p, double v, int* err) {
   }
   return v;
 }
+// Bit t set when input slot t (in the 4-bit code word c) still holds the sentinel:
+// one test for all of a node's inputs, so the usual case takes no branch per slot.
+__device__ inline unsigned empty_slots(const double* v, unsigned c) {
+  unsigned m = 0;
+#pragma unroll
+  for (int t = 0; t < 8; ++t)
+    m |= (((c >> (4 * t)) & 15u) && __double_as_longlong(v[t]) == kSlotEmpty ? 1u : 0u) << t;
+  return m;
+}
 
 // a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115);
 // k's dependents are its distinct receivers.  With `clamp` set and lines
@@ -362,9 +371,11 @@ struct AccMfdOp {
     // aw = d[0..7], base = d[8], dep = u[18..25], don = u[26], rpos = u[27]
     const LineWords<7> L(line + k);
     const unsigned dc = L.u[26], rpos = L.u[27];
+    if (empty_slots(av, dc)) {
 #pragma unroll
-    for (int t = 0; t < 8; ++t)
-      if ((dc >> (4 * t)) & 15u) av[t] = slot_value(&in[t], av[t], err);
+      for (int t = 0; t < 8; ++t)
+        if ((dc >> (4 * t)) & 15u) av[t] = slot_value(&in[t], av[t], err);
+    }
     int nd = 0;
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
@@ -440,9 +451,11 @@ struct SplMfdOp {
     const unsigned rcode = meta & 15u;
     if (rcode) {
       wr = slot_value(&in[8], wr, err);
+      if (empty_slots(hq, qc)) {
 #pragma unroll
-      for (int t = 0; t < 8; ++t)
-        if ((qc >> (4 * t)) & 15u) hq[t] = slot_value(&in[t], hq[t], err);
+        for (int t = 0; t < 8; ++t)
+          if ((qc >> (4 * t)) & 15u) hq[t] = slot_value(&in[t], hq[t], err);
+      }
       if (GS) hk = hstart[k];
       const double elev = GS ? this->elev[k] : ht;
       if (elev > wr) {
@@ -498,10 +511,11 @@ struct SplMfdOp {
     for (int t = 0; t < 8; ++t) {
       if (t >= nd) break;
       double* out = slots + (size_t)dep[t] * kSlotStride;
-      const unsigned m = (L.u[28 + (t >> 2)] >> (8 * (t & 3))) & 0xffu;
-#pragma unroll
-      for (int p = 0; p < 8; ++p)
-        if ((m >> p) & 1u) st_relaxed_gpu(&out[p], hk);
+      unsigned m = (L.u[28 + (t >> 2)] >> (8 * (t & 3))) & 0xffu;
+      while (m) {  // usually one bit
+        st_relaxed_gpu(&out[__ffs(m) - 1], hk);
+        m &= m - 1u;
+      }
       if ((wflag >> t) & 1u) {
         st_relaxed_gpu(&out[8], wk);
         if (GS) st_relaxed_gpu(&out[9], __longlong_as_double((long long)sk));
