@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cuda/atomic>
 #include <cfloat>
+#include <cstddef>
 
 #include "fsb_kernels.cuh"
 
@@ -229,20 +230,56 @@ struct __align__(128) SplLine {
   int pad;
 };
 static_assert(sizeof(AccLine) == 128 && sizeof(SplLine) == 128, "one line per node");
+static_assert(offsetof(AccLine, dep) == 72 && offsetof(AccLine, don) == 104 && offsetof(AccLine, rpos) == 108,
+              "AccLine words: aw 0-15, base 16-17, dep 18-25, don 26, rpos 27");
+static_assert(offsetof(SplLine, dep) == 72 && offsetof(SplLine, q) == 104 && offsetof(SplLine, meta) == 108 &&
+                  offsetof(SplLine, qmask) == 112 && offsetof(SplLine, wflag) == 120,
+              "SplLine words: fact 0-15, ht 16-17, dep 18-25, q 26, meta 27, qmask 28-29, wflag 30");
 
 __device__ inline unsigned short prio16(int size) { return (unsigned short)(__float_as_uint((float)size) >> 16); }
 
-// Inserts node v of priority p as the n-th entry of dep[] / pr[], kept in
+// The line builders keep their short lists in registers: every entry is
+// addressed by an index known after unrolling, selected by a predicate.
+// Inserts node v of priority p into dep[0..n) / pr[0..n) (n < 8), kept in
 // decreasing priority with ties in insertion order.
-__device__ inline void insert_by_priority(int* dep, unsigned short* pr, int n, int v, unsigned short p) {
-  int t = n;
-  while (t > 0 && pr[t - 1] < p) {
-    dep[t] = dep[t - 1];
-    pr[t] = pr[t - 1];
-    --t;
-  }
-  dep[t] = v;
-  pr[t] = p;
+__device__ inline void insert_by_priority(int (&dep)[8], unsigned (&pr)[8], int n, int v, unsigned p) {
+  int pos = 0;  // entries of priority >= p stay in front
+#pragma unroll
+  for (int t = 0; t < 8; ++t) pos += (t < n && pr[t] >= p) ? 1 : 0;
+#pragma unroll
+  for (int t = 7; t > 0; --t)
+    if (t > pos && t <= n) {
+      dep[t] = dep[t - 1];
+      pr[t] = pr[t - 1];
+    }
+#pragma unroll
+  for (int t = 0; t < 8; ++t)
+    if (t == pos) {
+      dep[t] = v;
+      pr[t] = p;
+    }
+}
+template <class T>
+__device__ inline void set_at(T (&a)[8], int n, T v) {
+#pragma unroll
+  for (int t = 0; t < 8; ++t)
+    if (t == n) a[t] = v;
+}
+template <class T>
+__device__ inline bool contains(const T (&a)[8], int n, T v) {
+  bool f = false;
+#pragma unroll
+  for (int t = 0; t < 8; ++t) f |= t < n && a[t] == v;
+  return f;
+}
+__device__ inline int4 pack2(double a, double b) {
+  return make_int4(__double2loint(a), __double2hiint(a), __double2loint(b), __double2hiint(b));
+}
+// Writes a record line from its 32 words: eight 16-byte stores.
+__device__ inline void store_line(void* dst, const int4 (&w)[8]) {
+  int4* p = reinterpret_cast<int4*>(dst);
+#pragma unroll
+  for (int t = 0; t < 8; ++t) p[t] = w[t];
 }
 
 __device__ inline unsigned nbr_code(int di, int dj) { return 1u + 3u * (unsigned)(dj + 1) + (unsigned)(di + 1); }
@@ -580,52 +617,68 @@ __global__ void k_acc_lines(Bounds bd, double dxdy, const int* __restrict__ mrec
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
     const int i = k % nx, j = k / nx;
     const size_t o = (size_t)k * 8;
-    AccLine L;
     // distinct receivers (dependents), largest priority first
     const int nr = mnrec[k];
-    unsigned short pr[8];
+    int mr[8], dep[8];
+    unsigned pr[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      mr[t] = t < nr ? mrec[o + t] : -1;
+      dep[t] = -1;
+      pr[t] = 0u;
+    }
     int rn = 0;
-    for (int t = 0; t < 8; ++t) L.dep[t] = -1;
-    for (int t = 0; t < nr; ++t) {
-      const int q = mrec[o + t];
-      bool dup = false;
-      for (int u = 0; u < t; ++u) dup |= mrec[o + u] == q;
-      if (dup) continue;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      if (t >= nr) break;
+      const int q = mr[t];
+      if (contains(mr, t, q)) continue;
       (void)nbr_code_of(i, j, q, nx, ny, err);  // checks that q is a neighbour
-      insert_by_priority(L.dep, pr, rn++, q, prio16(prio[q]));
+      insert_by_priority(dep, pr, rn++, q, prio16(prio[q]));
     }
     // distinct donors among the 3x3 neighbours and the summed weight of their slots to k
     unsigned don = 0;
     int an = 0, ns = 0;
-    int seen[9];
-    for (int t = 0; t < 8; ++t) L.aw[t] = 0.0;
+    int seen[8];
+    double aw[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) aw[t] = 0.0;
+#pragma unroll
     for (int jj = -1; jj <= 1; ++jj) {
       int y = j + jj;
       if (y < 0) { if (!bd.ycyc) continue; y += ny; }
       if (y >= ny) { if (!bd.ycyc) continue; y -= ny; }
+#pragma unroll
       for (int ii = -1; ii <= 1; ++ii) {
         int x = i + ii;
         if (x < 0) { if (!bd.xcyc) continue; x += nx; }
         if (x >= nx) { if (!bd.xcyc) continue; x -= nx; }
         const int d = x + y * nx;
-        if (d == k) continue;
-        bool dup = false;
-        for (int t = 0; t < ns; ++t) dup |= seen[t] == d;
-        if (dup) continue;
-        seen[ns++] = d;
+        if (d == k || contains(seen, ns, d)) continue;
+        set_at(seen, ns++, d);
         const int nd = mnrec[d];
         double wsum = 0.0;
         int hits = 0;
-        for (int t = 0; t < nd; ++t)
-          if (mrec[(size_t)d * 8 + t] == k) { wsum = hits ? wsum + mwrec[(size_t)d * 8 + t] : mwrec[(size_t)d * 8 + t]; ++hits; }
-        if (hits && an < 8) { don |= nbr_code(ii, jj) << (4 * an); L.aw[an] = wsum; ++an; }
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+          if (t < nd && mrec[(size_t)d * 8 + t] == k) {
+            const double w = mwrec[(size_t)d * 8 + t];
+            wsum = hits ? wsum + w : w;
+            ++hits;
+          }
+        if (hits && an < 8) {
+          don |= nbr_code(ii, jj) << (4 * an);
+          set_at(aw, an++, wsum);
+        }
       }
     }
-    L.base = dxdy * precip[k];
-    L.don = don;
-    L.rpos = 0;
-    for (int t = 0; t < 4; ++t) L.pad[t] = 0;
-    line[k] = L;
+    const double base = dxdy * precip[k];
+    const int4 w[8] = {pack2(aw[0], aw[1]), pack2(aw[2], aw[3]), pack2(aw[4], aw[5]), pack2(aw[6], aw[7]),
+                       make_int4(__double2loint(base), __double2hiint(base), dep[0], dep[1]),
+                       make_int4(dep[2], dep[3], dep[4], dep[5]),
+                       make_int4(dep[6], dep[7], (int)don, 0),  // rpos: filled by k_acc_slotpos
+                       make_int4(0, 0, 0, 0)};
+    store_line(line + k, w);
     cnt_acc[k] = an;
   }
 }
@@ -642,72 +695,76 @@ __global__ void k_spl_lines(Bounds bd, int n_is_one, double kfsed, double dt, do
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
     const int i = k % nx, j = k / nx;
     const size_t o = (size_t)k * 8;
-    SplLine L;
     const double htk = h[k];
     const int nr = mnrec[k];
     const int r = rec[k];
     const double kk = ((kfsed > 0.0 && (htk - b[k]) > 1.0) ? kfsed : kf[k]) * dt;
     const double ak = a[k];
-    int qv[8];
+    int qv[8], dep[8];
+    unsigned pr[8];
+    double fact[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      qv[t] = -1;
+      dep[t] = -1;
+      pr[t] = 0u;
+      fact[t] = 0.0;
+    }
     unsigned qc = 0;
     int nq = 0;
-    unsigned short pr[8];
-    for (int t = 0; t < 8; ++t) { L.fact[t] = 0.0; L.dep[t] = -1; }
-    for (int t = 0; t < nr; ++t) {
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      if (t >= nr) break;
       const int q = mrec[o + t];
       if (n_is_one ? (htk >= h[q]) : (htk > h[q])) {
         const double w = mwrec[o + t], l = mlrec[o + t];
-        qv[nq] = q;
         qc |= nbr_code_of(i, j, q, nx, ny, err) << (4 * nq);
-        L.fact[nq] = n_is_one ? kk * pow(ak * w, m) / l : kk * pow(ak * w, m) / pow(l, n);
-        ++nq;
+        set_at(fact, nq, n_is_one ? kk * pow(ak * w, m) / l : kk * pow(ak * w, m) / pow(l, n));
+        set_at(qv, nq++, q);
       }
     }
     int cs = 0;
     if (r != k) {
-      for (int t = 0; t < nq; ++t) {
-        bool dup = false;
-        for (int u = 0; u < t; ++u) dup |= qv[u] == qv[t];
-        if (!dup) ++cs;
-      }
-      bool r_gated = false;
-      for (int t = 0; t < nq; ++t) r_gated |= qv[t] == r;
-      if (!r_gated) ++cs;
+#pragma unroll
+      for (int t = 0; t < 8; ++t)
+        if (t < nq && !contains(qv, t, qv[t])) ++cs;
+      if (!contains(qv, nq, r)) ++cs;
     }
     // donors that wait for k: they read hnew(k) (gated) or water(k) (rec == k),
     // largest priority first
     int dn = 0, ns = 0;
-    int seen[9];
+    int seen[8];
+#pragma unroll
     for (int jj = -1; jj <= 1; ++jj) {
       int y = j + jj;
       if (y < 0) { if (!bd.ycyc) continue; y += ny; }
       if (y >= ny) { if (!bd.ycyc) continue; y -= ny; }
+#pragma unroll
       for (int ii = -1; ii <= 1; ++ii) {
         int x = i + ii;
         if (x < 0) { if (!bd.xcyc) continue; x += nx; }
         if (x >= nx) { if (!bd.xcyc) continue; x -= nx; }
         const int d = x + y * nx;
-        if (d == k) continue;
-        bool dup = false;
-        for (int t = 0; t < ns; ++t) dup |= seen[t] == d;
-        if (dup) continue;
-        seen[ns++] = d;
+        if (d == k || contains(seen, ns, d)) continue;
+        set_at(seen, ns++, d);
         const int rd = rec[d];
         if (rd == d) continue;
         bool hits = false;
         const int nd = mnrec[d];
-        for (int t = 0; t < nd; ++t) hits |= mrec[(size_t)d * 8 + t] == k;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) hits |= t < nd && mrec[(size_t)d * 8 + t] == k;
         const bool gated = hits && (n_is_one ? (h[d] >= htk) : (h[d] > htk));
-        if ((gated || rd == k) && dn < 8) insert_by_priority(L.dep, pr, dn++, d, prio16(prio[d]));
+        if ((gated || rd == k) && dn < 8) insert_by_priority(dep, pr, dn++, d, prio16(prio[d]));
       }
     }
-    L.ht = htk;
-    L.q = qc;
-    L.meta = (int)((r != k ? nbr_code_of(i, j, r, nx, ny, err) : 0u) | (nr > 0 ? 16u : 0u));
-    L.qmask[0] = L.qmask[1] = 0;
-    L.wflag = 0;
-    L.pad = 0;
-    line[k] = L;
+    const int meta = (int)((r != k ? nbr_code_of(i, j, r, nx, ny, err) : 0u) | (nr > 0 ? 16u : 0u));
+    const int4 w[8] = {pack2(fact[0], fact[1]), pack2(fact[2], fact[3]), pack2(fact[4], fact[5]),
+                       pack2(fact[6], fact[7]),
+                       make_int4(__double2loint(htk), __double2hiint(htk), dep[0], dep[1]),
+                       make_int4(dep[2], dep[3], dep[4], dep[5]),
+                       make_int4(dep[6], dep[7], (int)qc, meta),
+                       make_int4(0, 0, 0, 0)};  // qmask, wflag: filled by k_spl_slotpos
+    store_line(line + k, w);
     cnt_spl[k] = cs;
   }
 }
