@@ -55,7 +55,9 @@ __device__ inline unsigned long long ordered_key(double x) {
 // its warp mates' loads and Newton iterations.  The sweeps are bound by their
 // critical path, not by node throughput; at 2049^2 (B200) 8 lanes suit the
 // area sweep and 1 lane the stream-power sweep (32 lanes: 25.8 and 46.1 ms,
-// these: 24.4 and 41.2 ms).
+// these: 24.4 and 41.2 ms).  Re-measured with the dependents stored as node
+// indices: area sweep 14.2 ms with 8 lanes, 14.7 / 15.4 / 16.0 ms with 4 / 2 / 1
+// (grids of side/4, /2, /1 blocks).
 #ifndef FSB_LANES_ACC
 #define FSB_LANES_ACC 8
 #endif
