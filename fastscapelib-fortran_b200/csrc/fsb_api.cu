@@ -138,6 +138,7 @@ size_t layout(fsb::Ctx& c, char* base) {
   c.nr_lpos = L.take<int>(E + 2); c.nr_rpos = L.take<int>(E + 2);
   c.nr_segof = L.take<int>(E + 2);
   c.nr_seg = L.take<int>(E + 8); c.nr_seg2 = L.take<int>(E + 8); c.nr_small = L.take<int>(E + 16);
+  c.nr_med = L.take<int>(2 * (E / 8 + 8));
   c.nr_piv = L.take<double>(E / 2 + 8); c.nr_segmeta = L.take<int>(2 * E + 32);
   c.nr_bsum_cap = 2 * 4096; c.nr_bsum = L.take<int>(c.nr_bsum_cap);
   c.e_rank = L.take<int>(E); c.e_inmst = L.take<int>(E); c.tree = L.take<int>(N);

@@ -88,6 +88,7 @@ struct Ctx {
       *nr_rs = nullptr, *nr_lpos = nullptr, *nr_rpos = nullptr, *nr_segof = nullptr;
   int *nr_seg = nullptr, *nr_seg2 = nullptr;  // segments: pairs (l, ir), 1-based
   int *nr_small = nullptr;                    // small segments (l, ir)
+  int *nr_med = nullptr;                      // segments of 8..512 elements (l, ir), finished in shared memory
   double* nr_piv = nullptr;
   int* nr_segmeta = nullptr;  // per segment: pv, i, j, T
   int *e_rank = nullptr, *e_inmst = nullptr, *tree = nullptr;

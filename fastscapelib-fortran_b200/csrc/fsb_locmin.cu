@@ -34,8 +34,15 @@ namespace {
 enum {
   C_NBASINS = 0, C_NLOCMIN = 1, C_BASIN0 = 2, C_NEDGE = 3, C_NSEG = 4, C_NSMALL = 5,
   C_CHANGED = 6, C_NTREE = 7, C_NLOCMIN_AFTER = 8, C_OVERFLOW = 9, C_NOTFLAT = 10, C_NSEG2 = 11,
-  C_NRIDX = 12, C_NRLEVELS = 13
+  C_NRIDX = 12, C_NRLEVELS = 13, C_NMED = 14
 };
+constexpr int kNrCounters = 15;  // counters the NR sort reads back
+
+// Segments of 8..kNrMedium elements leave the level-synchronous partition and
+// are finished each by one warp in shared memory (k_nr_medium): the last
+// levels of the sort, which hold only such segments, would otherwise each
+// cost a round of grid-wide barriers.
+constexpr int kNrMedium = 512;
 
 __constant__ int c_ii[8] = {-1, 1, 0, 0, -1, 1, -1, 1};
 __constant__ int c_jj[8] = {0, 0, -1, 1, -1, -1, 1, 1};
@@ -202,15 +209,18 @@ __global__ void k_conn_gather(int n, const int* __restrict__ perm, const int* __
 // ---- loc_min_3_indexx emulation (1-based positions l..ir) -----------------
 // idx[1..n] holds 1-based edge ids, arr[1..n] the weights (arr = w - 1).
 __global__ void k_nr_init(int n, int* __restrict__ idx, int* __restrict__ segof, int* __restrict__ seg,
-                          int* __restrict__ small, int* __restrict__ cnt) {
+                          int* __restrict__ small, int* __restrict__ med, int* __restrict__ cnt) {
+  const bool level = n > kNrMedium;  // else the whole array is one medium or small segment
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= n + 1; q += gridDim.x * blockDim.x) {
     if (q >= 1 && q <= n) idx[q] = q;
-    segof[q] = (q >= 1 && q <= n && n - 1 >= 7) ? 0 : -1;
+    segof[q] = (q >= 1 && q <= n && level) ? 0 : -1;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    if (n - 1 >= 7) { seg[0] = 1; seg[1] = n; cnt[C_NSEG] = 1; }
-    else if (n >= 2) { small[0] = 1; small[1] = n; cnt[C_NSMALL] = 1; cnt[C_NSEG] = 0; }
-    else cnt[C_NSEG] = 0;
+    cnt[C_NSEG] = 0;
+    cnt[C_NMED] = 0;
+    if (level) { seg[0] = 1; seg[1] = n; cnt[C_NSEG] = 1; }
+    else if (n - 1 >= 7) { med[0] = 1; med[1] = n; cnt[C_NMED] = 1; }
+    else if (n >= 2) { small[0] = 1; small[1] = n; cnt[C_NSMALL] = 1; }
   }
 }
 
@@ -313,17 +323,23 @@ __device__ inline int nr_apply_one(int q, const int* segof, const int* seg,
   return nr_newval(q, l, ir, T, idx, lf, rf, ls, rs, lpos, rpos);
 }
 
-// children segments [l, j-1] and [i, ir]: partitioned further when they hold
-// at least M+1=8 elements (counted in cnt[out_slot]), insertion-sorted otherwise
+// children segments [l, j-1] and [i, ir]: partitioned at the next level when
+// they hold more than kNrMedium elements (counted in cnt[out_slot]), finished
+// in shared memory when they hold 8..kNrMedium (cnt[C_NMED]), insertion-sorted
+// when fewer (M = 7)
 __device__ inline void nr_newsegs_one(int s, int out_slot, const int* seg, int* meta,
-                                      int* seg2, int* small, int* cnt,
-                                      int small_cap) {
+                                      int* seg2, int* small, int* med, int* cnt,
+                                      int small_cap, int med_cap) {
   const int l = seg[2 * s], ir = seg[2 * s + 1];
   const int i = meta[4 * s + 1], j = meta[4 * s + 2];
   int ids[2] = {-1, -1};
   const int lo[2] = {l, i}, hi[2] = {j - 1, ir};
   for (int c = 0; c < 2; ++c) {
-    if (hi[c] - lo[c] >= 7) {
+    if (hi[c] - lo[c] >= 7 && hi[c] - lo[c] < kNrMedium) {
+      const int id = atomicAdd(&cnt[C_NMED], 1);
+      if (id < med_cap) { med[2 * id] = lo[c]; med[2 * id + 1] = hi[c]; }
+      else atomicExch(&cnt[C_OVERFLOW], 1);
+    } else if (hi[c] - lo[c] >= 7) {
       const int id = atomicAdd(&cnt[out_slot], 1);
       seg2[2 * id] = lo[c];
       seg2[2 * id + 1] = hi[c];
@@ -400,11 +416,11 @@ __global__ void k_nr_apply(int n, const int* __restrict__ segof, const int* __re
 // reads the level's segment count from cnt[in_slot] and counts the next
 // level's segments in cnt[out_slot] (zeroed before the launch)
 __global__ void k_nr_newsegs(int in_slot, int out_slot, const int* __restrict__ seg, int* __restrict__ meta,
-                             int* __restrict__ seg2, int* __restrict__ small, int* __restrict__ cnt,
-                             int small_cap) {
+                             int* __restrict__ seg2, int* __restrict__ small, int* __restrict__ med,
+                             int* __restrict__ cnt, int small_cap, int med_cap) {
   const int nseg = cnt[in_slot];
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x)
-    nr_newsegs_one(s, out_slot, seg, meta, seg2, small, cnt, small_cap);
+    nr_newsegs_one(s, out_slot, seg, meta, seg2, small, med, cnt, small_cap, med_cap);
 }
 
 __global__ void k_nr_segof(int n, const int* __restrict__ seg, const int* __restrict__ meta,
@@ -424,9 +440,9 @@ __global__ void k_nr_segof(int n, const int* __restrict__ seg, const int* __rest
 struct NrCoop {
   int n;
   const double* arr;
-  int *idx, *idx2, *seg, *seg2, *segof, *lf, *rf, *ls, *rs, *lpos, *rpos, *meta, *small, *cnt, *bsum;
+  int *idx, *idx2, *seg, *seg2, *segof, *lf, *rf, *ls, *rs, *lpos, *rpos, *meta, *small, *med, *cnt, *bsum;
   double* piv;
-  int small_cap;
+  int small_cap, med_cap;
 };
 
 constexpr int kCoopThreads = 256;
@@ -530,7 +546,8 @@ __global__ void __launch_bounds__(kCoopThreads) k_nr_levels(NrCoop A) {
     for (int q = tid + 1; q <= n; q += nthreads)
       idx2[q] = nr_apply_one(q, A.segof, seg, A.meta, idx, A.lf, A.rf, A.ls, A.rs, A.lpos, A.rpos);
     grid.sync();
-    for (int s = tid; s < nseg; s += nthreads) nr_newsegs_one(s, out, seg, A.meta, seg2, A.small, A.cnt, A.small_cap);
+    for (int s = tid; s < nseg; s += nthreads)
+      nr_newsegs_one(s, out, seg, A.meta, seg2, A.small, A.med, A.cnt, A.small_cap, A.med_cap);
     grid.sync();
     for (int q = tid; q <= n + 1; q += nthreads) nr_segof_one(q, seg, A.meta, A.segof);
     grid.sync();
@@ -561,6 +578,96 @@ __global__ void k_nr_insertion(int nsmall, const int* __restrict__ small, const 
       }
       idx[i + 1] = indxt;
     }
+  }
+}
+
+// The whole NR quicksort of one segment of 8..kNrMedium elements, as the
+// reference runs it (LocalMinima.f90:953-1044: median of three, Hoare scans,
+// larger part stacked, straight insertion below M = 7), by one thread on the
+// segment's keys and ids in shared memory; positions are relative to the
+// segment (the median index (l+ir)/2 keeps its value relative to l).
+// Segments are independent, so the order they are finished in does not
+// matter, and the insertion stops at the segment's start as k_nr_insertion's does.
+__device__ bool nr_sort_local(double* key, int* id, int n) {
+  int stk[32];
+  int js = 0, l = 0, ir = n - 1;
+  for (int it = 0; it < 4 * kNrMedium; ++it) {
+    if (ir - l < 7) {
+      for (int j = l + 1; j <= ir; ++j) {
+        const double a = key[j];
+        const int v = id[j];
+        int i = j - 1;
+        for (; i >= l; --i) {
+          if (key[i] <= a) break;
+          key[i + 1] = key[i];
+          id[i + 1] = id[i];
+        }
+        key[i + 1] = a;
+        id[i + 1] = v;
+      }
+      if (js == 0) return true;
+      ir = stk[--js];
+      l = stk[--js];
+    } else {
+      auto swap = [&](int x, int y) {
+        const double t = key[x]; key[x] = key[y]; key[y] = t;
+        const int u = id[x]; id[x] = id[y]; id[y] = u;
+      };
+      swap((l + ir) / 2, l + 1);
+      if (key[l + 1] > key[ir]) swap(l + 1, ir);
+      if (key[l] > key[ir]) swap(l, ir);
+      if (key[l + 1] > key[l]) swap(l + 1, l);
+      int i = l + 1, j = ir;
+      const double a = key[l];
+      const int v = id[l];
+      for (;;) {  // the median of three leaves stoppers at l+1 and ir
+        do ++i; while (key[i] < a);
+        do --j; while (key[j] > a);
+        if (j < i) break;
+        swap(i, j);
+      }
+      key[l] = key[j];
+      id[l] = id[j];
+      key[j] = a;
+      id[j] = v;
+      if (js + 2 > 32) return false;  // depth <= 2*log2(kNrMedium) = 18
+      if (ir - i + 1 >= j - l) {
+        stk[js++] = i;
+        stk[js++] = ir;
+        ir = j - 1;
+      } else {
+        stk[js++] = l;
+        stk[js++] = j - 1;
+        l = i;
+      }
+    }
+  }
+  return false;
+}
+
+constexpr int kNrMedWarps = 4;
+__global__ void __launch_bounds__(32 * kNrMedWarps) k_nr_medium(int nmed, const int* __restrict__ med,
+                                                               const double* __restrict__ arr, int* __restrict__ idx,
+                                                               int* __restrict__ cnt) {
+  __shared__ double key[kNrMedWarps][kNrMedium];
+  __shared__ int id[kNrMedWarps][kNrMedium];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int s = blockIdx.x * kNrMedWarps + w; s < nmed; s += gridDim.x * kNrMedWarps) {
+    const int l = med[2 * s], n = med[2 * s + 1] - l + 1;
+    if (n < 8 || n > kNrMedium) {  // never: nr_newsegs_one routes only such segments here
+      if (lane == 0) atomicExch(&cnt[C_OVERFLOW], 1);
+      continue;
+    }
+    for (int p = lane; p < n; p += 32) {
+      const int v = idx[l + p];
+      id[w][p] = v;
+      key[w][p] = arr[v];
+    }
+    __syncwarp();
+    if (lane == 0 && !nr_sort_local(key[w], id[w], n)) atomicExch(&cnt[C_OVERFLOW], 1);
+    __syncwarp();
+    for (int p = lane; p < n; p += 32) idx[l + p] = id[w][p];
+    __syncwarp();
   }
 }
 
@@ -746,6 +853,8 @@ __global__ void k_copy_nroots(const int* src, int* cnt) {
 // 1-based ids in sorted order.  Returns false on buffer overflow.
 // All levels in one cooperative launch; false when the device cannot run it
 // (the caller then runs one launch per level).  Reads the counters back.
+static int nr_med_cap(const Ctx& c) { return (int)(c.conn_cap / 8 + 8); }
+
 static bool nr_levels_coop(Ctx& c, int n, const double* arr, int small_cap) {
   int dev = 0, coop = 0, sms = 0, per_sm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||
@@ -757,8 +866,9 @@ static bool nr_levels_coop(Ctx& c, int n, const double* arr, int small_cap) {
   // about 2048 positions per block, at most what is resident at once
   const int want = (n + 2 + 2047) / 2048;
   const int blocks = std::max(1, std::min(want, std::min(sms * per_sm, c.nr_bsum_cap / 2)));
-  NrCoop A{n, arr, c.nr_idx, c.nr_idx2, c.nr_seg, c.nr_seg2, c.nr_segof, c.nr_lf, c.nr_rf, c.nr_ls, c.nr_rs,
-           c.nr_lpos, c.nr_rpos, c.nr_segmeta, c.nr_small, c.d_cnt, c.nr_bsum, c.nr_piv, small_cap};
+  NrCoop A{n,         arr,       c.nr_idx,  c.nr_idx2, c.nr_seg,     c.nr_seg2,  c.nr_segof,
+           c.nr_lf,   c.nr_rf,   c.nr_ls,   c.nr_rs,   c.nr_lpos,    c.nr_rpos,  c.nr_segmeta,
+           c.nr_small, c.nr_med, c.d_cnt,   c.nr_bsum, c.nr_piv,     small_cap,  nr_med_cap(c)};
   void* args[] = {&A};
   if (cudaLaunchCooperativeKernel((const void*)k_nr_levels, dim3(blocks), dim3(kCoopThreads), args, 0, c.stream) !=
       cudaSuccess) {
@@ -766,7 +876,7 @@ static bool nr_levels_coop(Ctx& c, int n, const double* arr, int small_cap) {
     return false;
   }
   c.count_launch();
-  fetch_counters(c, 14);
+  fetch_counters(c, kNrCounters);
   return true;
 }
 
@@ -777,9 +887,9 @@ static bool nr_indexx(Ctx& c, int n, const double* w) {
   int* seg = c.nr_seg;
   int* seg2 = c.nr_seg2;
   const int small_cap = (int)(c.conn_cap / 2 + 8);
-  k_nr_init<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, idx, c.nr_segof, seg, c.nr_small, c.d_cnt);
+  k_nr_init<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, idx, c.nr_segof, seg, c.nr_small, c.nr_med, c.d_cnt);
   c.count_launch();
-  fetch_counters(c, 10);
+  fetch_counters(c, kNrCounters);
   int nseg = c.h_cnt[C_NSEG];
   if (nseg > 0 && nr_levels_coop(c, n, arr, small_cap)) {
     if (c.h_cnt[C_OVERFLOW]) { c.err = "NR sort emulation: small-segment buffer overflow"; return false; }
@@ -808,20 +918,31 @@ static bool nr_indexx(Ctx& c, int n, const double* w) {
                                                           c.nr_ls, c.nr_rs, c.nr_lpos, c.nr_rpos, idx2);
       std::swap(idx, idx2);
       cudaMemsetAsync(c.d_cnt + out, 0, sizeof(int), c.stream);
-      k_nr_newsegs<<<gseg, kBlock, 0, c.stream>>>(in, out, seg, c.nr_segmeta, seg2, c.nr_small, c.d_cnt, small_cap);
+      k_nr_newsegs<<<gseg, kBlock, 0, c.stream>>>(in, out, seg, c.nr_segmeta, seg2, c.nr_small, c.nr_med, c.d_cnt,
+                                                  small_cap, nr_med_cap(c));
       k_nr_segof<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, seg, c.nr_segmeta, c.nr_segof);
       c.count_launch(7);
       std::swap(seg, seg2);
       std::swap(in, out);
     }
-    fetch_counters(c, 12);
+    fetch_counters(c, kNrCounters);
     nseg = c.h_cnt[in];
     if (c.h_cnt[C_OVERFLOW]) { c.err = "NR sort emulation: small-segment buffer overflow"; return false; }
+  }
+  const int nmed = c.h_cnt[C_NMED];
+  if (nmed > 0) {
+    const int blocks = std::min((nmed + kNrMedWarps - 1) / kNrMedWarps, 148 * 16);
+    k_nr_medium<<<blocks, 32 * kNrMedWarps, 0, c.stream>>>(nmed, c.nr_med, arr, idx, c.d_cnt);
+    c.count_launch();
   }
   const int nsmall = c.h_cnt[C_NSMALL];
   if (nsmall > 0) {
     k_nr_insertion<<<grid1d(nsmall), kBlock, 0, c.stream>>>(nsmall, c.nr_small, arr, idx);
     c.count_launch();
+  }
+  if (nmed > 0) {  // the medium kernel reports an impossible segment through the overflow flag
+    fetch_counters(c, kNrCounters);
+    if (c.h_cnt[C_OVERFLOW]) { c.err = "NR sort emulation: medium segment out of range"; return false; }
   }
   if (idx != c.nr_idx)
     cudaMemcpyAsync(c.nr_idx, idx, sizeof(int) * (n + 2), cudaMemcpyDeviceToDevice, c.stream);
