@@ -34,6 +34,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -70,10 +71,25 @@ def workload(size, seed=12345):
     return W.mfd(size, seed=seed)
 
 
+def clocks_path(name):
+    """Where a run's sampled clock log goes: $FSB_CLOCKS_DIR if set, else the
+    temporary directory (the JSON line carries the summary either way)."""
+    return os.path.join(os.environ.get("FSB_CLOCKS_DIR") or tempfile.gettempdir(), name)
+
+
+def l2_note(nodes):
+    """How the timed steps stand against the 126 MB L2: the instance's arena
+    is about 1.1 KB per node and every step sweeps all of it."""
+    ws = 1100.0 * nodes
+    if ws > 4 * 126e6:
+        return "working set %.1f GB >> 126 MB L2 (no flush needed)" % (ws / 1e9)
+    return "working set %.0f MB, not flushed between steps (small case; not a bench configuration)" % (ws / 1e6)
+
+
 def config(args, wl, ranks):
     return {"workload": f"mfd_{wl.nx}x{wl.ny}_bc{wl.bc}_p{wl.p}_n{wl.n}", "nx": wl.nx, "ny": wl.ny,
             "grids_per_gpu": 1, "parallelism": f"replicas{ranks}" if ranks > 1 else "single",
-            "l2": "working set >> 126 MB L2 (no flush needed)"}
+            "l2": l2_note(wl.nx * wl.ny)}
 
 
 # ---------------------------------------------------------------------------
@@ -258,8 +274,7 @@ def run_gpu(args):
 
     g.set_profile(True)
     g.stage_times(reset=True)
-    clocks = ClockSampler(local, os.path.join(ROOT, "gpurun_out", f"clocks_r{rank}.csv")) \
-        if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ClockSampler(local, f"/tmp/clocks_r{rank}.csv")
+    clocks = ClockSampler(local, clocks_path(f"clocks_r{rank}.csv"))
     launches0 = g.launch_count()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -372,8 +387,7 @@ def run_batched(args):
         b.run([w.job() for w in W.uneven_d8(args.workers, seed=999, nsteps=max(args.warmup, 1),
                                             lo=129, hi=257)])
         jobs = [w.job() for w in wls]
-        clocks = ClockSampler(0, os.path.join(ROOT, "gpurun_out", "clocks_batched.csv")
-                              if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp/clocks_batched.csv")
+        clocks = ClockSampler(0, clocks_path("clocks_batched.csv"))
         t0 = time.perf_counter()
         b.run(jobs)
         wall = time.perf_counter() - t0
@@ -448,8 +462,7 @@ def run_served(args):
         lat, thr = serve(b, probe, 0.0, np.random.default_rng(0))
         work = np.mean([r.nn * r.nsteps for r in probe])
         mu = thr / work  # requests per second the GPU completes when saturated
-        clocks = ClockSampler(0, os.path.join(ROOT, "gpurun_out", "clocks_served.csv")
-                              if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp/clocks_served.csv")
+        clocks = ClockSampler(0, clocks_path("clocks_served.csv"))
         for lv, frac in enumerate((0.2, 0.4, 0.6, 0.8, 0.95)):
             rate = frac * mu
             lat, thr = serve(b, requests(1000 + lv), rate, np.random.default_rng(lv))
