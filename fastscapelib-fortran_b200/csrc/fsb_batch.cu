@@ -45,6 +45,7 @@ struct Job {
   std::string msg;
   double t_submit = 0, t_start = 0, t_end = 0;
   bool done = false;
+  bool waited = false;  // a thread is waiting for it (one waiter per job)
 };
 
 }  // namespace
@@ -71,30 +72,37 @@ int run_job(Job& j, cudaStream_t stream, std::string& msg) {
   fsb_ctx* h = nullptr;
   void* arena = nullptr;
   int rc = fsb_create(&h);
-  auto step = [&](int r) {
-    if (rc == 0 && r != 0) { rc = r; msg = fsb_last_error(); }
-  };
   if (rc != 0) { msg = fsb_last_error(); return rc; }
-  step(fsb_set_nx_ny(h, s.nx, s.ny));
-  step(fsb_set_stream(h, stream));
+  // each call runs only while every earlier one has succeeded: after a
+  // failure (say the job's arena could not be had) nothing more is set up,
+  // allocated or run for this job
+  auto step = [&](auto&& call) {
+    if (rc != 0) return;
+    const int r = call();
+    if (r != 0) { rc = r; msg = fsb_last_error(); }
+  };
+  step([&] { return fsb_set_nx_ny(h, s.nx, s.ny); });
+  step([&] { return fsb_set_stream(h, stream); });
   size_t bytes = 0;
-  step(fsb_workspace_bytes(h, &bytes));
+  step([&] { return fsb_workspace_bytes(h, &bytes); });
   if (rc == 0) {
     const cudaError_t e = cudaMallocAsync(&arena, bytes, stream);
     if (e != cudaSuccess) { rc = 1; msg = std::string("device memory for the job: ") + cudaGetErrorString(e); arena = nullptr; }
   }
-  step(fsb_setup(h, arena, bytes));
-  step(fsb_set_xl_yl(h, s.xl, s.yl));
-  step(fsb_set_dt(h, s.dt));
-  step(fsb_init_h(h, s.h0, FSB_HOST));
-  step(fsb_set_erosional_parameters(h, s.kf, s.kfsed, s.m, s.n, s.kd, s.kdsed, s.g1, s.g2, s.p, FSB_HOST));
-  step(fsb_set_u(h, s.u, FSB_HOST));
-  if (s.precip) step(fsb_set_precip(h, s.precip, FSB_HOST));
-  step(fsb_set_bc(h, s.bc));
-  step(fsb_execute_steps(h, s.nsteps));
-  if (s.h_out) step(fsb_copy_field(h, FSB_H, s.h_out, FSB_HOST));
-  if (s.a_out) step(fsb_copy_field(h, FSB_DRAINAGE_AREA, s.a_out, FSB_HOST));
-  if (s.etot_out) step(fsb_copy_field(h, FSB_TOTAL_EROSION, s.etot_out, FSB_HOST));
+  step([&] { return fsb_setup(h, arena, bytes); });
+  step([&] { return fsb_set_xl_yl(h, s.xl, s.yl); });
+  step([&] { return fsb_set_dt(h, s.dt); });
+  step([&] { return fsb_init_h(h, s.h0, FSB_HOST); });
+  step([&] {
+    return fsb_set_erosional_parameters(h, s.kf, s.kfsed, s.m, s.n, s.kd, s.kdsed, s.g1, s.g2, s.p, FSB_HOST);
+  });
+  step([&] { return fsb_set_u(h, s.u, FSB_HOST); });
+  if (s.precip) step([&] { return fsb_set_precip(h, s.precip, FSB_HOST); });
+  step([&] { return fsb_set_bc(h, s.bc); });
+  step([&] { return fsb_execute_steps(h, s.nsteps); });
+  if (s.h_out) step([&] { return fsb_copy_field(h, FSB_H, s.h_out, FSB_HOST); });
+  if (s.a_out) step([&] { return fsb_copy_field(h, FSB_DRAINAGE_AREA, s.a_out, FSB_HOST); });
+  if (s.etot_out) step([&] { return fsb_copy_field(h, FSB_TOTAL_EROSION, s.etot_out, FSB_HOST); });
   fsb_destroy(h);  // the arena is caller-owned: freed here, after the handle
   if (arena) cudaFreeAsync(arena, stream);
   const cudaError_t e = cudaStreamSynchronize(stream);
@@ -211,6 +219,9 @@ int fsb_batch_wait(fsb_batch* b, long long id, int* status, double* times) {
   auto it = b->jobs.find(id);
   if (it == b->jobs.end()) return fsb::report_error("fsb_batch_wait: unknown job id " + std::to_string(id));
   Job* j = it->second.get();
+  if (j->waited)  // the first waiter erases the job when it returns
+    return fsb::report_error("fsb_batch_wait: job " + std::to_string(id) + " is already being waited for");
+  j->waited = true;
   b->cv_done.wait(lk, [&] { return j->done; });
   if (status) *status = j->status;
   if (times) { times[0] = j->t_submit; times[1] = j->t_start; times[2] = j->t_end; }

@@ -229,7 +229,8 @@ int fsb_batch_submit(fsb_batch* b, const fsb_job* job, long long* id);
 /* Blocks until job `id` has finished and forgets it; `status` receives 0 or
    the job's error code (whose message fsb_last_error then returns) and
    `times` (may be NULL) its submit, start and end times in seconds on one
-   monotonic clock. */
+   monotonic clock.  One thread waits per job: a second wait on the same id,
+   while the first is blocked, returns an error. */
 int fsb_batch_wait(fsb_batch* b, long long id, int* status, double* times);
 /* Submits `njobs` jobs and waits for all of them; status[k] and
    times[3k..3k+2] as fsb_batch_wait (either may be NULL). */
