@@ -9,6 +9,7 @@ Reference file:line for each routine is given in its docstring.
 from __future__ import annotations
 
 import math
+import struct
 import sys
 
 TINY = sys.float_info.min
@@ -359,3 +360,101 @@ def routing_sfd(h0, nx, ny, dx, dy, jbc):
     out.update(rec=rec[1:], length=length[1:], stack=stack[1:], ndon=ndon[1:],
                don=[don[k][1:ndon[k] + 1] for k in range(1, nn + 1)])
     return out
+
+
+def find_mult_rec(h, rec0, stack0, nx, ny, dx, dy, p, p_mfd_exp, bounds):
+    """find_mult_rec -- src/FlowRouting.f90:147-298.  ``h``, ``rec0``, ``stack0``
+    and ``p_mfd_exp`` are 1-based; returns (rec, nrec, wrec, lrec, stack,
+    water, p_mfd_exp), 1-based, with rec/wrec/lrec as lists of 8-slot lists."""
+    i1, i2, j1, j2, xc, yc = bounds
+    nn = nx * ny
+    h0 = list(h)
+    deltah = 1.0e-8
+    for i in range(1, nn + 1):  # :187-196
+        ijk = stack0[i]
+        ijr = rec0[ijk]
+        if ijr != 0:
+            if h0[ijr] > h0[ijk]:
+                h0[ijk] = h0[ijr] + deltah
+    water = list(h0)
+    nrec = [0] * (nn + 1)
+    rec = [[0] * 9 for _ in range(nn + 1)]
+    wrec = [[0.0] * 9 for _ in range(nn + 1)]
+    lrec = [[0.0] * 9 for _ in range(nn + 1)]
+    for j in range(j1, j2 + 1):  # :204-230
+        for i in range(i1, i2 + 1):
+            ij = (j - 1) * nx + i
+            for jj in (-1, 0, 1):
+                jjj = j + jj
+                if jjj < 1 and yc:
+                    jjj = jjj + ny
+                jjj = max(jjj, 1)
+                if jjj > ny and yc:
+                    jjj = jjj - ny
+                jjj = min(jjj, ny)
+                for ii in (-1, 0, 1):
+                    iii = i + ii
+                    if iii < 1 and xc:
+                        iii = iii + nx
+                    iii = max(iii, 1)
+                    if iii > nx and xc:
+                        iii = iii - nx
+                    iii = min(iii, nx)
+                    ijk = (jjj - 1) * nx + iii
+                    if h0[ij] > h0[ijk]:
+                        nrec[ij] += 1
+                        k = nrec[ij]
+                        rec[ij][k] = ijk
+                        lrec[ij][k] = math.sqrt((ii * dx) * (ii * dx) + (jj * dy) * (jj * dy))
+                        wrec[ij][k] = (h0[ij] - h0[ijk]) / lrec[ij][k]
+    pexp = list(p_mfd_exp)
+    f32 = lambda x: struct.unpack("f", struct.pack("f", x))[0]  # noqa: E731  Fortran real()
+    for ij in range(1, nn + 1):  # :232-243
+        if p < 0.0:
+            slope = 0.0
+            if nrec[ij] != 0:
+                s = 0.0
+                for k in range(1, nrec[ij] + 1):
+                    s = s + wrec[ij][k]
+                slope = f32(s / nrec[ij])
+            pexp[ij] = f32(0.5) + f32(0.6) * slope
+        for k in range(1, nrec[ij] + 1):
+            wrec[ij][k] = wrec[ij][k] ** pexp[ij]
+        sumweight = 0.0
+        for k in range(1, nrec[ij] + 1):
+            sumweight = sumweight + wrec[ij][k]
+        for k in range(1, nrec[ij] + 1):
+            wrec[ij][k] = wrec[ij][k] / sumweight
+    ndon = [0] * (nn + 1)  # :247-255
+    for ij in range(1, nn + 1):
+        for k in range(1, nrec[ij] + 1):
+            ndon[rec[ij][k]] += 1
+    stack = [0] * (nn + 1)  # :259-292, LIFO parse stack
+    vis = [0] * (nn + 1)
+    parse = []
+    nstack = 0
+    for ij in range(1, nn + 1):
+        if ndon[ij] == 0:
+            parse.append(ij)
+        while parse:
+            ijn = parse.pop()
+            nstack += 1
+            stack[nstack] = ijn
+            for k in range(1, nrec[ijn] + 1):
+                ijr = rec[ijn][k]
+                vis[ijr] += 1
+                if vis[ijr] == ndon[ijr]:
+                    parse.append(ijr)
+    if nstack != nn:
+        raise RuntimeError("error in stack")
+    return rec, nrec, wrec, lrec, stack, water, pexp
+
+
+def flow_accumulation_mfd(mstack, mrec, mnrec, mwrec, precip, nn, dx, dy):
+    """FlowAccumulation -- src/FlowRouting.f90:97-119 (1-based)."""
+    a = [0.0] + [dx * dy * precip[ij] for ij in range(1, nn + 1)]
+    for ij in range(1, nn + 1):
+        ijk = mstack[ij]
+        for k in range(1, mnrec[ijk] + 1):
+            a[mrec[ijk][k]] = a[mrec[ijk][k]] + a[ijk] * mwrec[ijk][k]
+    return a

@@ -345,6 +345,39 @@ def _literal_spl(sfd, h, b, ht_bc, rec, stack, mstack, a, length, mrec, mnrec, m
     return h, ngs
 
 
+@pytest.mark.parametrize("bc,p,seed", [(1010, 1.1, 71), (1111, 1.0, 72), (101, -1.0, 73), (1000, 0.0, 74)])
+def test_mfd_routing_matches_literal(bc, p, seed):
+    """The oracle's multiple-flow routing (find_mult_rec: fill, receivers with
+    their clamp duplicates, weights and the p < 0 single-precision exponent,
+    lengths, the LIFO mstack) and its drainage area against a literal
+    transliteration, bit for bit.  With no uplift the routing sees init_h's h;
+    rec and stack are the oracle's single-flow result after LocalMinima, which
+    test_routing_matches_literal pins separately."""
+    wl = W.mfd(23, 19, seed=seed, nsteps=1, p=p, bc=bc)
+    wl.u = np.zeros(wl.nn)
+    wl.apply(O)
+    O.fastscape_execute_step()
+    nx, ny, nn = wl.nx, wl.ny, wl.nn
+    dx, dy = wl.xl / (nx - 1), wl.yl / (ny - 1)
+    _, bounds = FL.set_bc(nx, ny, wl.bc)
+    rec0 = [0] + [r + 1 for r in O.copy_int("rec").tolist()]
+    stack0 = [0] + [s + 1 for s in O.copy_int("stack").tolist()]
+    rec, nrec, wrec, lrec, mstack, water, _ = FL.find_mult_rec(
+        [0.0] + wl.h0.tolist(), rec0, stack0, nx, ny, dx, dy, p, [0.0] + [p] * nn, bounds)
+    assert nrec[1:] == O.copy_int("mnrec").tolist()
+    assert sum(nrec) > nn  # many nodes have several receivers
+    mrec, mw, ml = O.copy_slots("mrec"), O.copy_slots("mwrec"), O.copy_slots("mlrec")
+    for ij in range(1, nn + 1):
+        k = nrec[ij]
+        assert [r - 1 for r in rec[ij][1:k + 1]] == mrec[ij - 1, :k].tolist()
+        assert wrec[ij][1:k + 1] == mw[ij - 1, :k].tolist()
+        assert lrec[ij][1:k + 1] == ml[ij - 1, :k].tolist()
+    assert [s - 1 for s in mstack[1:]] == O.copy_int("mstack").tolist()
+    assert water[1:] == O.copy_double("hwater").tolist()
+    a = FL.flow_accumulation_mfd(mstack, rec, nrec, wrec, [0.0] + [1.0] * nn, nn, dx, dy)
+    assert a[1:] == O.copy_double("drainage_area").tolist()
+
+
 @pytest.mark.parametrize("sfd,n", [(True, 1.0), (True, 1.5), (False, 1.0), (False, 1.5)])
 def test_sediment_spl_matches_literal(sfd, n):
     """The oracle's g > 0 stream power law against a literal transliteration:
