@@ -404,6 +404,37 @@ def test_sediment_spl_matches_literal(sfd, n):
     assert np.max(np.abs(O.copy_double("h") - h_lit)) <= 1e-12 * (np.abs(h_lit).max() + 1.0)
 
 
+@pytest.mark.parametrize("sfd,n", [(False, 1.5), (False, 1.0), (True, 1.5), (True, 1.0)])
+def test_spl_g0_matches_literal(sfd, n):
+    """The oracle's stream power law as the benchmark runs it (g = 0: one
+    Gauss-Seidel pass; multiple flow with Newton at n = 1.5 first) against the
+    literal transliteration; no uplift and no diffusion, so a step's change of
+    h is the SPL alone."""
+    wl = W.plain_d8(19, 17, seed=53) if sfd else W.mfd(19, 17, seed=54, p=1.1, bc=1010)
+    wl.n, wl.g1, wl.g2 = n, 0.0, 0.0
+    wl.kf = np.full(wl.nn, (1e-4 if n == 1.0 else 2e-3) if sfd else 2e-5)
+    wl.u = np.zeros(wl.nn)
+    wl.kd = np.zeros(wl.nn)
+    wl.apply(O)
+    for _ in range(2):
+        O.fastscape_execute_step()
+    h0, b0 = O.copy_double("h"), O.copy_double("basement")
+    O.fastscape_execute_step()
+    _, (i1, i2, j1, j2, xc, yc) = FL.set_bc(wl.nx, wl.ny, wl.bc)
+    ii, jj = np.meshgrid(np.arange(1, wl.nx + 1), np.arange(1, wl.ny + 1))
+    fixed = ((ii < i1) | (ii > i2) | (jj < j1) | (jj > j2)).ravel()
+    dx, dy = wl.xl / (wl.nx - 1), wl.yl / (wl.ny - 1)
+    h_lit, ngs = _literal_spl(sfd, h0, b0, fixed, O.copy_int("rec"), O.copy_int("stack"),
+                              O.copy_int("mstack"), O.copy_double("drainage_area"),
+                              O.copy_double("length"), O.copy_slots("mrec"), O.copy_int("mnrec"),
+                              O.copy_slots("mwrec"), O.copy_slots("mlrec"), wl.kf, wl.kfsed, wl.m, n,
+                              wl.g1, wl.g2, wl.dt, dx, dy)
+    assert ngs == 1
+    dh = np.abs(O.copy_double("h") - h0)
+    assert dh.max() > 0.0  # the step eroded something
+    assert np.max(np.abs(O.copy_double("h") - h_lit)) <= 1e-12 * (np.abs(h_lit).max() + 1.0)
+
+
 def _tridag(a, b, c, r):
     """tridag (Diffusion.f90:164-202), 0-based."""
     n = len(b)
