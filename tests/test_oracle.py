@@ -450,6 +450,103 @@ def _tridag(a, b, c, r):
     return u
 
 
+def _literal_diffusion(h, b, kd, kdsed, nx, ny, dx, dy, dt, jbc):
+    """Diffusion (Diffusion.f90:1-160), statement for statement on 1-based
+    (i, j) arrays; returns h, b, and the etot and erate increments.  The
+    bottom-boundary branch reads kdint(i, j) with j = ny, the value the
+    preceding loop leaves (Diffusion.f90:114)."""
+    cbc = "****" if (jbc > 9999 or jbc < -999) else "%4d" % jbc
+    z = np.zeros((nx + 2, ny + 2))
+    kdi = np.zeros((nx + 2, ny + 2))
+    for j in range(1, ny + 1):
+        for i in range(1, nx + 1):
+            ij = (j - 1) * nx + i - 1
+            z[i, j] = h[ij]
+            kdi[i, j] = kd[ij]
+            if kdsed > 0.0 and (h[ij] - b[ij]) > 1.0e-6:
+                kdi[i, j] = kdsed
+    zp = z.copy()
+    hdt = dt / 2.0
+    fx = lambda a, c: (a + c) / 2.0 * hdt / (dx * dx)  # noqa: E731
+    fy = lambda a, c: (a + c) / 2.0 * hdt / (dy * dy)  # noqa: E731
+    for j in range(2, ny):
+        diag, sup, inf, f = np.zeros(nx + 1), np.zeros(nx + 1), np.zeros(nx + 1), np.zeros(nx + 1)
+        for i in range(2, nx):
+            fxp, fxm = fx(kdi[i + 1, j], kdi[i, j]), fx(kdi[i - 1, j], kdi[i, j])
+            fyp, fym = fy(kdi[i, j + 1], kdi[i, j]), fy(kdi[i, j - 1], kdi[i, j])
+            diag[i] = 1.0 + fxp + fxm
+            sup[i] = -fxp
+            inf[i] = -fxm
+            f[i] = zp[i, j] + fyp * zp[i, j + 1] - (fyp + fym) * zp[i, j] + fym * zp[i, j - 1]
+        if cbc[3] == "1":
+            diag[1], sup[1], f[1] = 1.0, 0.0, zp[1, j]
+        else:
+            fxp, fyp, fym = fx(kdi[2, j], kdi[1, j]), fy(kdi[1, j + 1], kdi[1, j]), fy(kdi[1, j - 1], kdi[1, j])
+            diag[1], sup[1] = 1.0 + fxp, -fxp
+            f[1] = zp[1, j] + fyp * zp[1, j + 1] - (fyp + fym) * zp[1, j] + fym * zp[1, j - 1]
+        if cbc[1] == "1":
+            diag[nx], inf[nx], f[nx] = 1.0, 0.0, zp[nx, j]
+        else:
+            fxm = fx(kdi[nx - 1, j], kdi[nx, j])
+            fyp, fym = fy(kdi[nx, j + 1], kdi[nx, j]), fy(kdi[nx, j - 1], kdi[nx, j])
+            diag[nx], inf[nx] = 1.0 + fxm, -fxm
+            f[nx] = zp[nx, j] + fyp * zp[nx, j + 1] - (fyp + fym) * zp[nx, j] + fym * zp[nx, j - 1]
+        z[1:nx + 1, j] = _tridag(inf[1:], diag[1:], sup[1:], f[1:])
+    for i in range(2, nx):
+        diag, sup, inf, f = np.zeros(ny + 1), np.zeros(ny + 1), np.zeros(ny + 1), np.zeros(ny + 1)
+        for j in range(2, ny):
+            fxp, fxm = fx(kdi[i + 1, j], kdi[i, j]), fx(kdi[i - 1, j], kdi[i, j])
+            fyp, fym = fy(kdi[i, j + 1], kdi[i, j]), fy(kdi[i, j - 1], kdi[i, j])
+            diag[j] = 1.0 + fyp + fym
+            sup[j] = -fyp
+            inf[j] = -fym
+            f[j] = z[i, j] + fxp * z[i + 1, j] - (fxp + fxm) * z[i, j] + fxm * z[i - 1, j]
+        jq = ny  # the loop variable after `do j=2,ny-1`
+        if cbc[0] == "1":
+            diag[1], sup[1], f[1] = 1.0, 0.0, z[i, 1]
+        else:
+            fxp, fxm = fx(kdi[i + 1, 1], kdi[i, jq]), fx(kdi[i - 1, 1], kdi[i, 1])
+            fyp = fy(kdi[i, 2], kdi[i, 1])
+            diag[1], sup[1] = 1.0 + fyp, -fyp
+            f[1] = z[i, 1] + fxp * z[i + 1, 1] - (fxp + fxm) * z[i, 1] + fxm * z[i - 1, 1]
+        if cbc[2] == "1":
+            diag[ny], inf[ny], f[ny] = 1.0, 0.0, z[i, ny]
+        else:
+            fxp, fxm = fx(kdi[i + 1, ny], kdi[i, ny]), fx(kdi[i - 1, ny], kdi[i, ny])
+            fym = fy(kdi[i, ny - 1], kdi[i, ny])
+            diag[ny], inf[ny] = 1.0 + fym, -fym
+            f[ny] = z[i, ny] + fxp * z[i + 1, ny] - (fxp + fxm) * z[i, ny] + fxm * z[i - 1, ny]
+        zp[i, 1:ny + 1] = _tridag(inf[1:], diag[1:], sup[1:], f[1:])
+    hn = zp[1:nx + 1, 1:ny + 1].T.ravel().copy()
+    return hn, np.minimum(hn, b), h - hn, (h - hn) / dt
+
+
+@pytest.mark.parametrize("bc,kdsed,seed", [(1111, -1.0, 81), (1010, 0.05, 82), (101, -1.0, 83), (1000, 0.05, 84)])
+def test_diffusion_matches_literal(bc, kdsed, seed):
+    """The oracle's ADI diffusion against a literal transliteration, bit for
+    bit: no uplift and kf = 0 (the stream power law then leaves h as it is),
+    so a step's change of h, b, etot and erate is the diffusion alone; a
+    spatially varying kd, and kdsed on nodes with sediment above the basement."""
+    wl = W.plain_d8(17, 13, seed=seed)
+    rng = np.random.default_rng(seed)
+    wl.bc = bc
+    wl.kdsed = kdsed
+    wl.kf = np.zeros(wl.nn)
+    wl.u = np.zeros(wl.nn)
+    wl.kd = 1.0e2 * (0.5 + rng.random(wl.nn))
+    wl.apply(O)
+    b = wl.h0 - np.where(rng.random(wl.nn) < 0.5, 2.0, 0.0)
+    O.fastscape_set_basement(b)
+    O.fastscape_execute_step()
+    dx, dy = wl.xl / (wl.nx - 1), wl.yl / (wl.ny - 1)
+    h, bl, de, dr = _literal_diffusion(wl.h0, b, wl.kd, kdsed, wl.nx, wl.ny, dx, dy, wl.dt, bc)
+    assert np.max(np.abs(h - wl.h0)) > 1e-3  # the step diffused something
+    np.testing.assert_array_equal(O.copy_double("h"), h)
+    np.testing.assert_array_equal(O.copy_double("basement"), bl)
+    np.testing.assert_array_equal(O.copy_double("total_erosion"), de)
+    np.testing.assert_array_equal(O.copy_double("erosion_rate"), dr)
+
+
 def _literal_advect(h, b, etot, vx, vy, nx, ny, dx, dy, dt):
     """Advect (Advect.f90:1-103) on (ny, nx) arrays."""
     h, b, etot = h.reshape(ny, nx).copy(), b.reshape(ny, nx).copy(), etot.reshape(ny, nx).copy()
