@@ -358,7 +358,7 @@ def routing_sfd(h0, nx, ny, dx, dy, jbc):
     ndon, don = find_donor(rec, nn)
     stack = find_stack(rec, don, ndon, nn)
     out.update(rec=rec[1:], length=length[1:], stack=stack[1:], ndon=ndon[1:],
-               don=[don[k][1:ndon[k] + 1] for k in range(1, nn + 1)])
+               don=[don[k][1:ndon[k] + 1] for k in range(1, nn + 1)], rec_1b=rec, stack_1b=stack)
     return out
 
 
@@ -457,4 +457,26 @@ def flow_accumulation_mfd(mstack, mrec, mnrec, mwrec, precip, nn, dx, dy):
         ijk = mstack[ij]
         for k in range(1, mnrec[ijk] + 1):
             a[mrec[ijk][k]] = a[mrec[ijk][k]] + a[ijk] * mwrec[ijk][k]
+    return a
+
+
+def lake_fill_sfd(h, rec, stack, nn):
+    """hwater of FlowRoutingSingleFlowDirection -- src/FlowRouting.f90:73-89 (1-based)."""
+    hwater = list(h)
+    deltah = 1.0e-8
+    for i in range(1, nn + 1):
+        ijk = stack[i]
+        ijr = rec[ijk]
+        if ijr != 0:
+            if hwater[ijr] > hwater[ijk]:
+                hwater[ijk] = hwater[ijr] + deltah
+    return hwater
+
+
+def flow_accumulation_sfd(stack, rec, precip, nn, dx, dy):
+    """FlowAccumulationSingleFlowDirection -- src/FlowRouting.f90:123-143 (1-based)."""
+    a = [0.0] + [dx * dy * precip[ij] for ij in range(1, nn + 1)]
+    for ij in range(nn, 0, -1):
+        ijk = stack[ij]
+        a[rec[ijk]] = a[rec[ijk]] + a[ijk]
     return a

@@ -84,6 +84,14 @@ def test_routing_matches_literal(nx, ny, bc, seed):
     assert np.array_equal(O.copy_int("stack"), np.asarray(lit["stack"]) - 1)
     assert np.array_equal(O.copy_double("length"), np.asarray(lit["length"]))
     assert d["nlocmin_after"] == 0
+    # the lake fill and the drainage area on the re-routed forest
+    nn = nx * ny
+    h1 = [0.0] + list(h_up)
+    hw = FL.lake_fill_sfd(h1, lit["rec_1b"], lit["stack_1b"], nn)
+    assert O.copy_double("hwater").tolist() == hw[1:]
+    assert O.copy_double("lake_depth").tolist() == [hw[k] - h1[k] for k in range(1, nn + 1)]
+    a = FL.flow_accumulation_sfd(lit["stack_1b"], lit["rec_1b"], [0.0] + [1.0] * nn, nn, dx, dy)
+    assert O.copy_double("drainage_area").tolist() == a[1:]
 
 
 # --------------------------------------------------------------------------
