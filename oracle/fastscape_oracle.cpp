@@ -1,6 +1,6 @@
 // Oracle: a single-threaded CPU restatement of fastscapelib-fortran's continental
-// time step (FastScape_Execute_Step with marine, stratigraphy, flexure and
-// advection switched off).
+// time step (FastScape_Execute_Step with marine, stratigraphy and flexure
+// switched off; advection runs when velocities are set).
 //
 // TEST INFRASTRUCTURE ONLY.  This file is the checker that tests/, the smoke
 // test and the benchmark's cpu_baseline leg compare the CUDA library against.
@@ -9,8 +9,10 @@
 // The reference cannot be compiled in this environment (it is Fortran and no
 // Fortran compiler is installed), so parity with the reference itself is
 // UNPINNED: this restatement follows the Fortran statement by statement and
-// cites, for every routine, the reference file:line it restates.  Fortran
-// semantics that matter for bit-exactness are kept:
+// cites, for every routine, the reference file:line it restates, and the
+// tests check every stage of it against a second, independent literal
+// transliteration in Python (tests/fortran_literal.py, tests/test_oracle.py).
+// Fortran semantics that matter for bit-exactness are kept:
 //   * 1-based node numbering ij = i + (j-1)*nx internally; the C-ABI exports
 //     0-based node ids (value - 1).
 //   * no fused multiply-add (build with -ffp-contract=off), left-to-right
