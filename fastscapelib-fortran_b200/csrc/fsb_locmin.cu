@@ -44,6 +44,13 @@ constexpr int kNrCounters = 15;  // counters the NR sort reads back
 // cost a round of grid-wide barriers.
 constexpr int kNrMedium = 512;
 
+// Level bound of the emulation: every level shrinks every segment by at least
+// its pivot, so n + 8 levels always suffice.  A fixed bound would not do: the
+// reference's median of three (LocalMinima.f90:985-1006) degenerates on
+// descending keys, to a quicksort tree about n/6 levels deep, which the
+// reference runs sequentially (slowly) and this emulation level by level.
+inline int nr_max_levels(int n) { return n + 8; }
+
 __constant__ int c_ii[8] = {-1, 1, 0, 0, -1, 1, -1, 1};
 __constant__ int c_jj[8] = {0, 0, -1, 1, -1, -1, 1, 1};
 
@@ -443,6 +450,7 @@ struct NrCoop {
   int *idx, *idx2, *seg, *seg2, *segof, *lf, *rf, *ls, *rs, *lpos, *rpos, *meta, *small, *med, *cnt, *bsum;
   double* piv;
   int small_cap, med_cap;
+  int max_levels;
 };
 
 constexpr int kCoopThreads = 256;
@@ -479,7 +487,7 @@ __global__ void __launch_bounds__(kCoopThreads) k_nr_levels(NrCoop A) {
   int *idx = A.idx, *idx2 = A.idx2, *seg = A.seg, *seg2 = A.seg2;
   int in = C_NSEG, out = C_NSEG2;
   int level = 0;
-  for (; level < 200; ++level) {
+  for (; level < A.max_levels; ++level) {
     const int nseg = __ldcg(&A.cnt[in]);
     if (nseg == 0) break;
     if (tid == 0) A.cnt[out] = 0;
@@ -868,7 +876,8 @@ static bool nr_levels_coop(Ctx& c, int n, const double* arr, int small_cap) {
   const int blocks = std::max(1, std::min(want, std::min(sms * per_sm, c.nr_bsum_cap / 2)));
   NrCoop A{n,         arr,       c.nr_idx,  c.nr_idx2, c.nr_seg,     c.nr_seg2,  c.nr_segof,
            c.nr_lf,   c.nr_rf,   c.nr_ls,   c.nr_rs,   c.nr_lpos,    c.nr_rpos,  c.nr_segmeta,
-           c.nr_small, c.nr_med, c.d_cnt,   c.nr_bsum, c.nr_piv,     small_cap,  nr_med_cap(c)};
+           c.nr_small, c.nr_med, c.d_cnt,   c.nr_bsum, c.nr_piv,     small_cap,  nr_med_cap(c),
+           nr_max_levels(n)};
   void* args[] = {&A};
   if (cudaLaunchCooperativeKernel((const void*)k_nr_levels, dim3(blocks), dim3(kCoopThreads), args, 0, c.stream) !=
       cudaSuccess) {
@@ -893,7 +902,7 @@ static bool nr_indexx(Ctx& c, int n, const double* w) {
   int nseg = c.h_cnt[C_NSEG];
   if (nseg > 0 && nr_levels_coop(c, n, arr, small_cap)) {
     if (c.h_cnt[C_OVERFLOW]) { c.err = "NR sort emulation: small-segment buffer overflow"; return false; }
-    if (c.h_cnt[C_NRLEVELS] >= 200) { c.err = "NR sort emulation: too many levels"; return false; }
+    if (c.h_cnt[C_NRLEVELS] >= nr_max_levels(n)) { c.err = "NR sort emulation: too many levels"; return false; }
     if (c.h_cnt[C_NRIDX]) std::swap(idx, idx2);
     nseg = 0;  // all levels done
   }
@@ -905,7 +914,7 @@ static bool nr_indexx(Ctx& c, int n, const double* w) {
   int levels = 0;
   while (nseg > 0) {
     for (int b = 0; b < 4; ++b) {
-      if (++levels > 200) { c.err = "NR sort emulation: too many levels"; return false; }
+      if (++levels > nr_max_levels(n)) { c.err = "NR sort emulation: too many levels"; return false; }
       const int* nsegp = c.d_cnt + in;
       k_nr_median<<<gseg, kBlock, 0, c.stream>>>(nsegp, seg, arr, idx, c.nr_piv, c.nr_segmeta);
       k_nr_flags<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, c.nr_segof, seg, c.nr_piv, arr, idx, c.nr_lf, c.nr_rf);
