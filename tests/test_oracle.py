@@ -52,7 +52,9 @@ def test_indexx_distinct_is_argsort():
 # single-flow routing + LocalMinima against the literal transliteration
 
 CASES = [(21, 17, 1111, 1), (23, 19, 1010, 2), (19, 25, 101, 3), (17, 15, 1000, 4),
-         (16, 16, 11, 5), (31, 29, 1111, 6)]
+         (16, 16, 11, 5), (31, 29, 1111, 6),
+         # the smallest grids: one interior node, one interior row, one interior column
+         (3, 3, 1111, 7), (3, 4, 1010, 8), (5, 3, 101, 9), (4, 3, 1000, 10)]
 
 
 @pytest.mark.parametrize("nx,ny,bc,seed", CASES)
@@ -353,19 +355,21 @@ def _literal_spl(sfd, h, b, ht_bc, rec, stack, mstack, a, length, mrec, mnrec, m
     return h, ngs
 
 
-@pytest.mark.parametrize("bc,p,seed", [(1010, 1.1, 71), (1111, 1.0, 72), (101, -1.0, 73), (1000, 0.0, 74)])
-def test_mfd_routing_matches_literal(bc, p, seed):
+@pytest.mark.parametrize("nx,ny,bc,p,seed", [(23, 19, 1010, 1.1, 71), (23, 19, 1111, 1.0, 72),
+                                             (23, 19, 101, -1.0, 73), (23, 19, 1000, 0.0, 74),
+                                             (3, 4, 1000, 1.1, 75), (4, 3, 101, -1.0, 76)])
+def test_mfd_routing_matches_literal(nx, ny, bc, p, seed):
     """The oracle's multiple-flow routing (find_mult_rec: fill, receivers with
     their clamp duplicates, weights and the p < 0 single-precision exponent,
     lengths, the LIFO mstack) and its drainage area against a literal
     transliteration, bit for bit.  With no uplift the routing sees init_h's h;
     rec and stack are the oracle's single-flow result after LocalMinima, which
     test_routing_matches_literal pins separately."""
-    wl = W.mfd(23, 19, seed=seed, nsteps=1, p=p, bc=bc)
+    wl = W.mfd(nx, ny, seed=seed, nsteps=1, p=p, bc=bc)
     wl.u = np.zeros(wl.nn)
     wl.apply(O)
     O.fastscape_execute_step()
-    nx, ny, nn = wl.nx, wl.ny, wl.nn
+    nn = wl.nn
     dx, dy = wl.xl / (nx - 1), wl.yl / (ny - 1)
     _, bounds = FL.set_bc(nx, ny, wl.bc)
     rec0 = [0] + [r + 1 for r in O.copy_int("rec").tolist()]
@@ -373,7 +377,7 @@ def test_mfd_routing_matches_literal(bc, p, seed):
     rec, nrec, wrec, lrec, mstack, water, _ = FL.find_mult_rec(
         [0.0] + wl.h0.tolist(), rec0, stack0, nx, ny, dx, dy, p, [0.0] + [p] * nn, bounds)
     assert nrec[1:] == O.copy_int("mnrec").tolist()
-    assert sum(nrec) > nn  # many nodes have several receivers
+    assert nn < 20 or sum(nrec) > nn  # on the larger grids many nodes have several receivers
     mrec, mw, ml = O.copy_slots("mrec"), O.copy_slots("mwrec"), O.copy_slots("mlrec")
     for ij in range(1, nn + 1):
         k = nrec[ij]
@@ -529,13 +533,15 @@ def _literal_diffusion(h, b, kd, kdsed, nx, ny, dx, dy, dt, jbc):
     return hn, np.minimum(hn, b), h - hn, (h - hn) / dt
 
 
-@pytest.mark.parametrize("bc,kdsed,seed", [(1111, -1.0, 81), (1010, 0.05, 82), (101, -1.0, 83), (1000, 0.05, 84)])
-def test_diffusion_matches_literal(bc, kdsed, seed):
+@pytest.mark.parametrize("nx,ny,bc,kdsed,seed", [(17, 13, 1111, -1.0, 81), (17, 13, 1010, 0.05, 82),
+                                                 (17, 13, 101, -1.0, 83), (17, 13, 1000, 0.05, 84),
+                                                 (3, 3, 101, -1.0, 85), (4, 5, 1000, 0.05, 86)])
+def test_diffusion_matches_literal(nx, ny, bc, kdsed, seed):
     """The oracle's ADI diffusion against a literal transliteration, bit for
     bit: no uplift and kf = 0 (the stream power law then leaves h as it is),
     so a step's change of h, b, etot and erate is the diffusion alone; a
     spatially varying kd, and kdsed on nodes with sediment above the basement."""
-    wl = W.plain_d8(17, 13, seed=seed)
+    wl = W.plain_d8(nx, ny, seed=seed)
     rng = np.random.default_rng(seed)
     wl.bc = bc
     wl.kdsed = kdsed
@@ -548,7 +554,7 @@ def test_diffusion_matches_literal(bc, kdsed, seed):
     O.fastscape_execute_step()
     dx, dy = wl.xl / (wl.nx - 1), wl.yl / (wl.ny - 1)
     h, bl, de, dr = _literal_diffusion(wl.h0, b, wl.kd, kdsed, wl.nx, wl.ny, dx, dy, wl.dt, bc)
-    assert np.max(np.abs(h - wl.h0)) > 1e-3  # the step diffused something
+    assert nx * ny < 12 or np.max(np.abs(h - wl.h0)) > 0.0  # the step diffused something
     np.testing.assert_array_equal(O.copy_double("h"), h)
     np.testing.assert_array_equal(O.copy_double("basement"), bl)
     np.testing.assert_array_equal(O.copy_double("total_erosion"), de)
