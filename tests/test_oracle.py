@@ -390,16 +390,23 @@ def test_mfd_routing_matches_literal(nx, ny, bc, p, seed):
     assert a[1:] == O.copy_double("drainage_area").tolist()
 
 
-@pytest.mark.parametrize("sfd,n", [(True, 1.0), (True, 1.5), (False, 1.0), (False, 1.5)])
-def test_sediment_spl_matches_literal(sfd, n):
+@pytest.mark.parametrize("sfd,n,kfsed,g2", [(True, 1.0, -1.0, 0.0), (True, 1.5, -1.0, 0.0),
+                                             (False, 1.0, -1.0, 0.0), (False, 1.5, -1.0, 0.0),
+                                             (True, 1.0, 3e-4, 0.6), (False, 1.5, 5e-5, 0.6)])
+def test_sediment_spl_matches_literal(sfd, n, kfsed, g2):
     """The oracle's g > 0 stream power law against a literal transliteration:
-    with no uplift and no diffusion a step's change of h is the SPL alone."""
+    with no uplift and no diffusion a step's change of h is the SPL alone.
+    With kfsed and g2 set, nodes with more than 1 m of sediment above the
+    basement take them instead of kf and g1 (StreamPowerLaw.f90:236-243)."""
     wl = W.plain_d8(19, 17, seed=51) if sfd else W.mfd(19, 17, seed=52, p=1.1, bc=1111)
-    wl.n, wl.g1, wl.g2 = n, 1.2, 0.0
+    wl.n, wl.g1, wl.g2, wl.kfsed = n, 1.2, g2, kfsed
     wl.kf = np.full(wl.nn, (1e-4 if n == 1.0 else 2e-3) if sfd else 2e-5)
     wl.u = np.zeros(wl.nn)
     wl.kd = np.zeros(wl.nn)
     wl.apply(O)
+    if kfsed > 0.0:  # sediment thicker than 1 m on half of the nodes
+        rng = np.random.default_rng(57)
+        O.fastscape_set_basement(wl.h0 - np.where(rng.random(wl.nn) < 0.5, 3.0, 0.0))
     for _ in range(2):
         O.fastscape_execute_step()
     h0, b0 = O.copy_double("h"), O.copy_double("basement")
