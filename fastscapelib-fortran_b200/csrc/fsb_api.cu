@@ -223,6 +223,9 @@ int check_device_error(fsb::Ctx& c) {
       case fsb::DEV_TRIDAG_ZERO: return fail("tridag failed");
       case fsb::DEV_OVERFLOW: return fail("device: buffer overflow");
       case fsb::DEV_NOT_ADJACENT: return fail("device: a receiver is not a neighbour of its donor");
+      case fsb::DEV_NEWTON_LIMIT:
+        return fail("stream power law: a Newton solve did not converge within " +
+                    std::to_string(fsb::kNewtonLimit) + " iterations");
       default: return fail("device error " + std::to_string(e));
     }
   }

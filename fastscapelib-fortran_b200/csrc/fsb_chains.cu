@@ -545,7 +545,11 @@ __global__ void __launch_bounds__(128) k_spl_chains(ChainView cv, const int* __r
               const double tolp = 1.0e-3;
               double errp = 2.0 * tolp;
               int guard = 0;
-              while (errp > tolp && guard++ < 10000) {
+              while (errp > tolp) {
+                if (++guard > kNewtonLimit) {
+                  atomicExch(err, DEV_NEWTON_LIMIT);
+                  break;
+                }
                 double f = hk - elev, df = 1.0;
                 if (ht[i] > htr) {
                   const double x = fmax(0.0, hk - hr);

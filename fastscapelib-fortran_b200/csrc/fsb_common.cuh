@@ -44,7 +44,13 @@ enum DeviceError : int {
   DEV_TRIDAG_ZERO = 3,      // zero pivot in the tridiagonal solve
   DEV_OVERFLOW = 4,         // a data-dependent buffer bound was exceeded
   DEV_NOT_ADJACENT = 5,     // a receiver is not one of the node's 3x3 neighbours
+  DEV_NEWTON_LIMIT = 6,     // a Newton solve of the stream power law did not converge
 };
+
+// Newton iterations a node may take before the stream power law reports
+// DEV_NEWTON_LIMIT (the reference iterates until |h_new - h| <= 1e-3,
+// StreamPowerLaw.f90:146-162 and :343-358; about 1.5 iterations are typical)
+constexpr int kNewtonLimit = 10000;
 
 constexpr int kSpinLimit = 1 << 21;  // polls (~1 s) before a bounded wait gives up
 

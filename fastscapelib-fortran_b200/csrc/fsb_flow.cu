@@ -512,7 +512,11 @@ struct SplMfdOp {
             const double tolp = 1.0e-3;
             double errp = 2.0 * tolp;
             int guard = 0;
-            while (errp > tolp && guard++ < 10000) {
+            while (errp > tolp) {
+              if (++guard > kNewtonLimit) {
+                atomicExch(err, DEV_NEWTON_LIMIT);
+                break;
+              }
               double f = hk - elev, df = 1.0;
 #pragma unroll
               for (int t = 0; t < 8; ++t)

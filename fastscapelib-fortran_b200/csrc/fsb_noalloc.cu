@@ -1,8 +1,8 @@
 // One ADI hillslope-diffusion step for callers that cannot allocate device
 // memory.
 //
-// Some callers cannot call cudaMalloc: code that runs inside a host callback
-// or a real-time loop, code embedded in a framework that owns every device
+// Some callers cannot call cudaMalloc: a real-time loop that must not stall
+// on the allocator, code embedded in a framework that owns every device
 // allocation through its own pool, or a host program that must not change
 // the device's memory footprint after start-up.  fsb_diffusion_step_noalloc
 // gives them the library's ADI diffusion step (the same kernels as the step
@@ -16,7 +16,6 @@
 #include <cuda_runtime.h>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "fsb_kernels.cuh"
@@ -28,10 +27,6 @@ constexpr int kNoAllocMaxNodes = 1 << 16;  // nx*ny limit (e.g. 256 x 256)
 constexpr int kScratchDoubles = 7 * kNoAllocMaxNodes + 32;  // 7 arrays + the error word
 
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-double* g_scratch_dev[kMaxDevices] = {};  // device address of g_noalloc_scratch per device
 
 int noalloc_fail(const std::string& m) { return fsb::report_error(m); }
 
@@ -47,24 +42,22 @@ int fsb_diffusion_step_noalloc(int nx, int ny, double xl, double yl, double dt, 
     return noalloc_fail("fsb_diffusion_step_noalloc: nx*ny = " + std::to_string((long long)nx * ny) +
                         " exceeds the static scratch limit of " + std::to_string(kNoAllocMaxNodes) + " nodes");
   if (!kd || !h || !b || !etot || !erate) return noalloc_fail("fsb_diffusion_step_noalloc: null array");
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-    return noalloc_fail("fsb_diffusion_step_noalloc: no usable current CUDA device");
-  double* scratch = nullptr;
-  {
-    // once per device, with that device current: the host-side name of the
-    // array is not a device address, so ask the runtime for the real one
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_dev[dev]) {
-      void* p = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess)
-        return noalloc_fail(std::string("fsb_diffusion_step_noalloc: cudaGetSymbolAddress failed: ") +
-                            cudaGetErrorString(e));
-      g_scratch_dev[dev] = static_cast<double*>(p);
-    }
-    scratch = g_scratch_dev[dev];
-  }
+  // An error left pending by earlier work of the caller's thread stays the
+  // caller's: this call neither reports it as its own nor clears it.
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess)
+    return noalloc_fail(std::string("fsb_diffusion_step_noalloc: an earlier CUDA error is pending: ") +
+                        cudaGetErrorString(pending));
+  // The host-side name of the array is not a device address.  The address is
+  // looked up on every call, with the caller's device and context current: the
+  // query allocates nothing and stays right after cudaDeviceReset or under
+  // another context on the same device.
+  void* sym = nullptr;
+  const cudaError_t se = cudaGetSymbolAddress(&sym, g_noalloc_scratch);
+  if (se != cudaSuccess)
+    return noalloc_fail(std::string("fsb_diffusion_step_noalloc: cudaGetSymbolAddress failed: ") +
+                        cudaGetErrorString(se));
+  double* scratch = static_cast<double*>(sym);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int* err = reinterpret_cast<int*>(scratch + 7 * (size_t)kNoAllocMaxNodes);
   if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess)
@@ -87,10 +80,13 @@ int fsb_diffusion_step_noalloc(int nx, int ny, double xl, double yl, double dt, 
   bd.xcyc = !bd.fix_left && !bd.fix_right;
   bd.ycyc = !bd.fix_bottom && !bd.fix_top;
   fsb::diffusion_raw(bd, xl / (nx - 1), yl / (ny - 1), dt, kdsed, kd, h, b, etot, erate, scratch, err, st);
+  // launch errors of this call only (nothing was pending at entry)
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return noalloc_fail(std::string("fsb_diffusion_step_noalloc: launch failed: ") + cudaGetErrorString(e));
   int herr = 0;
-  cudaError_t e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return noalloc_fail(std::string("fsb_diffusion_step_noalloc: ") + cudaGetErrorString(e));
   if (herr != 0) return noalloc_fail("fsb_diffusion_step_noalloc: tridag failed (zero pivot)");
   return 0;

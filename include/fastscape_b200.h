@@ -179,16 +179,18 @@ int fsb_stage_times(fsb_ctx* c, double* ms, long long* calls, int n, int reset);
 /* One ADI hillslope-diffusion step on caller-owned device arrays (h, b,
    etot, erate updated in place; kd read) that allocates nothing.  It has no
    counterpart in the reference.  It serves callers that cannot call
-   cudaMalloc -- code inside host callbacks or real-time loops, frameworks
-   that own every allocation through their own pools, programs that must not
-   grow their device footprint after start-up.  The scratch space lives in a
-   static device array of the library sized for nx*ny <= 65536 nodes; larger
-   grids are rejected with an error.  Every GPU that loads the library holds
-   that array (about 3.7 MB) until exit.  The first call on a device looks up
-   the array's device address, so make it before any stream capture.  All
-   calls share the array: calls that overlap on the GPU race.  The call waits
-   for its work on `stream` (a cudaStream_t, may be NULL) to finish and
-   reports a zero pivot as an error (fsb_last_error). */
+   cudaMalloc -- real-time loops that must not stall on the allocator,
+   frameworks that own every allocation through their own pools, programs
+   that must not grow their device footprint after start-up.  The scratch
+   space lives in a static device array of the library sized for
+   nx*ny <= 65536 nodes; larger grids are rejected with an error.  Every GPU
+   that loads the library holds that array (about 3.7 MB) until exit.  Each
+   call looks up the array's device address for the current device and
+   context (a query that allocates nothing).  All calls share the array:
+   calls that overlap on the GPU race.  The call waits for its work on
+   `stream` (a cudaStream_t, may be NULL) to finish, reports a zero pivot as
+   an error (fsb_last_error), and refuses to run while an earlier CUDA error
+   of the calling thread is pending, leaving that error in place. */
 int fsb_diffusion_step_noalloc(int nx, int ny, double xl, double yl, double dt, int bc, double kdsed,
                                const double* kd, double* h, double* b, double* etot, double* erate,
                                void* stream);

@@ -1077,6 +1077,15 @@ int fso_execute_step() {
   return 0;
 }
 
+// Diffusion.f90:1-160 alone on the current state (test entry: compares an
+// ADI step on its own, e.g. on grids the full step refuses)
+int fso_diffusion_only() {
+  Ctx& c = *C;
+  if (!c.setup_done) return fail("Diffusion - You need to run SetUp first");
+  if (!diffusion(c)) return fail("tridag failed");
+  return 0;
+}
+
 int fso_get_step(int* s) { *s = C->step; return 0; }
 int fso_get_sizes(int* nx, int* ny) { *nx = C->nx; *ny = C->ny; return 0; }
 int fso_get_nn() { return C->nn; }

@@ -150,6 +150,11 @@ def fastscape_execute_step():
     _check(lib().fso_execute_step())
 
 
+def diffusion_only():
+    """One ADI diffusion step (Diffusion.f90) on the current state, nothing else."""
+    _check(lib().fso_diffusion_only())
+
+
 def fastscape_get_step() -> int:
     s = ctypes.c_int(0)
     _check(lib().fso_get_step(ctypes.byref(s)))

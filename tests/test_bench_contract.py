@@ -37,3 +37,20 @@ def test_reference_arm_prints_one_contract_line():
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_reference_arm_maps_no_cuda_library():
+    """The reference arm runs the oracle only: after one of its instances has
+    stepped in the bench process, the process has mapped the oracle's library
+    and not the CUDA library of the package."""
+    code = (
+        "import sys; sys.argv=['bench.py']; sys.path.insert(0, %r)\n"
+        "import bench\n"
+        "bench._oracle_worker((33, 1, 0, 1))\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('fsgpu' if 'libfsgpu.so' in maps else 'no-fsgpu')\n"
+        "print('oracle' if 'libfsoracle.so' in maps else 'no-oracle')\n" % ROOT)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300,
+                         cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert out.stdout.split() == ["no-fsgpu", "oracle"], out.stdout

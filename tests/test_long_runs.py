@@ -1,0 +1,121 @@
+"""Free-running error after many steps, GPU against the oracle.
+
+No re-synchronisation: the GPU and the oracle each step the same seeded grid
+from the same initial surface, and the relative L-infinity error
+max |x_gpu - x_oracle| / max(|x_oracle|, 1) is taken per field.
+
+  * Configuration 1 as specified: 101x101, bc = 1111, n = 1, 200 steps, with
+    single flow (p = -2, the D8 the configuration means) against the oracle run
+    alongside, and with the literal p = 0 (uniform multiple flow) against the
+    oracle's checkpoints in tests/golden/long_run.json (steps 50 and 200).
+  * Configuration 2 as specified: the 2049x2049 multiple-flow grid (p = 1.1,
+    n = 1.5 Newton, bc = 1010) for its full 500 steps, against the oracle's
+    checkpoints after 20, 100 and 500 steps (a 2048-node sample of every
+    field, made by tests/golden/make_long_run.py).
+
+Stated bounds (relative L-infinity of h; other fields in BOUNDS below):
+single flow 1e-10 after 200 steps, uniform multiple flow 1e-9 after 200 steps,
+the 2049^2 multiple-flow grid 1e-8 after 20, 1e-7 after 100 and 1e-6 after
+500 steps.  Per step the multiple-flow floats differ by about 1e-12..1e-9
+(summation order of the area); the errors grow slowly along the run.
+Set FSB_REPORT_DIR to also write the measured errors to long_run_errors.json.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from fastscapelib_fortran import workloads as W
+
+from test_gpu_parity import gpu_float, make_gpu, rel_err
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIX_PATH = os.path.join(HERE, "golden", "long_run.json")
+FIX = json.load(open(FIX_PATH)) if os.path.exists(FIX_PATH) else {}
+FIELDS = ("h", "drainage_area", "total_erosion", "erosion_rate", "basement", "lake_depth")
+
+# relative L-infinity bounds per case and checkpoint: h, and every other field
+BOUNDS = {
+    ("plain_101_d8", 200): (1e-10, 1e-8),
+    ("plain_101_p0", 50): (1e-9, 1e-6),
+    ("plain_101_p0", 200): (1e-9, 1e-6),
+    ("mfd_2049", 20): (1e-8, 1e-5),
+    ("mfd_2049", 100): (1e-7, 1e-4),
+    ("mfd_2049", 500): (1e-6, 1e-3),
+}
+_REPORT = {}
+
+
+def _report(case, step, errs):
+    _REPORT.setdefault(case, {})[str(step)] = errs
+    d = os.environ.get("FSB_REPORT_DIR")
+    if d:
+        os.makedirs(d, exist_ok=True)
+        with open(os.path.join(d, "long_run_errors.json"), "w") as fh:
+            json.dump(_REPORT, fh, indent=1)
+
+
+def _check(case, step, errs):
+    _report(case, step, errs)
+    hb, ob = BOUNDS[(case, step)]
+    assert errs["h"] <= hb, (case, step, errs)
+    for f, e in errs.items():
+        assert e <= ob, (case, step, f, errs)
+
+
+def test_config1_single_flow_200_steps():
+    wl = W.plain_d8(101, 101, seed=12345, nsteps=200)
+    wl.apply(O)
+    g = make_gpu(wl)
+    g.set_capture(False)
+    for _ in range(200):
+        O.fastscape_execute_step()
+        g.execute_step()
+    errs = {f: rel_err(gpu_float(g, f), O.copy_double(f)) for f in FIELDS}
+    _check("plain_101_d8", 200, errs)
+    assert np.array_equal(g.copy_int("rec"), O.copy_int("rec"))
+    assert np.array_equal(g.copy_int("stack"), O.copy_int("stack"))
+
+
+def _run_against_fixture(case, wl):
+    import fastscapelib_fortran as fs
+    fx = FIX[case]
+    assert (wl.nx, wl.ny) == (fx["nx"], fx["ny"])
+    idx = np.sort(np.random.default_rng(fx["sample_index_seed"]).choice(
+        wl.nn, fx["sample_size"], replace=False))
+    g = fs.FastScape()
+    g.set_nx_ny(wl.nx, wl.ny)
+    g.setup()
+    g.set_xl_yl(wl.xl, wl.yl)
+    g.set_dt(wl.dt)
+    g.init_h(wl.h0)
+    g.set_erosional_parameters(wl.kf, wl.kfsed, wl.m, wl.n, wl.kd, wl.kdsed, wl.g1, wl.g2, wl.p)
+    g.set_u(wl.u)
+    g.set_bc(wl.bc)
+    step = 0
+    out = np.empty(wl.nn)
+    for cp in sorted(int(k) for k in fx["checkpoints"]):
+        g.execute_step(cp - step)
+        step = cp
+        ref = fx["checkpoints"][str(cp)]
+        errs = {}
+        for f in FIELDS:
+            g.copy(f, out)
+            r = np.asarray(ref["sample"][f])
+            errs[f] = float(np.max(np.abs(out[idx] - r) / np.maximum(np.abs(r), 1.0)))
+        _check(case, cp, errs)
+    g.destroy()
+
+
+@pytest.mark.skipif("plain_101_p0" not in FIX, reason="fixture missing")
+def test_config1_uniform_multiple_flow_200_steps():
+    _run_against_fixture("plain_101_p0", W.plain_d8(101, nsteps=200, p=0.0))
+
+
+@pytest.mark.skipif("mfd_2049" not in FIX, reason="fixture missing")
+def test_config2_multiple_flow_500_steps():
+    _run_against_fixture("mfd_2049", W.mfd(2049, nsteps=500))
