@@ -158,6 +158,21 @@ size_t layout(fsb::Ctx& c, char* base) {
   c.la_ctl = L.take<unsigned>(128);
   c.mfd_line = L.take<double>(16 * N); c.hw = L.take<double>(2 * N);
   c.slots = L.take<double>(fsb::kSlotStride * N);
+  {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+    c.tmap = fsb::plan_tiles(c.nx, c.ny, sms);
+    const size_t P = (size_t)std::max(0ll, c.tmap.padded());
+    const int T = c.tmap.tiles();
+    c.rl_icap = c.tmap.ntx ? 2 * ((1 << c.tmap.ltx) + (1 << c.tmap.lty)) + 16 : 0;
+    c.rl_line = L.take<double>(16 * P);
+    c.rl_val = L.take<double>(2 * P);
+    c.rl_cnt0 = L.take<unsigned char>(P);
+    c.rl_xcnt = L.take<int>(P);
+    c.rl_inbox = L.take<int>((size_t)T * c.rl_icap);
+    c.rl_itail = L.take<unsigned>((size_t)T);
+  }
   c.s_scan2 = L.take<int>(N + 1);
   c.done = L.take<unsigned>(N); c.ticket = L.take<unsigned>(4);
   c.water = L.take<double>(N); c.hnew = L.take<double>(N);
@@ -482,6 +497,20 @@ int fsb_set_erosional_parameters(fsb_ctx* h, const double* kf, double kfsed, dou
   double mx = -DBL_MAX;
   for (double v : hk) mx = std::max(mx, v);
   if (mx > DBL_MIN || kdsed > DBL_MIN) c.runDiffusion = true;
+  return 0;
+}
+
+int fsb_set_precision(fsb_ctx* h, int precision) {
+  if (!h) return fail("null fsb_ctx");
+  if (precision != FSB_PREC_FP64 && precision != FSB_PREC_MIXED)
+    return fail("set_precision: precision must be FSB_PREC_FP64 or FSB_PREC_MIXED");
+  h->c.mixed = precision == FSB_PREC_MIXED;
+  return 0;
+}
+
+int fsb_get_precision(fsb_ctx* h, int* precision) {
+  if (!h || !precision) return fail("null argument");
+  *precision = h->c.mixed ? FSB_PREC_MIXED : FSB_PREC_FP64;
   return 0;
 }
 

@@ -99,6 +99,7 @@ int run_job(Job& j, cudaStream_t stream, std::string& msg) {
   step([&] { return fsb_set_u(h, s.u, FSB_HOST); });
   if (s.precip) step([&] { return fsb_set_precip(h, s.precip, FSB_HOST); });
   step([&] { return fsb_set_bc(h, s.bc); });
+  step([&] { return fsb_set_precision(h, s.precision); });
   step([&] { return fsb_execute_steps(h, s.nsteps); });
   if (s.h_out) step([&] { return fsb_copy_field(h, FSB_H, s.h_out, FSB_HOST); });
   if (s.a_out) step([&] { return fsb_copy_field(h, FSB_DRAINAGE_AREA, s.a_out, FSB_HOST); });

@@ -570,6 +570,10 @@ struct SplMfdOp {
 
 
 // ---- find_mult_rec (FlowRouting.f90:200-243) --------------------------------
+// MIXED: the receivers (FP64 comparisons of the filled surface) are the
+// same; the slopes, their powers and the normalisation run in FP32 (the
+// height differences are taken in FP64 and rounded once).
+template <bool MIXED>
 __global__ void k_mfd_receivers(Bounds bd, double p, const double* __restrict__ h0, const double* __restrict__ ltab,
                                 int* __restrict__ mrec, int* __restrict__ mnrec, double* __restrict__ mwrec,
                                 double* __restrict__ mlrec) {
@@ -605,10 +609,19 @@ __global__ void k_mfd_receivers(Bounds bd, double p, const double* __restrict__ 
       }
       pe = (double)0.5f + (double)0.6f * slope;
     }
-    for (int t = 0; t < nr; ++t) w[t] = pow(w[t], pe);
-    double sumw = 0.0;
-    for (int t = 0; t < nr; ++t) sumw = sumw + w[t];
-    for (int t = 0; t < nr; ++t) mwrec[(size_t)ij * 8 + t] = w[t] / sumw;
+    if constexpr (MIXED) {
+      float wf[8], sumf = 0.0f;
+      for (int t = 0; t < nr; ++t) {
+        wf[t] = powf((float)w[t], (float)pe);
+        sumf = sumf + wf[t];
+      }
+      for (int t = 0; t < nr; ++t) mwrec[(size_t)ij * 8 + t] = (double)(wf[t] / sumf);
+    } else {
+      for (int t = 0; t < nr; ++t) w[t] = pow(w[t], pe);
+      double sumw = 0.0;
+      for (int t = 0; t < nr; ++t) sumw = sumw + w[t];
+      for (int t = 0; t < nr; ++t) mwrec[(size_t)ij * 8 + t] = w[t] / sumw;
+    }
     for (int t = nr; t < 8; ++t) { mrec[(size_t)ij * 8 + t] = -1; mwrec[(size_t)ij * 8 + t] = 0.0; mlrec[(size_t)ij * 8 + t] = 0.0; }
     mnrec[ij] = nr;
   }
@@ -874,11 +887,29 @@ __global__ void k_diff_kdint(int nn, double kdsed, const double* __restrict__ kd
   }
 }
 
+// What a coefficient kernel stores for one equation a*z(t-1) + bb*z(t) +
+// c*z(t+1) = f.  Plain (T = double): the coefficients and f.  Mixed
+// precision (T = float): the coefficients rounded to float and, in place of
+// f, the residual r = f - (a*z0(t-1) + bb*z0(t) + c*z0(t+1)) of the current
+// surface z0, evaluated in FP64; the FP32 solve then gives the increment
+// z - z0, which is added to z0 in FP64.
+template <class T>
+__device__ inline void store_equation(T* A, T* B, T* C, T* F, size_t o, double a, double bb, double c, double f,
+                                      double zm, double z0, double zp) {
+  if constexpr (sizeof(T) == sizeof(double)) {
+    A[o] = a; B[o] = bb; C[o] = c; F[o] = f;
+  } else {
+    const double r = f - (a * zm + bb * z0 + c * zp);
+    A[o] = (T)a; B[o] = (T)bb; C[o] = (T)c; F[o] = (T)r;
+  }
+}
+
 // x pass coefficients for rows j=1..ny-2, stored transposed: element i of
 // row j at [i*ny + j]
+template <class T>
 __global__ void k_diff_xcoef(Bounds bd, double dt2, double dx2, double dy2, const double* __restrict__ K,
-                             const double* __restrict__ z, double* __restrict__ A, double* __restrict__ B,
-                             double* __restrict__ C, double* __restrict__ F) {
+                             const double* __restrict__ z, T* __restrict__ A, T* __restrict__ B,
+                             T* __restrict__ C, T* __restrict__ F) {
   const int nx = bd.nx, ny = bd.ny;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y + 1;
@@ -919,13 +950,14 @@ __global__ void k_diff_xcoef(Bounds bd, double dt2, double dx2, double dy2, cons
       f = Z(nx - 1, j) + fyp * Z(nx - 1, j + 1) - (fyp + fym) * Z(nx - 1, j) + fym * Z(nx - 1, j - 1);
     }
   }
-  A[o] = a; B[o] = bb; C[o] = c; F[o] = f;
+  store_equation(A, B, C, F, o, a, bb, c, f, i > 0 ? Z(i - 1, j) : 0.0, Z(i, j), i < nx - 1 ? Z(i + 1, j) : 0.0);
 }
 
 // y pass coefficients for columns i=1..nx-2 (natural layout [j*nx + i])
+template <class T>
 __global__ void k_diff_ycoef(Bounds bd, double dt2, double dx2, double dy2, const double* __restrict__ K,
-                             const double* __restrict__ z, double* __restrict__ A, double* __restrict__ B,
-                             double* __restrict__ C, double* __restrict__ F) {
+                             const double* __restrict__ z, T* __restrict__ A, T* __restrict__ B,
+                             T* __restrict__ C, T* __restrict__ F) {
   const int nx = bd.nx, ny = bd.ny;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
@@ -967,7 +999,7 @@ __global__ void k_diff_ycoef(Bounds bd, double dt2, double dx2, double dy2, cons
       f = Z(i, ny - 1) + fxp * Z(i + 1, ny - 1) - (fxp + fxm) * Z(i, ny - 1) + fxm * Z(i - 1, ny - 1);
     }
   }
-  A[o] = a; B[o] = bb; C[o] = c; F[o] = f;
+  store_equation(A, B, C, F, o, a, bb, c, f, j > 0 ? Z(i, j - 1) : 0.0, Z(i, j), j < ny - 1 ? Z(i, j + 1) : 0.0);
 }
 
 // tridag (Diffusion.f90:164-202) for independent systems s in [s0, s1):
@@ -976,32 +1008,37 @@ __global__ void k_diff_ycoef(Bounds bd, double dt2, double dx2, double dy2, cons
 // memory in chunks of kTC steps so that the sequential recurrence only waits
 // on arithmetic, not on DRAM latency.
 constexpr int kTC = 32;
-__device__ inline void cp_async8(void* smem, const void* gmem) {
+__device__ inline void cp_async_elem(double* smem, const double* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ inline void cp_async_elem(float* smem, const float* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem));
 }
 __device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ inline void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-__global__ void __launch_bounds__(32) k_thomas(int N, int L, int s0, int s1, const double* __restrict__ A,
-                                               const double* __restrict__ B, const double* __restrict__ C,
-                                               double* __restrict__ F, double* __restrict__ G,
+template <class T>
+__global__ void __launch_bounds__(32) k_thomas(int N, int L, int s0, int s1, const T* __restrict__ A,
+                                               const T* __restrict__ B, const T* __restrict__ C,
+                                               T* __restrict__ F, T* __restrict__ G,
                                                int* __restrict__ err) {
-  __shared__ double sa[kTC][33], sb[kTC][33], sc[kTC][33], sf[kTC][33];
+  __shared__ T sa[kTC][33], sb[kTC][33], sc[kTC][33], sf[kTC][33];
   const int lane = threadIdx.x;
   const int s = s0 + blockIdx.x * 32 + lane;
   const bool act = s < s1;
-  double bet = 0.0, up = 0.0;
+  T bet = 0, up = 0;
   bool bad = false;
   for (int t0 = 0; t0 < N; t0 += kTC) {
     const int tn = min(kTC, N - t0);
     if (act) {  // all loads of the chunk in flight at once
       for (int r = 0; r < tn; ++r) {
         const size_t o = (size_t)(t0 + r) * L + s;
-        cp_async8(&sa[r][lane], &A[o]);
-        cp_async8(&sb[r][lane], &B[o]);
-        cp_async8(&sf[r][lane], &F[o]);
-        if (t0 + r > 0) cp_async8(&sc[r][lane], &C[o - L]);
+        cp_async_elem(&sa[r][lane], &A[o]);
+        cp_async_elem(&sb[r][lane], &B[o]);
+        cp_async_elem(&sf[r][lane], &F[o]);
+        if (t0 + r > 0) cp_async_elem(&sc[r][lane], &C[o - L]);
       }
     }
     cp_async_commit();
@@ -1017,7 +1054,7 @@ __global__ void __launch_bounds__(32) k_thomas(int N, int L, int s0, int s1, con
           sf[0][lane] = up;
           sc[0][lane] = 0.0;
         } else {
-          const double g = sc[r][lane] / bet;
+          const T g = sc[r][lane] / bet;
           sc[r][lane] = g;
           bet = sb[r][lane] - sa[r][lane] * g;
           if (bet == 0.0) { bad = true; break; }
@@ -1044,8 +1081,8 @@ __global__ void __launch_bounds__(32) k_thomas(int N, int L, int s0, int s1, con
     if (act)
       for (int r = 0; r < tn; ++r) {
         const size_t o = (size_t)(tlo + r) * L + s;
-        cp_async8(&sf[r][lane], &F[o]);
-        cp_async8(&sc[r][lane], &G[o + L]);
+        cp_async_elem(&sf[r][lane], &F[o]);
+        cp_async_elem(&sc[r][lane], &G[o + L]);
       }
     cp_async_commit();
     cp_async_wait_all();
@@ -1062,10 +1099,12 @@ __global__ void __launch_bounds__(32) k_thomas(int N, int L, int s0, int s1, con
   }
 }
 
-// zint = x-pass result on rows 1..ny-2, h elsewhere (natural layout)
-__global__ void k_diff_xgather(Bounds bd, const double* __restrict__ Ux, const double* __restrict__ h,
+// zint = x-pass result on rows 1..ny-2, h elsewhere (natural layout); in the
+// mixed form the solve gave the increment, added to h in FP64
+template <class T>
+__global__ void k_diff_xgather(Bounds bd, const T* __restrict__ Ux, const double* __restrict__ h,
                                double* __restrict__ zint) {
-  __shared__ double tile[32][33];
+  __shared__ T tile[32][33];
   const int nx = bd.nx, ny = bd.ny;
   // tile over (i, j): read Ux[i*ny + j] coalesced along j, write zint coalesced along i
   const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
@@ -1078,8 +1117,28 @@ __global__ void k_diff_xgather(Bounds bd, const double* __restrict__ Ux, const d
     const int j = j0 + r, i = i0 + threadIdx.x;
     if (i < nx && j < ny) {
       const size_t o = (size_t)j * nx + i;
-      zint[o] = (j >= 1 && j <= ny - 2) ? tile[threadIdx.x][r] : h[o];
+      if constexpr (sizeof(T) == sizeof(double))
+        zint[o] = (j >= 1 && j <= ny - 2) ? tile[threadIdx.x][r] : h[o];
+      else
+        zint[o] = (j >= 1 && j <= ny - 2) ? h[o] + (double)tile[threadIdx.x][r] : h[o];
     }
+  }
+}
+
+// mixed form of k_diff_finish: zintp = zint + the y-pass increment on columns
+// 1..nx-2, h elsewhere
+__global__ void k_diff_finish_m(Bounds bd, double dt, const float* __restrict__ dUy, const double* __restrict__ zint,
+                                double* __restrict__ h, double* __restrict__ b, double* __restrict__ etot,
+                                double* __restrict__ erate) {
+  const int nx = bd.nx, nn = nx * bd.ny;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const int i = k % nx;
+    const double hk = h[k];
+    const double zp = (i >= 1 && i <= nx - 2) ? zint[k] + (double)dUy[k] : hk;
+    etot[k] = etot[k] + hk - zp;
+    erate[k] = erate[k] + (hk - zp) / dt;
+    h[k] = zp;
+    b[k] = fmin(zp, b[k]);
   }
 }
 
@@ -1104,7 +1163,12 @@ __global__ void k_diff_finish(Bounds bd, double dt, const double* __restrict__ U
 
 void mfd_receivers(Ctx& c) {
   const int nn = c.nn;
-  k_mfd_receivers<<<grid1d(nn), kBlock, 0, c.stream>>>(c.bd, c.p, c.hwater, c.ltab, c.mrec, c.mnrec, c.mwrec, c.mlrec);
+  if (c.mixed)
+    k_mfd_receivers<true><<<grid1d(nn), kBlock, 0, c.stream>>>(c.bd, c.p, c.hwater, c.ltab, c.mrec, c.mnrec, c.mwrec,
+                                                               c.mlrec);
+  else
+    k_mfd_receivers<false><<<grid1d(nn), kBlock, 0, c.stream>>>(c.bd, c.p, c.hwater, c.ltab, c.mrec, c.mnrec,
+                                                                c.mwrec, c.mlrec);
   c.count_launch();
   if (c.capture) {  // a topological order of mrec (the reference's mstack is a LIFO Kahn order)
     k_order_keys<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, c.stack, c.hwater, c.o_keys, c.o_vals);
@@ -1168,6 +1232,7 @@ void accumulate(Ctx& c) {
     }
     return;
   }
+  if (region_accumulate(c)) return;
   AccLine* line = static_cast<AccLine*>(c.mfd_line);
   k_acc_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, c.dx * c.dy, c.mrec, c.mnrec, c.mwrec, c.precip, c.size,
                                                      line, c.cnt_acc, c.d_err);
@@ -1228,6 +1293,7 @@ void stream_power(Ctx& c) {
     c.count_launch();
     return;
   }
+  if (region_stream_power(c)) return;
   // the erosion factors need the drainage area: the lines are built now
   SplLine* line = static_cast<SplLine*>(c.mfd_line);
   k_spl_lines<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec, c.mnrec, c.mwrec,
@@ -1245,11 +1311,38 @@ void stream_power(Ctx& c) {
 void thomas_lines(Ctx& c, int N, int L, int s0, int s1, const double* A, const double* B, const double* C, double* F,
                   double* G) {
   if (s1 <= s0) return;
-  k_thomas<<<(s1 - s0 + 31) / 32, 32, 0, c.stream>>>(N, L, s0, s1, A, B, C, F, G, c.d_err);
+  k_thomas<double><<<(s1 - s0 + 31) / 32, 32, 0, c.stream>>>(N, L, s0, s1, A, B, C, F, G, c.d_err);
   c.count_launch();
 }
 
+// Mixed-precision ADI step: coefficients as in the plain form, each line
+// solved in FP32 for the increment of the surface against the FP64 residual
+// of the current surface, the increment added in FP64.
+static void diffusion_mixed(Ctx& c) {
+  const int nx = c.nx, ny = c.ny, nn = c.nn;
+  const double dt2 = c.dt / 2.0, dx2 = c.dx * c.dx, dy2 = c.dy * c.dy;
+  double *K = c.dK, *Z = c.dZ;
+  float *A = reinterpret_cast<float*>(c.dA), *B = reinterpret_cast<float*>(c.dB),
+        *C = reinterpret_cast<float*>(c.dC), *F = reinterpret_cast<float*>(c.dF),
+        *G = reinterpret_cast<float*>(c.dG);
+  k_diff_kdint<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, c.kdsed, c.kd, c.h, c.b, K);
+  dim3 gx((nx + 127) / 128, ny - 2);
+  k_diff_xcoef<float><<<gx, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, c.h, A, B, C, F);
+  k_thomas<float><<<(ny - 2 + 31) / 32, 32, 0, c.stream>>>(nx, ny, 1, ny - 1, A, B, C, F, G, c.d_err);
+  dim3 g2((nx + 31) / 32, (ny + 31) / 32);
+  k_diff_xgather<float><<<g2, dim3(32, 8), 0, c.stream>>>(c.bd, F, c.h, Z);
+  dim3 gy((nx + 127) / 128, ny);
+  k_diff_ycoef<float><<<gy, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, Z, A, B, C, F);
+  k_thomas<float><<<(nx - 2 + 31) / 32, 32, 0, c.stream>>>(ny, nx, 1, nx - 1, A, B, C, F, G, c.d_err);
+  k_diff_finish_m<<<grid1d(nn), kBlock, 0, c.stream>>>(c.bd, c.dt, F, Z, c.h, c.b, c.etot, c.erate);
+  c.count_launch(7);
+}
+
 void diffusion(Ctx& c) {
+  if (c.mixed) {
+    diffusion_mixed(c);
+    return;
+  }
   const int nx = c.nx, ny = c.ny, nn = c.nn;
   const double dt2 = c.dt / 2.0, dx2 = c.dx * c.dx, dy2 = c.dy * c.dy;
   double *K = c.dK, *A = c.dA, *B = c.dB, *C = c.dC, *F = c.dF, *G = c.dG, *Z = c.dZ;
@@ -1257,17 +1350,17 @@ void diffusion(Ctx& c) {
   c.count_launch();
   {
     dim3 g((nx + 127) / 128, ny - 2);
-    k_diff_xcoef<<<g, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, c.h, A, B, C, F);
+    k_diff_xcoef<double><<<g, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, c.h, A, B, C, F);
     // systems are rows j=1..ny-2 with element i at [i*ny + j]
-    k_thomas<<<(ny - 2 + 31) / 32, 32, 0, c.stream>>>(nx, ny, 1, ny - 1, A, B, C, F, G, c.d_err);
+    k_thomas<double><<<(ny - 2 + 31) / 32, 32, 0, c.stream>>>(nx, ny, 1, ny - 1, A, B, C, F, G, c.d_err);
     dim3 g2((nx + 31) / 32, (ny + 31) / 32);
-    k_diff_xgather<<<g2, dim3(32, 8), 0, c.stream>>>(c.bd, F, c.h, Z);
+    k_diff_xgather<double><<<g2, dim3(32, 8), 0, c.stream>>>(c.bd, F, c.h, Z);
     c.count_launch(3);
   }
   {
     dim3 g((nx + 127) / 128, ny);
-    k_diff_ycoef<<<g, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, Z, A, B, C, F);
-    k_thomas<<<(nx - 2 + 31) / 32, 32, 0, c.stream>>>(ny, nx, 1, nx - 1, A, B, C, F, G, c.d_err);
+    k_diff_ycoef<double><<<g, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, Z, A, B, C, F);
+    k_thomas<double><<<(nx - 2 + 31) / 32, 32, 0, c.stream>>>(ny, nx, 1, nx - 1, A, B, C, F, G, c.d_err);
     c.count_launch(2);
   }
   k_diff_finish<<<grid1d(nn), kBlock, 0, c.stream>>>(c.bd, c.dt, F, c.h, c.b, c.etot, c.erate);
@@ -1290,13 +1383,13 @@ void diffusion_raw(const Bounds& bd, double dx, double dy, double dt, double kds
   double* Z = G + nn;
   k_diff_kdint<<<grid1d(nn), kBlock, 0, st>>>(nn, kdsed, kd, h, b, K);
   dim3 gx((nx + 127) / 128, ny - 2);
-  k_diff_xcoef<<<gx, 128, 0, st>>>(bd, dt2, dx2, dy2, K, h, A, B, C, F);
-  k_thomas<<<(ny - 2 + 31) / 32, 32, 0, st>>>(nx, ny, 1, ny - 1, A, B, C, F, G, err);
+  k_diff_xcoef<double><<<gx, 128, 0, st>>>(bd, dt2, dx2, dy2, K, h, A, B, C, F);
+  k_thomas<double><<<(ny - 2 + 31) / 32, 32, 0, st>>>(nx, ny, 1, ny - 1, A, B, C, F, G, err);
   dim3 gt((nx + 31) / 32, (ny + 31) / 32);
-  k_diff_xgather<<<gt, dim3(32, 8), 0, st>>>(bd, F, h, Z);
+  k_diff_xgather<double><<<gt, dim3(32, 8), 0, st>>>(bd, F, h, Z);
   dim3 gy((nx + 127) / 128, ny);
-  k_diff_ycoef<<<gy, 128, 0, st>>>(bd, dt2, dx2, dy2, K, Z, A, B, C, F);
-  k_thomas<<<(nx - 2 + 31) / 32, 32, 0, st>>>(ny, nx, 1, nx - 1, A, B, C, F, G, err);
+  k_diff_ycoef<double><<<gy, 128, 0, st>>>(bd, dt2, dx2, dy2, K, Z, A, B, C, F);
+  k_thomas<double><<<(nx - 2 + 31) / 32, 32, 0, st>>>(ny, nx, 1, nx - 1, A, B, C, F, G, err);
   k_diff_finish<<<grid1d(nn), kBlock, 0, st>>>(bd, dt, F, h, b, etot, erate);
 }
 

@@ -23,6 +23,23 @@ inline unsigned grid1d(size_t n, int block = kBlock) {
   return (unsigned)g;
 }
 
+// Tile-major numbering of the grid for the region-owned sweeps (fsb_region.cu):
+// tiles of 2^ltx x 2^lty nodes, tile t = ty*ntx + tx, node (i, j) at
+// g = t*2^(ltx+lty) + (j mod 2^lty)*2^ltx + (i mod 2^ltx).  Slots of partial
+// tiles beyond the grid are padding.
+struct TileMap {
+  int nx = 0, ny = 0;
+  int ltx = 0, lty = 0;
+  int ntx = 0, nty = 0;  // ntx == 0: no plan
+  __host__ __device__ int lr() const { return ltx + lty; }
+  __host__ __device__ int tiles() const { return ntx * nty; }
+  __host__ __device__ long long padded() const { return (long long)tiles() << lr(); }
+  __host__ __device__ int g(int i, int j) const {
+    const int t = (j >> lty) * ntx + (i >> ltx);
+    return (t << lr()) | ((j & ((1 << lty) - 1)) << ltx) | (i & ((1 << ltx) - 1));
+  }
+};
+
 struct Ctx {
   // ---- configuration (setters of FastScape_ctx.f90) ----
   int nx = 0, ny = 0, nn = 0;
@@ -32,6 +49,9 @@ struct Ctx {
   double dx = 0, dy = 0;
   bool sfd = false, runSPL = false, runDiffusion = false, runUplift = false;
   bool setup_done = false;
+  // mixed precision (fsb_set_precision): FP32 weights, area, Newton iterations
+  // and tridiagonal solves; FP64 state, h update and residuals
+  bool mixed = false;
   bool capture = false;  // keep LocalMinima intermediates of the last step
   bool routed = false;   // a step has built receivers, stack, chains and area
   bool precip_uniform = true;  // every node has precipitation precip_value (SetUp: 1)
@@ -109,6 +129,17 @@ struct Ctx {
   void* mfd_line = nullptr;  // one 128-byte record per node (area, then stream power)
   double* hw = nullptr;      // (elevation, water surface) pairs of the stream-power sweep
   double* slots = nullptr;   // kSlotStride input slots per node of the multiple-flow sweeps
+  // region-owned sweeps (fsb_region.cu): tile plan and tile-major buffers
+  TileMap tmap{};
+  bool region_enabled = true;  // use them when the plan and a cooperative launch allow
+  int region_state = 0;        // 0 unchecked, 1 usable, -1 not usable on this device
+  void* rl_line = nullptr;     // one 128-byte line per tile-major slot
+  double* rl_val = nullptr;    // 2 doubles per slot: area, or (h, water)
+  unsigned char* rl_cnt0 = nullptr;  // initial counters, one byte per slot
+  int* rl_xcnt = nullptr;      // cross-tile inputs per slot
+  int* rl_inbox = nullptr;     // per tile: nodes whose cross-tile inputs are all in
+  unsigned* rl_itail = nullptr;
+  int rl_icap = 0;
   unsigned* la_ctl = nullptr;  // head, tail, done count
   int* s_scan2 = nullptr;
   // sweeps
@@ -171,6 +202,11 @@ void flux_chains(Ctx& c, double* flux);               // compute_fluxes' flux, s
 void chi_chains(Ctx& c, double a0, double mn, double* chi);
 void flux_mfd(Ctx& c, double* flux);                  // compute_fluxes' flux, multiple flow
 // tridiagonal systems s0..s1-1, element t of system s at [t*L + s], F solved in place
+// region-owned multiple-flow sweeps (fsb_region.cu); false: not usable, the
+// queue engine of fsb_flow.cu runs instead
+TileMap plan_tiles(int nx, int ny, int sms);
+bool region_accumulate(Ctx& c);
+bool region_stream_power(Ctx& c);
 void thomas_lines(Ctx& c, int N, int L, int s0, int s1, const double* A, const double* B, const double* C, double* F,
                   double* G);
 void advect(Ctx& c);  // fsb_advect.cu

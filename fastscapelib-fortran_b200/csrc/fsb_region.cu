@@ -1,0 +1,965 @@
+// Region-owned sweeps of the multiple-flow receiver DAG: drainage area and
+// the implicit stream power law with g == 0.
+//
+// Reference loops restated (fastscapelib-fortran file:line):
+//   FlowAccumulation (MFD)   src/FlowRouting.f90:97-119
+//   StreamPowerLaw (MFD)     src/StreamPowerLaw.f90:89-177 (g == 0: one
+//                            Gauss-Seidel pass, elev = ht)
+//
+// Both sweeps are recurrences along the receiver DAG whose critical path is
+// about three grid sides long, so their time is the number of hops on that
+// path times the latency of one hop.  Here the grid is cut into 2^a x 2^b
+// tiles, one co-resident CTA per tile (cooperative launch), and nodes are
+// numbered tile-major (a tile's nodes are contiguous).  A CTA keeps its
+// tile's dependency counters (one byte per node, four to a word) and its
+// ready queue in shared memory: a hop between two nodes of one tile is a
+// shared-memory atomic and loads that the SM's L1 serves, not an L2 round
+// trip.  Every node's value lands once in a tile-major value array, from
+// which its dependents gather it, so no input slots need resetting.  A
+// dependency that crosses a tile boundary goes through a global counter; its
+// last producer posts the node into the owning CTA's inbox (release/acquire
+// at GPU scope), which one lane of the CTA polls.  The arithmetic of a node,
+// including the order of its sums, is that of the queue engine in
+// fsb_flow.cu, so both engines give bit-identical results.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+
+#include "fsb_kernels.cuh"
+
+namespace fsb {
+
+namespace {
+
+constexpr int kRegionThreads = 256;       // 8 warps: one inbox poller + 7 workers
+constexpr unsigned short kQEmpty = 0xFFFF;
+constexpr unsigned long long kRegionTimeLimitNs = 4000000000ull;  // a sweep giving up: 4 s
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// weak load that the SM's L1 may serve (values written by this CTA)
+__device__ __forceinline__ double ld_l1(const double* p) {
+  double v;
+  asm volatile("ld.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ double2 ld_l1(const double2* p) {
+  double2 v;
+  asm volatile("ld.global.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p) : "memory");
+  return v;
+}
+// load from L2 (values written by other SMs, after an acquire)
+__device__ __forceinline__ double ld_l2(const double* p) {
+  double v;
+  asm volatile("ld.global.cg.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ double2 ld_l2(const double2* p) {
+  double2 v;
+  asm volatile("ld.global.cg.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ float ld_l1f(const float* p) {
+  float v;
+  asm volatile("ld.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ float ld_l2f(const float* p) {
+  float v;
+  asm volatile("ld.global.cg.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_globalf(float* p, float v) {
+  asm volatile("st.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+__device__ __forceinline__ void st_global(double* p, double v) {
+  asm volatile("st.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_global(double2* p, double2 v) {
+  asm volatile("st.global.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(v.x), "d"(v.y) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_gpu_int(int* p, int v) {
+  asm volatile("st.relaxed.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+__device__ inline unsigned short prio16(int size) { return (unsigned short)(__float_as_uint((float)size) >> 16); }
+
+// Inserts node v of priority p into dep[0..n) / pr[0..n) (n < 8), kept in
+// decreasing priority with ties in insertion order (registers only).
+__device__ inline void insert_by_priority(int (&dep)[8], unsigned (&pr)[8], int n, int v, unsigned p) {
+  int pos = 0;
+#pragma unroll
+  for (int t = 0; t < 8; ++t) pos += (t < n && pr[t] >= p) ? 1 : 0;
+#pragma unroll
+  for (int t = 7; t > 0; --t)
+    if (t > pos && t <= n) {
+      dep[t] = dep[t - 1];
+      pr[t] = pr[t - 1];
+    }
+#pragma unroll
+  for (int t = 0; t < 8; ++t)
+    if (t == pos) {
+      dep[t] = v;
+      pr[t] = p;
+    }
+}
+template <class T>
+__device__ inline void set_at(T (&a)[8], int n, T v) {
+#pragma unroll
+  for (int t = 0; t < 8; ++t)
+    if (t == n) a[t] = v;
+}
+template <class T>
+__device__ inline bool contains(const T (&a)[8], int n, T v) {
+  bool f = false;
+#pragma unroll
+  for (int t = 0; t < 8; ++t) f |= t < n && a[t] == v;
+  return f;
+}
+__device__ inline bool is_neighbour(int i, int j, int q, int nx, int ny) {
+  int di = q % nx - i, dj = q / nx - j;
+  if (di > 1) di -= nx; else if (di < -1) di += nx;
+  if (dj > 1) dj -= ny; else if (dj < -1) dj += ny;
+  return di >= -1 && di <= 1 && dj >= -1 && dj <= 1 && (di != 0 || dj != 0);
+}
+
+// One record line per node, tile-major: the inputs a node gathers, their
+// coefficients, and its dependents (tile-major indices, -1 past the last;
+// dependents largest priority first).
+//   area:          c[t] = summed weight of input (donor) t's slots targeting k
+//   stream power:  c[t] = kf*dt*(a*w)^m/l^n of gated receiver slot t
+// The coefficients are double in the plain form and float in the mixed one.
+template <class T>
+struct __align__(128) RegionLineT {
+  T c[8];
+  int dep[8];
+  int inp[8];
+};
+using RegionLine = RegionLineT<double>;
+using RegionLineF = RegionLineT<float>;
+static_assert(sizeof(RegionLine) == 128 && sizeof(RegionLineF) == 128, "one line per node");
+
+// a line in registers: the words that hold data (128 bytes, or 96 with float
+// coefficients), read through the read-only path
+template <class T>
+struct LineRegsT {
+  static constexpr int kWords = (8 * (int)sizeof(T) + 64) / 16;
+  static constexpr int kDep = 2 * (int)sizeof(T);  // int index of dep[0]
+  union {
+    int4 v[kWords];
+    T c[8];
+    int s[4 * kWords];
+  };
+  __device__ explicit LineRegsT(const RegionLineT<T>* p) {
+#pragma unroll
+    for (int t = 0; t < kWords; ++t) v[t] = __ldg(reinterpret_cast<const int4*>(p) + t);
+  }
+  __device__ int dep(int t) const { return s[kDep + t]; }
+  __device__ int inp(int t) const { return s[kDep + 8 + t]; }
+};
+using LineRegs = LineRegsT<double>;
+
+// stream-power node metadata kept in the value array's water word until the
+// node is computed: rec (tile-major, or -1 for a root) and whether mnrec > 0
+__device__ inline double pack_meta(int rec_g, bool has_mrec) {
+  const long long v = (long long)(unsigned)rec_g | (has_mrec ? (1ll << 40) : 0ll);
+  return __longlong_as_double(v);
+}
+__device__ inline void unpack_meta(double w, int& rec_g, bool& has_mrec) {
+  const long long v = __double_as_longlong(w);
+  rec_g = (int)(unsigned)(v & 0xffffffffll);
+  has_mrec = (v >> 40) & 1;
+}
+
+// ---- line builders (natural node order in, tile-major out) ------------------
+
+// Area: inputs are k's distinct donors among its 3x3 neighbours (jj outer, ii
+// inner, as FlowRouting.f90's neighbour loops) with the summed weight of
+// their slots targeting k; dependents are k's distinct receivers.  cnt0 gets
+// the in-tile input count plus one if any input lies in another tile (that
+// token is released by the inbox); xcnt the number of cross-tile inputs.
+template <class T>
+__global__ void k_acc_lines_t(Bounds bd, TileMap tm, double dxdy, const int* __restrict__ mrec,
+                              const int* __restrict__ mnrec, const double* __restrict__ mwrec,
+                              const double* __restrict__ precip, const int* __restrict__ prio,
+                              RegionLineT<T>* __restrict__ line, T* __restrict__ val,
+                              unsigned char* __restrict__ cnt0, int* __restrict__ xcnt, int* err) {
+  const int nx = bd.nx, ny = bd.ny, nn = nx * ny;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const int i = k % nx, j = k / nx;
+    const int gk = tm.g(i, j);
+    const int tile = gk >> tm.lr();
+    const size_t o = (size_t)k * 8;
+    const int nr = mnrec[k];
+    int mr[8], dep[8];
+    unsigned pr[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      mr[t] = t < nr ? mrec[o + t] : -1;
+      dep[t] = -1;
+      pr[t] = 0u;
+    }
+    int rn = 0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      if (t >= nr) break;
+      const int q = mr[t];
+      if (contains(mr, t, q)) continue;
+      if (!is_neighbour(i, j, q, nx, ny)) atomicExch(err, DEV_NOT_ADJACENT);
+      insert_by_priority(dep, pr, rn++, tm.g(q % nx, q / nx), prio16(prio[q]));
+    }
+    int inp[8], seen[8];
+    double aw[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      aw[t] = 0.0;
+      inp[t] = -1;
+    }
+    int an = 0, ns = 0, nin = 0, nx_in = 0;
+#pragma unroll
+    for (int jj = -1; jj <= 1; ++jj) {
+      int y = j + jj;
+      if (y < 0) { if (!bd.ycyc) continue; y += ny; }
+      if (y >= ny) { if (!bd.ycyc) continue; y -= ny; }
+#pragma unroll
+      for (int ii = -1; ii <= 1; ++ii) {
+        int x = i + ii;
+        if (x < 0) { if (!bd.xcyc) continue; x += nx; }
+        if (x >= nx) { if (!bd.xcyc) continue; x -= nx; }
+        const int d = x + y * nx;
+        if (d == k || contains(seen, ns, d)) continue;
+        set_at(seen, ns++, d);
+        const int nd = mnrec[d];
+        double wsum = 0.0;
+        int hits = 0;
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+          if (t < nd && mrec[(size_t)d * 8 + t] == k) {
+            const double w = mwrec[(size_t)d * 8 + t];
+            wsum = hits ? wsum + w : w;
+            ++hits;
+          }
+        if (hits && an < 8) {
+          const int gd = tm.g(x, y);
+          set_at(inp, an, gd);
+          set_at(aw, an++, wsum);
+          if ((gd >> tm.lr()) == tile) ++nin; else ++nx_in;
+        }
+      }
+    }
+    RegionLineT<T> L;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      L.c[t] = (T)aw[t];
+      L.dep[t] = dep[t];
+      L.inp[t] = inp[t];
+    }
+    line[gk] = L;
+    val[gk] = (T)(dxdy * precip[k]);
+    cnt0[gk] = (unsigned char)(nin + (nx_in > 0 ? 1 : 0));
+    xcnt[gk] = nx_in;
+  }
+}
+
+// Stream power: inputs are k's gated receiver slots (ht(k) >= ht(q) for n = 1,
+// > otherwise: the terms StreamPowerLaw.f90:108-114 / 152-158 include), in
+// mrec slot order, duplicates kept; the counter also waits for rec(k), whose
+// water the node compares against.  Dependents are the donors that read
+// k's new elevation (gated) or its water (rec == k).  The value array starts
+// as (ht, metadata) and ends as (h, water).
+template <class T>
+__global__ void k_spl_lines_t(Bounds bd, TileMap tm, int n_is_one, double kfsed, double dt, double m, double n,
+                              const int* __restrict__ rec, const int* __restrict__ mrec,
+                              const int* __restrict__ mnrec, const double* __restrict__ mwrec,
+                              const double* __restrict__ mlrec, const double* __restrict__ h,
+                              const double* __restrict__ b, const double* __restrict__ kf,
+                              const double* __restrict__ a, const int* __restrict__ prio,
+                              RegionLineT<T>* __restrict__ line, double2* __restrict__ hw,
+                              unsigned char* __restrict__ cnt0, int* __restrict__ xcnt, int* err) {
+  const int nx = bd.nx, ny = bd.ny, nn = nx * ny;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const int i = k % nx, j = k / nx;
+    const int gk = tm.g(i, j);
+    const int tile = gk >> tm.lr();
+    const size_t o = (size_t)k * 8;
+    const double htk = h[k];
+    const int nr = mnrec[k];
+    const int r = rec[k];
+    const double kk = ((kfsed > 0.0 && (htk - b[k]) > 1.0) ? kfsed : kf[k]) * dt;
+    const double ak = a[k];
+    int qv[8], inp[8], dep[8];
+    unsigned pr[8];
+    T fact[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      qv[t] = -1;
+      inp[t] = -1;
+      dep[t] = -1;
+      pr[t] = 0u;
+      fact[t] = 0;
+    }
+    int nq = 0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      if (t >= nr) break;
+      const int q = mrec[o + t];
+      if (n_is_one ? (htk >= h[q]) : (htk > h[q])) {
+        const double w = mwrec[o + t], l = mlrec[o + t];
+        if (!is_neighbour(i, j, q, nx, ny)) atomicExch(err, DEV_NOT_ADJACENT);
+        if constexpr (sizeof(T) == sizeof(double)) {
+          set_at(fact, nq, n_is_one ? kk * pow(ak * w, m) / l : kk * pow(ak * w, m) / pow(l, n));
+        } else {  // mixed precision: the erosion factor in FP32
+          const float kf32 = (float)kk, aw32 = (float)(ak * w), l32 = (float)l;
+          set_at(fact, nq, n_is_one ? kf32 * powf(aw32, (float)m) / l32
+                                    : kf32 * powf(aw32, (float)m) / powf(l32, (float)n));
+        }
+        set_at(inp, nq, tm.g(q % nx, q / nx));
+        set_at(qv, nq++, q);
+      }
+    }
+    // distinct inputs: gated receivers and rec(k), split by tile
+    int nin = 0, nx_in = 0;
+    if (r != k) {
+      if (!is_neighbour(i, j, r, nx, ny)) atomicExch(err, DEV_NOT_ADJACENT);
+#pragma unroll
+      for (int t = 0; t < 8; ++t)
+        if (t < nq && !contains(qv, t, qv[t])) {
+          if ((tm.g(qv[t] % nx, qv[t] / nx) >> tm.lr()) == tile) ++nin; else ++nx_in;
+        }
+      if (!contains(qv, nq, r)) {
+        if ((tm.g(r % nx, r / nx) >> tm.lr()) == tile) ++nin; else ++nx_in;
+      }
+    }
+    int dn = 0, ns = 0;
+    int seen[8];
+#pragma unroll
+    for (int jj = -1; jj <= 1; ++jj) {
+      int y = j + jj;
+      if (y < 0) { if (!bd.ycyc) continue; y += ny; }
+      if (y >= ny) { if (!bd.ycyc) continue; y -= ny; }
+#pragma unroll
+      for (int ii = -1; ii <= 1; ++ii) {
+        int x = i + ii;
+        if (x < 0) { if (!bd.xcyc) continue; x += nx; }
+        if (x >= nx) { if (!bd.xcyc) continue; x -= nx; }
+        const int d = x + y * nx;
+        if (d == k || contains(seen, ns, d)) continue;
+        set_at(seen, ns++, d);
+        const int rd = rec[d];
+        if (rd == d) continue;
+        bool hits = false;
+        const int nd = mnrec[d];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) hits |= t < nd && mrec[(size_t)d * 8 + t] == k;
+        const bool gated = hits && (n_is_one ? (h[d] >= htk) : (h[d] > htk));
+        if ((gated || rd == k) && dn < 8) insert_by_priority(dep, pr, dn++, tm.g(x, y), prio16(prio[d]));
+      }
+    }
+    RegionLineT<T> L;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      L.c[t] = fact[t];
+      L.dep[t] = dep[t];
+      L.inp[t] = inp[t];
+    }
+    line[gk] = L;
+    hw[gk] = make_double2(htk, pack_meta(r != k ? tm.g(r % nx, r / nx) : -1, nr > 0));
+    cnt0[gk] = (unsigned char)(nin + (nx_in > 0 ? 1 : 0));
+    xcnt[gk] = nx_in;
+  }
+}
+
+// ---- node operations ----------------------------------------------------------
+// run(g, dep) computes tile-major node g, stores its value and returns its
+// dependents.  `mine` tells whether an index lies in the running CTA's tile:
+// inputs from the tile are read through L1, others from L2.
+
+// a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115)
+struct AccRegionOp {
+  const RegionLine* line;
+  double* val;
+  __device__ int run(int g, int tile, int lr, int (&dep)[8]) const {
+    const LineRegs L(line + g);
+    double x[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      const int d = L.inp(t);
+      x[t] = d < 0 ? 0.0 : ((d >> lr) == tile ? ld_l1(val + d) : ld_l2(val + d));
+    }
+    int nd = 0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      dep[t] = L.dep(t);
+      nd += dep[t] >= 0;
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (t < nd) prefetch_l1(line + dep[t]);
+    double acc = ld_l1(val + g);  // dx*dy*precip(k), stored by the line builder
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (L.inp(t) >= 0) acc = acc + x[t] * L.c[t];
+    st_global(val + g, acc);
+    return nd;
+  }
+};
+
+// x^n and x^(n-1) for the Newton update (as NewtonPow in fsb_flow.cu): for
+// n = 1.5 as x*sqrt(x) and sqrt(x); otherwise x*x^(n-1) with one pow for x > 0.
+struct RegionPow {
+  double n;
+  int half3;
+  __device__ void eval(double x, double& pn, double& pn1) const {
+    if (half3) {
+      const double r = sqrt(x);
+      pn = x * r;
+      pn1 = r;
+    } else if (x > 0.0) {
+      pn1 = pow(x, n - 1.0);
+      pn = x * pn1;
+    } else {
+      pn = pow(x, n);
+      pn1 = pow(x, n - 1.0);
+    }
+  }
+};
+
+// implicit stream power law over the multiple receivers with g == 0
+// (StreamPowerLaw.f90:92-177): hw[g] = (new h, water)
+struct SplRegionOp {
+  const RegionLine* line;
+  double2* hw;
+  RegionPow np;
+  double omega;
+  int n_is_one;
+  int* err;
+  __device__ int run(int g, int tile, int lr, int (&dep)[8]) const {
+    const LineRegs L(line + g);
+    const double2 self = ld_l1(hw + g);
+    int rg;
+    bool has_mrec;
+    unpack_meta(self.y, rg, has_mrec);
+    const double ht = self.x;
+    double hq[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, wr = 0.0;
+    if (rg >= 0) {
+      const double2 rv = (rg >> lr) == tile ? ld_l1(hw + rg) : ld_l2(hw + rg);
+      wr = rv.y;
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const int q = L.inp(t);
+        hq[t] = q < 0 ? 0.0 : ((q >> lr) == tile ? ld_l1(hw + q).x : ld_l2(hw + q).x);
+      }
+    }
+    int nd = 0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      dep[t] = L.dep(t);
+      nd += dep[t] >= 0;
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (t < nd) prefetch_l1(line + dep[t]);
+    double hk = ht, wk = ht;
+    if (rg >= 0) {
+      const double elev = ht;
+      if (elev > wr) {
+        if (has_mrec) {
+          if (n_is_one) {
+            double f = elev, df = 1.0;
+#pragma unroll
+            for (int t = 0; t < 8; ++t)
+              if (L.inp(t) >= 0) {
+                f = f + L.c[t] * hq[t];
+                df = df + L.c[t];
+              }
+            hk = f / df;
+          } else {
+            const double tolp = 1.0e-3;
+            double errp = 2.0 * tolp;
+            int guard = 0;
+            while (errp > tolp) {
+              if (++guard > kNewtonLimit) {
+                atomicExch(err, DEV_NEWTON_LIMIT);
+                break;
+              }
+              double f = hk - elev, df = 1.0;
+#pragma unroll
+              for (int t = 0; t < 8; ++t)
+                if (L.inp(t) >= 0) {
+                  const double x = fmax(0.0, hk - hq[t]);
+                  double pn, pn1;
+                  np.eval(x, pn, pn1);
+                  f = f + L.c[t] * pn;
+                  df = df + L.c[t] * np.n * pn1;
+                }
+              const double hn = hk - f / df;
+              errp = fabs(hn - hk);
+              hk = hk * (1.0 - omega) + hn * omega;
+            }
+          }
+        }
+        if (hk < wr) hk = wr;
+      } else {
+        hk = elev;
+      }
+      wk = fmax(wr, hk);
+    }
+    st_global(hw + g, make_double2(hk, wk));
+    return nd;
+  }
+};
+
+// Mixed precision: the area in FP32 (values, weights, sums)
+struct AccRegionOpF {
+  const RegionLineF* line;
+  float* val;
+  __device__ int run(int g, int tile, int lr, int (&dep)[8]) const {
+    const LineRegsT<float> L(line + g);
+    float x[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      const int d = L.inp(t);
+      x[t] = d < 0 ? 0.0f : ((d >> lr) == tile ? ld_l1f(val + d) : ld_l2f(val + d));
+    }
+    int nd = 0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      dep[t] = L.dep(t);
+      nd += dep[t] >= 0;
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (t < nd) prefetch_l1(line + dep[t]);
+    float acc = ld_l1f(val + g);
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (L.inp(t) >= 0) acc = acc + x[t] * L.c[t];
+    st_globalf(val + g, acc);
+    return nd;
+  }
+};
+
+// Mixed precision: the stream-power solve for the increment d = h - ht in FP32.
+// Elevations, water levels and the h update stay FP64; the distances to the
+// receivers' new elevations, ht(k) - h(q), are taken in FP64 and rounded once.
+// n = 1: d = -sum f*(ht - hq) / (1 + sum f), the closed form of
+// StreamPowerLaw.f90:108-118 rewritten for the increment; otherwise Newton on
+// d (x = max(0, ht - hq + d), :146-162) with the reference's tolerance and
+// relaxation.
+struct SplRegionOpM {
+  const RegionLineF* line;
+  double2* hw;
+  float n;
+  int half3;
+  float omega;
+  int n_is_one;
+  int* err;
+  __device__ int run(int g, int tile, int lr, int (&dep)[8]) const {
+    const LineRegsT<float> L(line + g);
+    const double2 self = ld_l1(hw + g);
+    int rg;
+    bool has_mrec;
+    unpack_meta(self.y, rg, has_mrec);
+    const double ht = self.x;
+    double hq[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, wr = 0.0;
+    if (rg >= 0) {
+      const double2 rv = (rg >> lr) == tile ? ld_l1(hw + rg) : ld_l2(hw + rg);
+      wr = rv.y;
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const int q = L.inp(t);
+        hq[t] = q < 0 ? 0.0 : ((q >> lr) == tile ? ld_l1(hw + q).x : ld_l2(hw + q).x);
+      }
+    }
+    int nd = 0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      dep[t] = L.dep(t);
+      nd += dep[t] >= 0;
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (t < nd) prefetch_l1(line + dep[t]);
+    double hk = ht, wk = ht;
+    if (rg >= 0) {
+      if (ht > wr) {
+        if (has_mrec) {
+          float dist[8];
+#pragma unroll
+          for (int t = 0; t < 8; ++t) dist[t] = L.inp(t) >= 0 ? (float)(ht - hq[t]) : 0.0f;
+          float d = 0.0f;
+          if (n_is_one) {
+            float num = 0.0f, den = 1.0f;
+#pragma unroll
+            for (int t = 0; t < 8; ++t)
+              if (L.inp(t) >= 0) {
+                num = num + L.c[t] * dist[t];
+                den = den + L.c[t];
+              }
+            d = -num / den;
+          } else {
+            const float tolp = 1.0e-3f;
+            float errp = 2.0f * tolp;
+            int guard = 0;
+            while (errp > tolp) {
+              if (++guard > kNewtonLimit) {
+                atomicExch(err, DEV_NEWTON_LIMIT);
+                break;
+              }
+              float f = d, df = 1.0f;
+#pragma unroll
+              for (int t = 0; t < 8; ++t)
+                if (L.inp(t) >= 0) {
+                  const float x = fmaxf(0.0f, dist[t] + d);
+                  float pn, pn1;
+                  if (half3) {
+                    pn1 = sqrtf(x);
+                    pn = x * pn1;
+                  } else if (x > 0.0f) {
+                    pn1 = powf(x, n - 1.0f);
+                    pn = x * pn1;
+                  } else {
+                    pn = powf(x, n);
+                    pn1 = powf(x, n - 1.0f);
+                  }
+                  f = f + L.c[t] * pn;
+                  df = df + L.c[t] * n * pn1;
+                }
+              const float dn = d - f / df;
+              errp = fabsf(dn - d);
+              d = d * (1.0f - omega) + dn * omega;
+            }
+          }
+          hk = ht + (double)d;
+        }
+        if (hk < wr) hk = wr;
+      } else {
+        hk = ht;
+      }
+      wk = fmax(wr, hk);
+    }
+    st_global(hw + g, make_double2(hk, wk));
+    return nd;
+  }
+};
+
+// ---- the sweep kernel ------------------------------------------------------------
+// One CTA per tile.  Shared memory: the tile's counters (bytes, four per word)
+// and its ready queue (local indices, filled once each, never wrapped).
+// Warp 0's lane 0 polls the tile's inbox; the other warps' first LANES lanes
+// take nodes: a lane that finishes a node continues with the first of its
+// dependents it made ready (they come largest priority first) and queues the
+// others.  A CTA ends when all nodes of its tile are done; every wait is
+// bounded by a 4 s limit, after which the sweep reports DEV_SPIN_LIMIT.
+template <class Op, int LANES>
+__global__ void __launch_bounds__(kRegionThreads, 2)
+    k_region_sweep(Op op, TileMap tm, const unsigned char* __restrict__ cnt0, int* xcnt, int* inbox, int icap,
+                   unsigned* itail, int* err) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lr = tm.lr();
+  const int R = 1 << lr;
+  unsigned* cnt = reinterpret_cast<unsigned*>(smem);                  // R bytes
+  unsigned short* q = reinterpret_cast<unsigned short*>(smem + R);    // R entries
+  __shared__ int qhead, qtail, ndone, stop;
+  const int tile = blockIdx.x;
+  const int gbase = tile << lr;
+  const int tx = tile % tm.ntx, ty = tile / tm.ntx;
+  const int count = min(1 << tm.ltx, tm.nx - (tx << tm.ltx)) * min(1 << tm.lty, tm.ny - (ty << tm.lty));
+  const unsigned long long t0 = global_ns();
+
+  if (threadIdx.x == 0) {
+    qhead = 0;
+    qtail = 0;
+    ndone = 0;
+    stop = 0;
+  }
+  for (int w = threadIdx.x; w < R / 4; w += blockDim.x)
+    cnt[w] = reinterpret_cast<const unsigned*>(cnt0 + gbase)[w];
+  for (int l = threadIdx.x; l < R; l += blockDim.x) q[l] = kQEmpty;
+  __syncthreads();
+  for (int l = threadIdx.x; l < R; l += blockDim.x)
+    if (cnt0[gbase + l] == 0) q[atomicAdd(&qtail, 1)] = (unsigned short)l;
+  __syncthreads();
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto push = [&](int l) {
+    __threadfence_block();
+    const int p = atomicAdd(&qtail, 1);
+    if (p < R) *(volatile unsigned short*)&q[p] = (unsigned short)l;
+    else atomicExch(err, DEV_OVERFLOW);
+  };
+  // decrements node l's counter; true when l became ready
+  auto release = [&](int l) {
+    const unsigned sh = 8u * (unsigned)(l & 3);
+    const unsigned old = atomicSub(&cnt[l >> 2], 1u << sh);
+    return ((old >> sh) & 0xffu) == 1u;
+  };
+  // periodic checks of the time limit and of failures elsewhere
+  auto should_stop = [&](int& ticks) {
+    if (*(volatile int*)&stop) return true;
+    if (++ticks < 256) return false;
+    ticks = 0;
+    if (*(volatile int*)err != 0) {
+      *(volatile int*)&stop = 1;
+      return true;
+    }
+    if (global_ns() - t0 > kRegionTimeLimitNs) {
+      atomicExch(err, DEV_SPIN_LIMIT);
+      *(volatile int*)&stop = 1;
+      return true;
+    }
+    return false;
+  };
+
+  if (warp == 0) {
+    if (lane != 0) return;
+    int ih = 0, ticks = 0;
+    int* box = inbox + (size_t)tile * icap;
+    for (;;) {
+      if (ih < icap) {
+        const int d = ld_relaxed_gpu(&box[ih]);
+        if (d >= 0) {
+          ++ih;
+          __threadfence();  // acquire: the cross-tile producers' values
+          if (release(d - gbase)) push(d - gbase);
+          continue;
+        }
+      }
+      if (*(volatile int*)&ndone >= count) return;
+      if (should_stop(ticks)) return;
+      __nanosleep(64);
+    }
+  }
+  if (lane >= LANES) return;
+  int cur = -1, slot = -1, ticks = 0;
+  for (;;) {
+    if (cur < 0) {
+      if (slot < 0) slot = atomicAdd(&qhead, 1);
+      if (slot < R) {
+        const unsigned short v = *(volatile unsigned short*)&q[slot];
+        if (v != kQEmpty) {
+          cur = v;
+          slot = -1;
+          __threadfence_block();  // acquire: the producers' values
+        }
+      }
+      if (cur < 0) {
+        if (*(volatile int*)&ndone >= count) return;
+        if (should_stop(ticks)) return;
+        __nanosleep(32);
+        continue;
+      }
+    }
+    int dep[8];
+    const int nd = op.run(gbase + cur, tile, lr, dep);
+    __threadfence_block();  // release: this node's value before its dependents' counters
+    int nxt = -1;
+    bool cross_fenced = false;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      if (t >= nd) break;
+      const int d = dep[t];
+      if ((d >> lr) == tile) {
+        if (release(d - gbase)) {
+          if (nxt < 0) nxt = d - gbase;
+          else push(d - gbase);
+        }
+      } else {
+        if (!cross_fenced) {
+          __threadfence();  // release at GPU scope before a cross-tile counter
+          cross_fenced = true;
+        }
+        if (atomicSub(&xcnt[d], 1) == 1) {
+          __threadfence();
+          const int owner = d >> lr;
+          const unsigned p = atomicAdd(&itail[owner], 1u);
+          if (p < (unsigned)icap) st_relaxed_gpu_int(&inbox[(size_t)owner * icap + p], d);
+          else atomicExch(err, DEV_OVERFLOW);
+        }
+      }
+    }
+    atomicAdd(&ndone, 1);
+    if (nxt >= 0) __threadfence_block();  // acquire for the continuation
+    cur = nxt;
+  }
+}
+
+// natural-order copies of the sweeps' results
+template <class T>
+__global__ void k_untile_area(int nx, int ny, TileMap tm, const T* __restrict__ val, double* __restrict__ a) {
+  const int nn = nx * ny;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x)
+    a[k] = (double)val[tm.g(k % nx, k / nx)];
+}
+
+// StreamPowerLaw.f90:380-393 with g == 0: b=min(h,b), etot=etot+ht-h,
+// erate=(ht-h)/dt, Sedflux=ht-h, from the tile-major (h, water) pairs
+__global__ void k_spl_finish_t(int nx, int ny, TileMap tm, double dt, const double2* __restrict__ hw,
+                               double* __restrict__ h, double* __restrict__ b, double* __restrict__ etot,
+                               double* __restrict__ erate, double* __restrict__ sedflux) {
+  const int nn = nx * ny;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const double ht = h[k], hn = hw[tm.g(k % nx, k / nx)].x;
+    b[k] = fmin(hn, b[k]);
+    etot[k] = etot[k] + ht - hn;
+    erate[k] = (ht - hn) / dt;
+    sedflux[k] = ht - hn;
+    h[k] = hn;
+  }
+}
+
+#ifndef FSB_REGION_LANES_ACC
+#define FSB_REGION_LANES_ACC 4
+#endif
+#ifndef FSB_REGION_LANES_SPL
+#define FSB_REGION_LANES_SPL 2
+#endif
+
+size_t region_smem(const TileMap& tm) { return (size_t)3 << tm.lr(); }
+
+// whether every tile's CTA of this sweep kernel can be co-resident
+template <class Op, int LANES>
+bool region_fits(const TileMap& tm) {
+  const size_t smem = region_smem(tm);
+  auto kern = k_region_sweep<Op, LANES>;
+  // the permitted maximum covers every plan (3 bytes per node, 32768 nodes per
+  // tile), so instances with different plans never undo each other's setting
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * 32768) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  int dev = 0, sms = 0, per_sm = 0, coop = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kRegionThreads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return per_sm * sms >= tm.tiles();
+}
+
+bool region_usable(Ctx& c) {
+  if (!c.region_enabled || c.tmap.ntx == 0) return false;
+  if (c.region_state == 0)
+    c.region_state = (region_fits<AccRegionOp, FSB_REGION_LANES_ACC>(c.tmap) &&
+                      region_fits<SplRegionOp, FSB_REGION_LANES_SPL>(c.tmap) &&
+                      region_fits<AccRegionOpF, FSB_REGION_LANES_ACC>(c.tmap) &&
+                      region_fits<SplRegionOpM, FSB_REGION_LANES_SPL>(c.tmap))
+                         ? 1
+                         : -1;
+  return c.region_state > 0;
+}
+
+template <class Op, int LANES>
+bool launch_region(Ctx& c, Op op) {
+  const TileMap& tm = c.tmap;
+  const int tiles = tm.tiles();
+  const size_t smem = region_smem(tm);
+  auto kern = k_region_sweep<Op, LANES>;
+  cudaMemsetAsync(c.rl_inbox, 0xff, sizeof(int) * (size_t)tiles * c.rl_icap, c.stream);
+  cudaMemsetAsync(c.rl_itail, 0, sizeof(unsigned) * (size_t)tiles, c.stream);
+  const unsigned char* cnt0 = c.rl_cnt0;
+  int* xcnt = c.rl_xcnt;
+  int* inbox = c.rl_inbox;
+  int icap = c.rl_icap;
+  unsigned* itail = c.rl_itail;
+  int* err = c.d_err;
+  TileMap tmv = tm;
+  void* args[] = {&op, &tmv, &cnt0, &xcnt, &inbox, &icap, &itail, &err};
+  const cudaError_t e =
+      cudaLaunchCooperativeKernel((const void*)kern, dim3(tiles), dim3(kRegionThreads), args, smem, c.stream);
+  c.count_launch();
+  if (e != cudaSuccess) {  // e.g. the GPU is shared and the tiles no longer fit: queue engine
+    cudaGetLastError();
+    c.region_state = -1;
+    return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+// Tile plan: the smallest tiles of 2^a x 2^b nodes (32 x 32 at least, 32768
+// nodes at most, width >= height) whose count fits the co-resident CTAs
+// (two per SM); none fits -> the queue engine runs.
+TileMap plan_tiles(int nx, int ny, int sms) {
+  TileMap tm{};
+  tm.nx = nx;
+  tm.ny = ny;
+  const int max_ctas = 2 * std::max(1, sms);
+  static const int cand[][2] = {{5, 5}, {6, 5}, {6, 6}, {7, 6}, {7, 7}, {8, 7}};
+  for (const auto& cd : cand) {
+    const int ntx = (nx + (1 << cd[0]) - 1) >> cd[0], nty = (ny + (1 << cd[1]) - 1) >> cd[1];
+    if (ntx * nty <= max_ctas) {
+      tm.ltx = cd[0];
+      tm.lty = cd[1];
+      tm.ntx = ntx;
+      tm.nty = nty;
+      return tm;
+    }
+  }
+  return tm;  // ntx == 0: no plan
+}
+
+bool region_accumulate(Ctx& c) {
+  if (!region_usable(c)) return false;
+  const TileMap& tm = c.tmap;
+  cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)tm.padded(), c.stream);  // padding slots never run
+  if (c.mixed) {
+    RegionLineF* line = static_cast<RegionLineF*>(c.rl_line);
+    float* val = reinterpret_cast<float*>(c.rl_val);
+    k_acc_lines_t<float><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, tm, c.dx * c.dy, c.mrec, c.mnrec, c.mwrec,
+                                                                c.precip, c.size, line, val, c.rl_cnt0, c.rl_xcnt,
+                                                                c.d_err);
+    c.count_launch();
+    if (!launch_region<AccRegionOpF, FSB_REGION_LANES_ACC>(c, AccRegionOpF{line, val})) return false;
+    k_untile_area<float><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, val, c.a);
+  } else {
+    RegionLine* line = static_cast<RegionLine*>(c.rl_line);
+    k_acc_lines_t<double><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, tm, c.dx * c.dy, c.mrec, c.mnrec, c.mwrec,
+                                                                 c.precip, c.size, line, c.rl_val, c.rl_cnt0,
+                                                                 c.rl_xcnt, c.d_err);
+    c.count_launch();
+    if (!launch_region<AccRegionOp, FSB_REGION_LANES_ACC>(c, AccRegionOp{line, c.rl_val})) return false;
+    k_untile_area<double><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, c.rl_val, c.a);
+  }
+  c.count_launch();
+  return true;
+}
+
+bool region_stream_power(Ctx& c) {
+  if (!region_usable(c)) return false;
+  const TileMap& tm = c.tmap;
+  const int n1 = fabs(c.n - 1.0) < DBL_MIN;
+  double2* hw = reinterpret_cast<double2*>(c.rl_val);
+  cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)tm.padded(), c.stream);
+  if (c.mixed) {
+    RegionLineF* line = static_cast<RegionLineF*>(c.rl_line);
+    k_spl_lines_t<float><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, tm, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec,
+                                                                c.mnrec, c.mwrec, c.mlrec, c.h, c.b, c.kf, c.a,
+                                                                c.size, line, hw, c.rl_cnt0, c.rl_xcnt, c.d_err);
+    c.count_launch();
+    SplRegionOpM op{line, hw, (float)c.n, c.n == 1.5, (float)(0.875 / c.n), n1, c.d_err};
+    if (!launch_region<SplRegionOpM, FSB_REGION_LANES_SPL>(c, op)) return false;
+  } else {
+    RegionLine* line = static_cast<RegionLine*>(c.rl_line);
+    k_spl_lines_t<double><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, tm, n1, c.kfsed, c.dt, c.m, c.n, c.rec,
+                                                                 c.mrec, c.mnrec, c.mwrec, c.mlrec, c.h, c.b, c.kf,
+                                                                 c.a, c.size, line, hw, c.rl_cnt0, c.rl_xcnt,
+                                                                 c.d_err);
+    c.count_launch();
+    SplRegionOp op{line, hw, RegionPow{c.n, c.n == 1.5}, 0.875 / c.n, n1, c.d_err};
+    if (!launch_region<SplRegionOp, FSB_REGION_LANES_SPL>(c, op)) return false;
+  }
+  k_spl_finish_t<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, c.dt, hw, c.h, c.b, c.etot, c.erate,
+                                                        c.sedflux);
+  c.count_launch();
+  return true;
+}
+
+}  // namespace fsb

@@ -54,6 +54,10 @@ FIELDS = {"h": 0, "basement": 1, "total_erosion": 2, "drainage_area": 3, "erosio
 INT_FIELDS = {"rec": 0, "ndon": 1, "stack": 2, "mnrec": 3, "mstack": 4, "basins": 5,
               "rec_pre": 6, "stack_pre": 7}
 SLOT_FIELDS = {"don": 0, "mrec": 1, "mwrec": 2, "mlrec": 3}
+# "fp64": every float in FP64, as the reference.  "mixed": FP64 state, h
+# update and residuals, exact routing; FP32 weights, area, Newton iterations
+# and tridiagonal solves (include/fastscape_b200.h, fsb_set_precision).
+PRECISIONS = {"fp64": 0, "mixed": 1}
 
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -78,6 +82,8 @@ _sig("fsb_set_xl_yl", _vp, _d, _d)
 _sig("fsb_set_dt", _vp, _d)
 _sig("fsb_set_erosional_parameters", _vp, _vp, _d, _d, _d, _vp, _d, _d, _d, _d, _i)
 _sig("fsb_set_bc", _vp, _i)
+_sig("fsb_set_precision", _vp, _i)
+_sig("fsb_get_precision", _vp, ctypes.POINTER(_i))
 _sig("fsb_set_v", _vp, _vp, _vp, _i)
 for _n in ("fsb_set_u", "fsb_init_h", "fsb_set_h", "fsb_set_basement", "fsb_set_precip"):
     _sig(_n, _vp, _vp, _i)
@@ -228,6 +234,15 @@ class FastScape:
                                                  pkd, float(kdsed), float(g1), float(g2),
                                                  float(p), wkf))
         self._sync_if_device(wkf)
+
+    def set_precision(self, precision: str) -> None:
+        """"fp64" (default, the reference's arithmetic) or "mixed"."""
+        _check(_lib.fsb_set_precision(self._h, PRECISIONS[precision]))
+
+    def get_precision(self) -> str:
+        v = _i()
+        _check(_lib.fsb_get_precision(self._h, ctypes.byref(v)))
+        return {b: a for a, b in PRECISIONS.items()}[v.value]
 
     def set_bc(self, bc: int) -> None:
         _check(_lib.fsb_set_bc(self._h, int(bc)))
@@ -404,7 +419,7 @@ class _JobRow(ctypes.Structure):
                 ("kfsed", _d), ("m", _d), ("n", _d), ("kdsed", _d), ("g1", _d), ("g2", _d),
                 ("p", _d),
                 ("kf", _vp), ("kd", _vp), ("u", _vp), ("h0", _vp), ("precip", _vp),
-                ("h_out", _vp), ("a_out", _vp), ("etot_out", _vp)]
+                ("h_out", _vp), ("a_out", _vp), ("etot_out", _vp), ("precision", _i)]
 
 
 def _f64(a, nn, name):
@@ -425,7 +440,7 @@ class Job:
 
     def __init__(self, nx, ny, xl, yl, dt, h0, kf, kd, u, m, n, p, bc=1111, nsteps=1,
                  kfsed=-1.0, kdsed=-1.0, g1=0.0, g2=0.0, precip=None, want_area=False,
-                 want_etot=False):
+                 want_etot=False, precision="fp64"):
         nn = int(nx) * int(ny)
         self.nx, self.ny, self.nsteps, self.bc = int(nx), int(ny), int(nsteps), int(bc)
         self.xl, self.yl, self.dt = float(xl), float(yl), float(dt)
@@ -439,6 +454,7 @@ class Job:
         self.h = np.empty(nn)
         self.a = np.empty(nn) if want_area else None
         self.etot = np.empty(nn) if want_etot else None
+        self.precision = PRECISIONS[precision]
         self.t_submit = self.t_start = self.t_end = float("nan")
         self.status = None
 
@@ -451,7 +467,7 @@ class Job:
         return _JobRow(self.nx, self.ny, self.bc, self.nsteps, self.xl, self.yl, self.dt,
                        self.kfsed, self.m, self.n, self.kdsed, self.g1, self.g2, self.p,
                        ptr(self.kf), ptr(self.kd), ptr(self.u), ptr(self.h0), ptr(self.precip),
-                       ptr(self.h), ptr(self.a), ptr(self.etot))
+                       ptr(self.h), ptr(self.a), ptr(self.etot), self.precision)
 
 
 class Batch:

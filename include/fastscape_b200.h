@@ -98,6 +98,16 @@ int fsb_set_u(fsb_ctx* c, const double* u, int where);
 /* FastScape_Set_V (api:634 -> ctx:616-632): advection velocities vx, vy;
    switches advection on (Advect.f90, run first in each step) */
 int fsb_set_v(fsb_ctx* c, const double* vx, const double* vy, int where);
+/* Arithmetic of the step (no counterpart in the reference, which is FP64
+   throughout).  FSB_PREC_FP64 (default): every float in FP64, as the
+   reference.  FSB_PREC_MIXED: elevation state, the per-step h update and
+   the ADI residuals stay FP64, integer routing stays exact; the multiple-flow
+   slopes and weights, the drainage area, the stream-power erosion factors and
+   Newton iterations (solved for the increment of h) and the tridiagonal
+   solves (for the increment of the surface) run in FP32. */
+enum { FSB_PREC_FP64 = 0, FSB_PREC_MIXED = 1 };
+int fsb_set_precision(fsb_ctx* c, int precision);
+int fsb_get_precision(fsb_ctx* c, int* precision);
 /* FastScape_Init_H (api:267 -> ctx:339-350): h and basement b */
 int fsb_init_h(fsb_ctx* c, const double* h, int where);
 /* FastScape_Set_H (api:664 -> ctx:636-644) */
@@ -221,6 +231,7 @@ typedef struct fsb_job {
   double* h_out;         /* [nx*ny] elevation after nsteps, or NULL    api:299 */
   double* a_out;         /* [nx*ny] drainage area, or NULL             api:347 */
   double* etot_out;      /* [nx*ny] total erosion, or NULL             api:331 */
+  int precision;         /* FSB_PREC_FP64 or FSB_PREC_MIXED (fsb_set_precision) */
 } fsb_job;
 /* `workers` threads (1..256) on CUDA device `device`; `mem_budget` bytes of
    device memory for job workspaces (0: 90% of the memory free now). */

@@ -16,7 +16,7 @@ max |x_gpu - x_oracle| / max(|x_oracle|, 1) is taken per field.
 Stated bounds (relative L-infinity of h; other fields in BOUNDS below):
 single flow 1e-10 after 200 steps, uniform multiple flow 1e-9 after 200 steps,
 the 2049^2 multiple-flow grid 1e-8 after 20, 1e-7 after 100 and 1e-6 after
-500 steps.  Per step the multiple-flow floats differ by about 1e-12..1e-9
+500 steps; its mixed-precision form 1e-6 at every checkpoint.  Per step the multiple-flow floats differ by about 1e-12..1e-9
 (summation order of the area); the errors grow slowly along the run.
 Set FSB_REPORT_DIR to also write the measured errors to long_run_errors.json.
 """
@@ -46,6 +46,10 @@ BOUNDS = {
     ("mfd_2049", 20): (1e-8, 1e-5),
     ("mfd_2049", 100): (1e-7, 1e-4),
     ("mfd_2049", 500): (1e-6, 1e-3),
+    # the mixed-precision form against the same FP64 oracle checkpoints
+    ("mfd_2049_mixed", 20): (1e-6, 1e-3),
+    ("mfd_2049_mixed", 100): (1e-6, 1e-3),
+    ("mfd_2049_mixed", 500): (1e-6, 1e-3),
 }
 _REPORT = {}
 
@@ -81,7 +85,7 @@ def test_config1_single_flow_200_steps():
     assert np.array_equal(g.copy_int("stack"), O.copy_int("stack"))
 
 
-def _run_against_fixture(case, wl):
+def _run_against_fixture(case, wl, precision="fp64"):
     import fastscapelib_fortran as fs
     fx = FIX[case]
     assert (wl.nx, wl.ny) == (fx["nx"], fx["ny"])
@@ -90,6 +94,7 @@ def _run_against_fixture(case, wl):
     g = fs.FastScape()
     g.set_nx_ny(wl.nx, wl.ny)
     g.setup()
+    g.set_precision(precision)
     g.set_xl_yl(wl.xl, wl.yl)
     g.set_dt(wl.dt)
     g.init_h(wl.h0)
@@ -107,7 +112,7 @@ def _run_against_fixture(case, wl):
             g.copy(f, out)
             r = np.asarray(ref["sample"][f])
             errs[f] = float(np.max(np.abs(out[idx] - r) / np.maximum(np.abs(r), 1.0)))
-        _check(case, cp, errs)
+        _check(case if precision == "fp64" else f"{case}_{precision}", cp, errs)
     g.destroy()
 
 
@@ -119,3 +124,10 @@ def test_config1_uniform_multiple_flow_200_steps():
 @pytest.mark.skipif("mfd_2049" not in FIX, reason="fixture missing")
 def test_config2_multiple_flow_500_steps():
     _run_against_fixture("mfd_2049", W.mfd(2049, nsteps=500))
+
+
+@pytest.mark.skipif("mfd_2049" not in FIX, reason="fixture missing")
+def test_config2_mixed_precision_500_steps():
+    """The mixed-precision form on configuration 2 for its full 500 steps:
+    final h within 1e-6 relative L-infinity of the FP64 oracle."""
+    _run_against_fixture("mfd_2049", W.mfd(2049, nsteps=500), precision="mixed")
