@@ -249,7 +249,10 @@ int check_device_error(fsb::Ctx& c) {
 
 enum { ST_UPLIFT, ST_RECEIVERS, ST_STACK, ST_LOCMIN, ST_FILL, ST_MFD, ST_ACCUM, ST_SPL, ST_DIFFUSION, ST_ADVECT };
 
-void stage_begin(fsb::Ctx& c, int s) {
+}  // namespace
+
+namespace fsb {
+void stage_begin(Ctx& c, int s) {
   if (!c.profile) return;
   if (!c.ev_begin[s]) {
     cudaEventCreate(&c.ev_begin[s]);
@@ -258,11 +261,16 @@ void stage_begin(fsb::Ctx& c, int s) {
   cudaEventRecord(c.ev_begin[s], c.stream);
 }
 
-void stage_end(fsb::Ctx& c, int s) {
+void stage_end(Ctx& c, int s) {
   if (!c.profile) return;
   cudaEventRecord(c.ev_end[s], c.stream);
   c.ev_pending[s] = true;
 }
+}  // namespace fsb
+
+namespace {
+using fsb::stage_begin;
+using fsb::stage_end;
 
 void collect_stage_times(fsb::Ctx& c) {
   for (int s = 0; s < fsb::Ctx::kStages; ++s) {
@@ -756,7 +764,7 @@ int fsb_debug(fsb_ctx* h) {
   std::printf(" Number of Gauss-Siedel iterations (SPL) %d\n", c.ngs);
   std::printf(" Timing (device milliseconds, accumulated while profiling is on):\n");
   static const char* names[] = {"Uplift", "Receivers", "Stack", "LocalMinima", "LakeFill", "MFDReceivers",
-                                "DrainageArea", "SPL", "Diffusion", "Advection"};
+                                "DrainageArea", "SPL", "Diffusion", "Advection"};  // stages; kernel timers follow
   for (int s = 0; s < fsb::Ctx::kStages && s < 10; ++s)
     if (c.stage_calls[s]) std::printf(" %s: %.6g\n", names[s], c.stage_ms[s]);
   std::fflush(stdout);

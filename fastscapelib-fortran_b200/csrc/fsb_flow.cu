@@ -1328,12 +1328,16 @@ static void diffusion_mixed(Ctx& c) {
   k_diff_kdint<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, c.kdsed, c.kd, c.h, c.b, K);
   dim3 gx((nx + 127) / 128, ny - 2);
   k_diff_xcoef<float><<<gx, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, c.h, A, B, C, F);
+  stage_begin(c, KT_THOMAS_ROWS);
   k_thomas<float><<<(ny - 2 + 31) / 32, 32, 0, c.stream>>>(nx, ny, 1, ny - 1, A, B, C, F, G, c.d_err);
+  stage_end(c, KT_THOMAS_ROWS);
   dim3 g2((nx + 31) / 32, (ny + 31) / 32);
   k_diff_xgather<float><<<g2, dim3(32, 8), 0, c.stream>>>(c.bd, F, c.h, Z);
   dim3 gy((nx + 127) / 128, ny);
   k_diff_ycoef<float><<<gy, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, Z, A, B, C, F);
+  stage_begin(c, KT_THOMAS_COLS);
   k_thomas<float><<<(nx - 2 + 31) / 32, 32, 0, c.stream>>>(ny, nx, 1, nx - 1, A, B, C, F, G, c.d_err);
+  stage_end(c, KT_THOMAS_COLS);
   k_diff_finish_m<<<grid1d(nn), kBlock, 0, c.stream>>>(c.bd, c.dt, F, Z, c.h, c.b, c.etot, c.erate);
   c.count_launch(7);
 }
@@ -1352,7 +1356,9 @@ void diffusion(Ctx& c) {
     dim3 g((nx + 127) / 128, ny - 2);
     k_diff_xcoef<double><<<g, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, c.h, A, B, C, F);
     // systems are rows j=1..ny-2 with element i at [i*ny + j]
+    stage_begin(c, KT_THOMAS_ROWS);
     k_thomas<double><<<(ny - 2 + 31) / 32, 32, 0, c.stream>>>(nx, ny, 1, ny - 1, A, B, C, F, G, c.d_err);
+    stage_end(c, KT_THOMAS_ROWS);
     dim3 g2((nx + 31) / 32, (ny + 31) / 32);
     k_diff_xgather<double><<<g2, dim3(32, 8), 0, c.stream>>>(c.bd, F, c.h, Z);
     c.count_launch(3);
@@ -1360,7 +1366,9 @@ void diffusion(Ctx& c) {
   {
     dim3 g((nx + 127) / 128, ny);
     k_diff_ycoef<double><<<g, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, Z, A, B, C, F);
+    stage_begin(c, KT_THOMAS_COLS);
     k_thomas<double><<<(nx - 2 + 31) / 32, 32, 0, c.stream>>>(ny, nx, 1, nx - 1, A, B, C, F, G, c.d_err);
+    stage_end(c, KT_THOMAS_COLS);
     c.count_launch(2);
   }
   k_diff_finish<<<grid1d(nn), kBlock, 0, c.stream>>>(c.bd, c.dt, F, c.h, c.b, c.etot, c.erate);

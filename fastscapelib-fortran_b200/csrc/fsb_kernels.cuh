@@ -161,7 +161,10 @@ struct Ctx {
   int nbasins = 0, basin0 = 0, nconn = 0, tree_size = 0, nlocmin_before = 0, nlocmin_after = 0;
 
   // per-stage device timing (CUDA events on the instance's stream)
-  static constexpr int kStages = 10;  // uplift receivers stack locmin fill mfd accum spl diffusion advection
+  // stages: uplift receivers stack locmin fill mfd accum spl diffusion advection;
+  // then single kernels inside them: the area sweep, the stream-power sweep,
+  // the row and the column tridiagonal solves of the diffusion
+  static constexpr int kStages = 14;
   bool profile = false;
   cudaEvent_t ev_begin[kStages] = {}, ev_end[kStages] = {};
   bool ev_pending[kStages] = {};
@@ -170,6 +173,11 @@ struct Ctx {
 
   std::string err;
 };
+
+// per-stage / per-kernel CUDA events while profiling is on (fsb_api.cu)
+enum { KT_AREA_SWEEP = 10, KT_SPL_SWEEP = 11, KT_THOMAS_ROWS = 12, KT_THOMAS_COLS = 13 };
+void stage_begin(Ctx& c, int s);
+void stage_end(Ctx& c, int s);
 
 // sets the message fsb_last_error() returns; returns 1 (fsb_api.cu)
 int report_error(const std::string& msg);

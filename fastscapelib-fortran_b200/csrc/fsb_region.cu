@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <type_traits>
 
 #include "fsb_kernels.cuh"
 
@@ -871,8 +872,12 @@ bool launch_region(Ctx& c, Op op) {
   int* err = c.d_err;
   TileMap tmv = tm;
   void* args[] = {&op, &tmv, &cnt0, &xcnt, &inbox, &icap, &itail, &err};
+  const int timer = std::is_same<Op, AccRegionOp>::value || std::is_same<Op, AccRegionOpF>::value ? KT_AREA_SWEEP
+                                                                                                  : KT_SPL_SWEEP;
+  stage_begin(c, timer);
   const cudaError_t e =
       cudaLaunchCooperativeKernel((const void*)kern, dim3(tiles), dim3(kRegionThreads), args, smem, c.stream);
+  stage_end(c, timer);
   c.count_launch();
   if (e != cudaSuccess) {  // e.g. the GPU is shared and the tiles no longer fit: queue engine
     cudaGetLastError();

@@ -121,7 +121,9 @@ _sig("fsb_batch_memory", _vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ct
 _sig("fsb_batch_destroy", _vp)
 
 STAGES = ("uplift", "receivers", "stack", "local_minima", "lake_fill", "mfd_receivers",
-          "drainage_area", "stream_power", "diffusion", "advection")
+          "drainage_area", "stream_power", "diffusion", "advection",
+          # single kernels inside the stages above
+          "k_area_sweep", "k_spl_sweep", "k_thomas_rows", "k_thomas_cols")
 
 
 def _check(rc: int) -> None:

@@ -181,8 +181,11 @@ long long fsb_launch_count(fsb_ctx* c);
    counterpart of the reference's cpu_time accumulators (api:209-257,
    ctx:27).  Stages: 0 uplift, 1 receivers, 2 stack, 3 LocalMinima, 4 lake
    fill, 5 multiple-flow receivers, 6 drainage area, 7 stream power law,
-   8 diffusion, 9 advection.  fsb_stage_times returns accumulated milliseconds and call
-   counts for the first n stages and optionally resets them. */
+   8 diffusion, 9 advection; then single kernels inside them: 10 the
+   multiple-flow area sweep, 11 the multiple-flow stream-power sweep, 12 and
+   13 the row and column tridiagonal solves of the diffusion.
+   fsb_stage_times returns accumulated milliseconds and call counts for the
+   first n of these and optionally resets them. */
 int fsb_set_profile(fsb_ctx* c, int on);
 int fsb_stage_times(fsb_ctx* c, double* ms, long long* calls, int n, int reset);
 

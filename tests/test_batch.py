@@ -9,7 +9,10 @@ Checked here:
     three free-running steps (1e-12 per step, see the parity tests);
   * admission by device memory: with a budget that holds one job at a time the
     jobs still all complete, correctly; a job larger than the budget is refused;
-  * a failing job reports its error without disturbing the others.
+  * a failing job reports its error without disturbing the others;
+  * continuous batching: a job submitted while others are on the GPU (the
+    served form's admission) gives the same bits as alone, in FP64 and in the
+    mixed-precision form.
 """
 import numpy as np
 import pytest
@@ -27,11 +30,12 @@ def mix():
             W.plain_d8(47, 31, seed=6, nsteps=5, p=-2.0)]
 
 
-def alone(wl):
+def alone(wl, precision="fp64"):
     import fastscapelib_fortran as fs
     g = fs.FastScape()
     g.set_nx_ny(wl.nx, wl.ny)
     g.setup()
+    g.set_precision(precision)
     g.set_xl_yl(wl.xl, wl.yl)
     g.set_dt(wl.dt)
     g.init_h(wl.h0.copy())
@@ -109,3 +113,28 @@ def test_failing_job_is_isolated():
         j2 = b.wait(ids[2])
     ref = alone(good)[0]
     assert np.array_equal(j0.h, ref) and np.array_equal(j2.h, ref)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_submitted_while_others_run(precision):
+    """Requests that arrive while others are running are admitted and overlap
+    with them on the device; each result equals its solo run bit for bit."""
+    import time
+
+    import fastscapelib_fortran as fs
+    long_jobs = [W.mfd(257, 257, seed=20 + k, nsteps=30) for k in range(3)]
+    late = [W.mfd(129, 121, seed=30, nsteps=6), W.plain_d8(97, 89, seed=31, nsteps=6)]
+    ref = [alone(w, precision)[0] for w in late]
+    with fs.Batch(workers=4) as b:
+        first = [b.submit(w.job(precision=precision)) for w in long_jobs]
+        t0 = time.perf_counter()
+        while b.memory()["running"] == 0 and time.perf_counter() - t0 < 60:
+            time.sleep(0.001)
+        assert b.memory()["running"] > 0
+        ids = [b.submit(w.job(precision=precision)) for w in late]
+        done_late = [b.wait(i) for i in ids]
+        done_first = [b.wait(i) for i in first]
+    # the late jobs started while a long job was still running
+    assert min(j.t_start for j in done_late) < max(j.t_end for j in done_first)
+    for j, r in zip(done_late, ref):
+        assert np.array_equal(j.h, r)
