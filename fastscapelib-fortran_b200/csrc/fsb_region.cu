@@ -374,38 +374,43 @@ __global__ void k_spl_lines_t(Bounds bd, TileMap tm, int n_is_one, double kfsed,
   }
 }
 
-// ---- node operations ----------------------------------------------------------
-// run(g, dep) computes tile-major node g, stores its value and returns its
-// dependents.  `mine` tells whether an index lies in the running CTA's tile:
-// inputs from the tile are read through L1, others from L2.
+// ---- node operations: one warp per node ------------------------------------------
+// A node is computed by a whole warp.  Lane t < 8 holds slot t of the node's
+// line (coefficient, input, dependent), loads input t and forms term t; the
+// node's sums then run over the terms in slot order -- the order of the
+// queue engine in fsb_flow.cu -- with every lane doing the same scalar
+// arithmetic on shuffled terms, so the warp never diverges and the loops over
+// eight slots become one instruction each.  Lane 0 stores the node's value.
+// run() returns the dependent in this lane's slot (-1 for none, and for lanes
+// 8..31).
+constexpr unsigned FULL = 0xffffffffu;
+__device__ __forceinline__ double shfl_d(double v, int src) { return __shfl_sync(FULL, v, src); }
+__device__ __forceinline__ float shfl_f(float v, int src) { return __shfl_sync(FULL, v, src); }
 
 // a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115)
 struct AccRegionOp {
   const RegionLine* line;
   double* val;
-  __device__ int run(int g, int tile, int lr, int (&dep)[8]) const {
-    const LineRegs L(line + g);
-    double x[8];
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      const int d = L.inp(t);
-      x[t] = d < 0 ? 0.0 : ((d >> lr) == tile ? ld_l1(val + d) : ld_l2(val + d));
-    }
-    int nd = 0;
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      dep[t] = L.dep(t);
-      nd += dep[t] >= 0;
-    }
-#pragma unroll
-    for (int t = 0; t < 8; ++t)
-      if (t < nd) prefetch_l1(line + dep[t]);
+  __device__ int run(int g, int lane, int tile, int lr) const {
+    const int t = lane & 7;
+    const RegionLine* L = line + g;
+    const double c = __ldg(&L->c[t]);
+    const int d = __ldg(&L->dep[t]);
+    const int q = __ldg(&L->inp[t]);
+    const bool mine = lane < 8 && q >= 0;
+    double x = 0.0;
+    if (mine) x = (q >> lr) == tile ? ld_l1(val + q) : ld_l2(val + q);
+    if (lane < 8 && d >= 0) prefetch_l1(line + d);
+    const double term = x * c;
+    const unsigned present = __ballot_sync(FULL, mine);
     double acc = ld_l1(val + g);  // dx*dy*precip(k), stored by the line builder
 #pragma unroll
-    for (int t = 0; t < 8; ++t)
-      if (L.inp(t) >= 0) acc = acc + x[t] * L.c[t];
-    st_global(val + g, acc);
-    return nd;
+    for (int s = 0; s < 8; ++s) {
+      const double v = shfl_d(term, s);
+      if ((present >> s) & 1u) acc = acc + v;
+    }
+    if (lane == 0) st_global(val + g, acc);
+    return lane < 8 ? d : -1;
   }
 };
 
@@ -430,7 +435,8 @@ struct RegionPow {
 };
 
 // implicit stream power law over the multiple receivers with g == 0
-// (StreamPowerLaw.f90:92-177): hw[g] = (new h, water)
+// (StreamPowerLaw.f90:92-177): hw[g] = (new h, water); each Newton
+// iteration evaluates the eight receivers' powers in parallel, one per lane
 struct SplRegionOp {
   const RegionLine* line;
   double2* hw;
@@ -438,69 +444,101 @@ struct SplRegionOp {
   double omega;
   int n_is_one;
   int* err;
-  __device__ int run(int g, int tile, int lr, int (&dep)[8]) const {
-    const LineRegs L(line + g);
+  __device__ int run(int g, int lane, int tile, int lr) const {
+    const int t = lane & 7;
+    const RegionLine* L = line + g;
+    const double c = __ldg(&L->c[t]);
+    const int d = __ldg(&L->dep[t]);
+    const int q = __ldg(&L->inp[t]);
     const double2 self = ld_l1(hw + g);
     int rg;
     bool has_mrec;
     unpack_meta(self.y, rg, has_mrec);
     const double ht = self.x;
-    double hq[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, wr = 0.0;
+    const bool mine = lane < 8 && q >= 0;
+    const unsigned present = __ballot_sync(FULL, mine);
+    double hq = 0.0, wr = 0.0;
     if (rg >= 0) {
-      const double2 rv = (rg >> lr) == tile ? ld_l1(hw + rg) : ld_l2(hw + rg);
-      wr = rv.y;
-#pragma unroll
-      for (int t = 0; t < 8; ++t) {
-        const int q = L.inp(t);
-        hq[t] = q < 0 ? 0.0 : ((q >> lr) == tile ? ld_l1(hw + q).x : ld_l2(hw + q).x);
-      }
+      if (mine) hq = (q >> lr) == tile ? ld_l1(hw + q).x : ld_l2(hw + q).x;
+      double w = 0.0;
+      if (lane == 0) w = (rg >> lr) == tile ? ld_l1(hw + rg).y : ld_l2(hw + rg).y;
+      wr = shfl_d(w, 0);
     }
-    int nd = 0;
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      dep[t] = L.dep(t);
-      nd += dep[t] >= 0;
-    }
-#pragma unroll
-    for (int t = 0; t < 8; ++t)
-      if (t < nd) prefetch_l1(line + dep[t]);
+    if (lane < 8 && d >= 0) prefetch_l1(line + d);
     double hk = ht, wk = ht;
     if (rg >= 0) {
       const double elev = ht;
       if (elev > wr) {
         if (has_mrec) {
           if (n_is_one) {
+            const double tf = c * hq;
             double f = elev, df = 1.0;
 #pragma unroll
-            for (int t = 0; t < 8; ++t)
-              if (L.inp(t) >= 0) {
-                f = f + L.c[t] * hq[t];
-                df = df + L.c[t];
+            for (int s = 0; s < 8; ++s) {
+              const double a = shfl_d(tf, s), b = shfl_d(c, s);
+              if ((present >> s) & 1u) {
+                f = f + a;
+                df = df + b;
               }
+            }
             hk = f / df;
-          } else {
+          } else if (np.half3) {  // n = 1.5: the receivers' square roots in parallel
             const double tolp = 1.0e-3;
             double errp = 2.0 * tolp;
             int guard = 0;
             while (errp > tolp) {
               if (++guard > kNewtonLimit) {
-                atomicExch(err, DEV_NEWTON_LIMIT);
+                if (lane == 0) atomicExch(err, DEV_NEWTON_LIMIT);
                 break;
               }
+              const double x = fmax(0.0, hk - hq);
+              const double r = sqrt(x);
+              const double tf = c * (x * r), tdf = c * np.n * r;
               double f = hk - elev, df = 1.0;
 #pragma unroll
-              for (int t = 0; t < 8; ++t)
-                if (L.inp(t) >= 0) {
-                  const double x = fmax(0.0, hk - hq[t]);
-                  double pn, pn1;
-                  np.eval(x, pn, pn1);
-                  f = f + L.c[t] * pn;
-                  df = df + L.c[t] * np.n * pn1;
+              for (int s = 0; s < 8; ++s) {
+                const double a = shfl_d(tf, s), b = shfl_d(tdf, s);
+                if ((present >> s) & 1u) {
+                  f = f + a;
+                  df = df + b;
                 }
+              }
               const double hn = hk - f / df;
               errp = fabs(hn - hk);
               hk = hk * (1.0 - omega) + hn * omega;
             }
+          } else {  // other n: the slots gathered to lane 0, which iterates with pow
+            double fs[8], qs[8];
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {
+              fs[s] = shfl_d(c, s);
+              qs[s] = shfl_d(hq, s);
+            }
+            if (lane == 0) {
+              const double tolp = 1.0e-3;
+              double errp = 2.0 * tolp;
+              int guard = 0;
+              while (errp > tolp) {
+                if (++guard > kNewtonLimit) {
+                  atomicExch(err, DEV_NEWTON_LIMIT);
+                  break;
+                }
+                double f = hk - elev, df = 1.0;
+#pragma unroll
+                for (int s = 0; s < 8; ++s)
+                  if ((present >> s) & 1u) {
+                    const double x = fmax(0.0, hk - qs[s]);
+                    double pn, pn1;
+                    np.eval(x, pn, pn1);
+                    f = f + fs[s] * pn;
+                    df = df + fs[s] * np.n * pn1;
+                  }
+                const double hn = hk - f / df;
+                errp = fabs(hn - hk);
+                hk = hk * (1.0 - omega) + hn * omega;
+              }
+            }
+            hk = shfl_d(hk, 0);
           }
         }
         if (hk < wr) hk = wr;
@@ -509,8 +547,8 @@ struct SplRegionOp {
       }
       wk = fmax(wr, hk);
     }
-    st_global(hw + g, make_double2(hk, wk));
-    return nd;
+    if (lane == 0) st_global(hw + g, make_double2(hk, wk));
+    return lane < 8 ? d : -1;
   }
 };
 
@@ -518,29 +556,26 @@ struct SplRegionOp {
 struct AccRegionOpF {
   const RegionLineF* line;
   float* val;
-  __device__ int run(int g, int tile, int lr, int (&dep)[8]) const {
-    const LineRegsT<float> L(line + g);
-    float x[8];
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      const int d = L.inp(t);
-      x[t] = d < 0 ? 0.0f : ((d >> lr) == tile ? ld_l1f(val + d) : ld_l2f(val + d));
-    }
-    int nd = 0;
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      dep[t] = L.dep(t);
-      nd += dep[t] >= 0;
-    }
-#pragma unroll
-    for (int t = 0; t < 8; ++t)
-      if (t < nd) prefetch_l1(line + dep[t]);
+  __device__ int run(int g, int lane, int tile, int lr) const {
+    const int t = lane & 7;
+    const RegionLineF* L = line + g;
+    const float c = __ldg(&L->c[t]);
+    const int d = __ldg(&L->dep[t]);
+    const int q = __ldg(&L->inp[t]);
+    const bool mine = lane < 8 && q >= 0;
+    float x = 0.0f;
+    if (mine) x = (q >> lr) == tile ? ld_l1f(val + q) : ld_l2f(val + q);
+    if (lane < 8 && d >= 0) prefetch_l1(line + d);
+    const float term = x * c;
+    const unsigned present = __ballot_sync(FULL, mine);
     float acc = ld_l1f(val + g);
 #pragma unroll
-    for (int t = 0; t < 8; ++t)
-      if (L.inp(t) >= 0) acc = acc + x[t] * L.c[t];
-    st_globalf(val + g, acc);
-    return nd;
+    for (int s = 0; s < 8; ++s) {
+      const float v = shfl_f(term, s);
+      if ((present >> s) & 1u) acc = acc + v;
+    }
+    if (lane == 0) st_globalf(val + g, acc);
+    return lane < 8 ? d : -1;
   }
 };
 
@@ -559,81 +594,108 @@ struct SplRegionOpM {
   float omega;
   int n_is_one;
   int* err;
-  __device__ int run(int g, int tile, int lr, int (&dep)[8]) const {
-    const LineRegsT<float> L(line + g);
+  __device__ int run(int g, int lane, int tile, int lr) const {
+    const int t = lane & 7;
+    const RegionLineF* L = line + g;
+    const float c = __ldg(&L->c[t]);
+    const int dp = __ldg(&L->dep[t]);
+    const int q = __ldg(&L->inp[t]);
     const double2 self = ld_l1(hw + g);
     int rg;
     bool has_mrec;
     unpack_meta(self.y, rg, has_mrec);
     const double ht = self.x;
-    double hq[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, wr = 0.0;
+    const bool mine = lane < 8 && q >= 0;
+    const unsigned present = __ballot_sync(FULL, mine);
+    double hq = 0.0, wr = 0.0;
     if (rg >= 0) {
-      const double2 rv = (rg >> lr) == tile ? ld_l1(hw + rg) : ld_l2(hw + rg);
-      wr = rv.y;
-#pragma unroll
-      for (int t = 0; t < 8; ++t) {
-        const int q = L.inp(t);
-        hq[t] = q < 0 ? 0.0 : ((q >> lr) == tile ? ld_l1(hw + q).x : ld_l2(hw + q).x);
-      }
+      if (mine) hq = (q >> lr) == tile ? ld_l1(hw + q).x : ld_l2(hw + q).x;
+      double w = 0.0;
+      if (lane == 0) w = (rg >> lr) == tile ? ld_l1(hw + rg).y : ld_l2(hw + rg).y;
+      wr = shfl_d(w, 0);
     }
-    int nd = 0;
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      dep[t] = L.dep(t);
-      nd += dep[t] >= 0;
-    }
-#pragma unroll
-    for (int t = 0; t < 8; ++t)
-      if (t < nd) prefetch_l1(line + dep[t]);
+    if (lane < 8 && dp >= 0) prefetch_l1(line + dp);
     double hk = ht, wk = ht;
     if (rg >= 0) {
       if (ht > wr) {
         if (has_mrec) {
-          float dist[8];
-#pragma unroll
-          for (int t = 0; t < 8; ++t) dist[t] = L.inp(t) >= 0 ? (float)(ht - hq[t]) : 0.0f;
+          const float dist = mine ? (float)(ht - hq) : 0.0f;
           float d = 0.0f;
           if (n_is_one) {
+            const float tf = c * dist;
             float num = 0.0f, den = 1.0f;
 #pragma unroll
-            for (int t = 0; t < 8; ++t)
-              if (L.inp(t) >= 0) {
-                num = num + L.c[t] * dist[t];
-                den = den + L.c[t];
+            for (int s = 0; s < 8; ++s) {
+              const float a = shfl_f(tf, s), b = shfl_f(c, s);
+              if ((present >> s) & 1u) {
+                num = num + a;
+                den = den + b;
               }
+            }
             d = -num / den;
-          } else {
+          } else if (half3) {  // n = 1.5: the receivers' square roots in parallel
             const float tolp = 1.0e-3f;
             float errp = 2.0f * tolp;
             int guard = 0;
             while (errp > tolp) {
               if (++guard > kNewtonLimit) {
-                atomicExch(err, DEV_NEWTON_LIMIT);
+                if (lane == 0) atomicExch(err, DEV_NEWTON_LIMIT);
                 break;
               }
+              const float x = fmaxf(0.0f, dist + d);
+              const float r = sqrtf(x);
+              const float tf = c * (x * r), tdf = c * n * r;
               float f = d, df = 1.0f;
 #pragma unroll
-              for (int t = 0; t < 8; ++t)
-                if (L.inp(t) >= 0) {
-                  const float x = fmaxf(0.0f, dist[t] + d);
-                  float pn, pn1;
-                  if (half3) {
-                    pn1 = sqrtf(x);
-                    pn = x * pn1;
-                  } else if (x > 0.0f) {
-                    pn1 = powf(x, n - 1.0f);
-                    pn = x * pn1;
-                  } else {
-                    pn = powf(x, n);
-                    pn1 = powf(x, n - 1.0f);
-                  }
-                  f = f + L.c[t] * pn;
-                  df = df + L.c[t] * n * pn1;
+              for (int s = 0; s < 8; ++s) {
+                const float a = shfl_f(tf, s), b = shfl_f(tdf, s);
+                if ((present >> s) & 1u) {
+                  f = f + a;
+                  df = df + b;
                 }
+              }
               const float dn = d - f / df;
               errp = fabsf(dn - d);
               d = d * (1.0f - omega) + dn * omega;
             }
+          } else {  // other n: the slots gathered to lane 0, which iterates with powf
+            float fs[8], ds[8];
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {
+              fs[s] = shfl_f(c, s);
+              ds[s] = shfl_f(dist, s);
+            }
+            if (lane == 0) {
+              const float tolp = 1.0e-3f;
+              float errp = 2.0f * tolp;
+              int guard = 0;
+              while (errp > tolp) {
+                if (++guard > kNewtonLimit) {
+                  atomicExch(err, DEV_NEWTON_LIMIT);
+                  break;
+                }
+                float f = d, df = 1.0f;
+#pragma unroll
+                for (int s = 0; s < 8; ++s)
+                  if ((present >> s) & 1u) {
+                    const float x = fmaxf(0.0f, ds[s] + d);
+                    float pn, pn1;
+                    if (x > 0.0f) {
+                      pn1 = powf(x, n - 1.0f);
+                      pn = x * pn1;
+                    } else {
+                      pn = powf(x, n);
+                      pn1 = powf(x, n - 1.0f);
+                    }
+                    f = f + fs[s] * pn;
+                    df = df + fs[s] * n * pn1;
+                  }
+                const float dn = d - f / df;
+                errp = fabsf(dn - d);
+                d = d * (1.0f - omega) + dn * omega;
+              }
+            }
+            d = shfl_f(d, 0);
           }
           hk = ht + (double)d;
         }
@@ -643,20 +705,22 @@ struct SplRegionOpM {
       }
       wk = fmax(wr, hk);
     }
-    st_global(hw + g, make_double2(hk, wk));
-    return nd;
+    if (lane == 0) st_global(hw + g, make_double2(hk, wk));
+    return lane < 8 ? dp : -1;
   }
 };
 
 // ---- the sweep kernel ------------------------------------------------------------
 // One CTA per tile.  Shared memory: the tile's counters (bytes, four per word)
 // and its ready queue (local indices, filled once each, never wrapped).
-// Warp 0's lane 0 polls the tile's inbox; the other warps' first LANES lanes
-// take nodes: a lane that finishes a node continues with the first of its
-// dependents it made ready (they come largest priority first) and queues the
-// others.  A CTA ends when all nodes of its tile are done; every wait is
-// bounded by a 4 s limit, after which the sweep reports DEV_SPIN_LIMIT.
-template <class Op, int LANES>
+// Warp 0's lane 0 polls the tile's inbox; each other warp computes one node
+// at a time: after a node, its lanes release the node's dependents (one per
+// lane), the warp continues with the first one made ready (they come largest
+// priority first) and queues the others.  An idle warp claims the next queue
+// slot and waits for it to be filled.  A CTA ends when all nodes of its tile
+// are done; every wait is bounded by a 4 s limit, after which the sweep
+// reports DEV_SPIN_LIMIT.
+template <class Op>
 __global__ void __launch_bounds__(kRegionThreads, 2)
     k_region_sweep(Op op, TileMap tm, const unsigned char* __restrict__ cnt0, int* xcnt, int* inbox, int icap,
                    unsigned* itail, int* err) {
@@ -699,7 +763,7 @@ __global__ void __launch_bounds__(kRegionThreads, 2)
     const unsigned old = atomicSub(&cnt[l >> 2], 1u << sh);
     return ((old >> sh) & 0xffu) == 1u;
   };
-  // periodic checks of the time limit and of failures elsewhere
+  // periodic checks of the time limit and of failures elsewhere (one lane)
   auto should_stop = [&](int& ticks) {
     if (*(volatile int*)&stop) return true;
     if (++ticks < 256) return false;
@@ -735,45 +799,39 @@ __global__ void __launch_bounds__(kRegionThreads, 2)
       __nanosleep(64);
     }
   }
-  if (lane >= LANES) return;
   int cur = -1, slot = -1, ticks = 0;
   for (;;) {
     if (cur < 0) {
-      if (slot < 0) slot = atomicAdd(&qhead, 1);
-      if (slot < R) {
-        const unsigned short v = *(volatile unsigned short*)&q[slot];
-        if (v != kQEmpty) {
-          cur = v;
-          slot = -1;
-          __threadfence_block();  // acquire: the producers' values
+      int got = -1, quit = 0;
+      if (lane == 0) {
+        if (slot < 0) slot = atomicAdd(&qhead, 1);
+        if (slot < R) {
+          const unsigned short v = *(volatile unsigned short*)&q[slot];
+          if (v != kQEmpty) {
+            got = v;
+            slot = -1;
+          }
         }
+        if (got < 0) quit = *(volatile int*)&ndone >= count || should_stop(ticks);
       }
-      if (cur < 0) {
-        if (*(volatile int*)&ndone >= count) return;
-        if (should_stop(ticks)) return;
+      got = __shfl_sync(FULL, got, 0);
+      if (got < 0) {
+        if (__shfl_sync(FULL, quit, 0)) return;
         __nanosleep(32);
         continue;
       }
+      cur = got;
+      __threadfence_block();  // acquire: the producers' values
     }
-    int dep[8];
-    const int nd = op.run(gbase + cur, tile, lr, dep);
-    __threadfence_block();  // release: this node's value before its dependents' counters
-    int nxt = -1;
-    bool cross_fenced = false;
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      if (t >= nd) break;
-      const int d = dep[t];
+    const int d = op.run(gbase + cur, lane, tile, lr);
+    __syncwarp();
+    __threadfence_block();  // release: the node's value before its dependents' counters
+    bool ready = false;
+    if (d >= 0) {
       if ((d >> lr) == tile) {
-        if (release(d - gbase)) {
-          if (nxt < 0) nxt = d - gbase;
-          else push(d - gbase);
-        }
+        ready = release(d - gbase);
       } else {
-        if (!cross_fenced) {
-          __threadfence();  // release at GPU scope before a cross-tile counter
-          cross_fenced = true;
-        }
+        __threadfence();  // release at GPU scope before a cross-tile counter
         if (atomicSub(&xcnt[d], 1) == 1) {
           __threadfence();
           const int owner = d >> lr;
@@ -783,8 +841,15 @@ __global__ void __launch_bounds__(kRegionThreads, 2)
         }
       }
     }
-    atomicAdd(&ndone, 1);
-    if (nxt >= 0) __threadfence_block();  // acquire for the continuation
+    const unsigned rm = __ballot_sync(FULL, ready);
+    int nxt = -1;
+    if (rm) {
+      const int first = __ffs(rm) - 1;
+      nxt = __shfl_sync(FULL, d - gbase, first);
+      if (ready && lane != first) push(d - gbase);
+      __threadfence_block();  // acquire for the continuation
+    }
+    if (lane == 0) atomicAdd(&ndone, 1);
     cur = nxt;
   }
 }
@@ -813,20 +878,14 @@ __global__ void k_spl_finish_t(int nx, int ny, TileMap tm, double dt, const doub
   }
 }
 
-#ifndef FSB_REGION_LANES_ACC
-#define FSB_REGION_LANES_ACC 4
-#endif
-#ifndef FSB_REGION_LANES_SPL
-#define FSB_REGION_LANES_SPL 2
-#endif
 
 size_t region_smem(const TileMap& tm) { return (size_t)3 << tm.lr(); }
 
 // whether every tile's CTA of this sweep kernel can be co-resident
-template <class Op, int LANES>
+template <class Op>
 bool region_fits(const TileMap& tm) {
   const size_t smem = region_smem(tm);
-  auto kern = k_region_sweep<Op, LANES>;
+  auto kern = k_region_sweep<Op>;
   // the permitted maximum covers every plan (3 bytes per node, 32768 nodes per
   // tile), so instances with different plans never undo each other's setting
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * 32768) != cudaSuccess) {
@@ -847,21 +906,21 @@ bool region_fits(const TileMap& tm) {
 bool region_usable(Ctx& c) {
   if (!c.region_enabled || c.tmap.ntx == 0) return false;
   if (c.region_state == 0)
-    c.region_state = (region_fits<AccRegionOp, FSB_REGION_LANES_ACC>(c.tmap) &&
-                      region_fits<SplRegionOp, FSB_REGION_LANES_SPL>(c.tmap) &&
-                      region_fits<AccRegionOpF, FSB_REGION_LANES_ACC>(c.tmap) &&
-                      region_fits<SplRegionOpM, FSB_REGION_LANES_SPL>(c.tmap))
+    c.region_state = (region_fits<AccRegionOp>(c.tmap) &&
+                      region_fits<SplRegionOp>(c.tmap) &&
+                      region_fits<AccRegionOpF>(c.tmap) &&
+                      region_fits<SplRegionOpM>(c.tmap))
                          ? 1
                          : -1;
   return c.region_state > 0;
 }
 
-template <class Op, int LANES>
+template <class Op>
 bool launch_region(Ctx& c, Op op) {
   const TileMap& tm = c.tmap;
   const int tiles = tm.tiles();
   const size_t smem = region_smem(tm);
-  auto kern = k_region_sweep<Op, LANES>;
+  auto kern = k_region_sweep<Op>;
   cudaMemsetAsync(c.rl_inbox, 0xff, sizeof(int) * (size_t)tiles * c.rl_icap, c.stream);
   cudaMemsetAsync(c.rl_itail, 0, sizeof(unsigned) * (size_t)tiles, c.stream);
   const unsigned char* cnt0 = c.rl_cnt0;
@@ -922,7 +981,7 @@ bool region_accumulate(Ctx& c) {
                                                                 c.precip, c.size, line, val, c.rl_cnt0, c.rl_xcnt,
                                                                 c.d_err);
     c.count_launch();
-    if (!launch_region<AccRegionOpF, FSB_REGION_LANES_ACC>(c, AccRegionOpF{line, val})) return false;
+    if (!launch_region<AccRegionOpF>(c, AccRegionOpF{line, val})) return false;
     k_untile_area<float><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, val, c.a);
   } else {
     RegionLine* line = static_cast<RegionLine*>(c.rl_line);
@@ -930,7 +989,7 @@ bool region_accumulate(Ctx& c) {
                                                                  c.precip, c.size, line, c.rl_val, c.rl_cnt0,
                                                                  c.rl_xcnt, c.d_err);
     c.count_launch();
-    if (!launch_region<AccRegionOp, FSB_REGION_LANES_ACC>(c, AccRegionOp{line, c.rl_val})) return false;
+    if (!launch_region<AccRegionOp>(c, AccRegionOp{line, c.rl_val})) return false;
     k_untile_area<double><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, c.rl_val, c.a);
   }
   c.count_launch();
@@ -950,7 +1009,7 @@ bool region_stream_power(Ctx& c) {
                                                                 c.size, line, hw, c.rl_cnt0, c.rl_xcnt, c.d_err);
     c.count_launch();
     SplRegionOpM op{line, hw, (float)c.n, c.n == 1.5, (float)(0.875 / c.n), n1, c.d_err};
-    if (!launch_region<SplRegionOpM, FSB_REGION_LANES_SPL>(c, op)) return false;
+    if (!launch_region<SplRegionOpM>(c, op)) return false;
   } else {
     RegionLine* line = static_cast<RegionLine*>(c.rl_line);
     k_spl_lines_t<double><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, tm, n1, c.kfsed, c.dt, c.m, c.n, c.rec,
@@ -959,7 +1018,7 @@ bool region_stream_power(Ctx& c) {
                                                                  c.d_err);
     c.count_launch();
     SplRegionOp op{line, hw, RegionPow{c.n, c.n == 1.5}, 0.875 / c.n, n1, c.d_err};
-    if (!launch_region<SplRegionOp, FSB_REGION_LANES_SPL>(c, op)) return false;
+    if (!launch_region<SplRegionOp>(c, op)) return false;
   }
   k_spl_finish_t<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, c.dt, hw, c.h, c.b, c.etot, c.erate,
                                                         c.sedflux);
