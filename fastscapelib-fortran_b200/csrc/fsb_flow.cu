@@ -23,7 +23,6 @@
 #include <cuda/atomic>
 #include <cfloat>
 #include <cstddef>
-#include <mutex>
 
 #include "fsb_kernels.cuh"
 
@@ -1032,6 +1031,10 @@ __device__ inline void cp_async_elem(double* smem, const double* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
 }
 
+__device__ inline void cp_async_elem(float* smem, const float* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem));
+}
 __device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ inline void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
@@ -1141,268 +1144,16 @@ __global__ void k_diff_xgather(Bounds bd, const T* __restrict__ Ux, const double
   }
 }
 
-// ---- fused ADI line solves ---------------------------------------------------
-// One pass of the ADI step without the coefficient arrays: each block of two
-// warps owns 32 grid lines.  Warp 1 computes the equations of the next chunk
-// of 32 elements of those lines (x_equation / y_equation, lane = element or
-// line) into shared memory while warp 0 runs the Thomas recurrence of tridag
-// (Diffusion.f90:164-202, one thread per line, the reference's arithmetic and
-// order) on the current chunk; the forward factors gam and u go to global
-// scratch in natural layout, and a backward sweep in the same kernel writes
-// the solution.  Plain form (T = double): the lines' solution.  Mixed form
-// (T = float): the equations carry the FP64 residual of the current surface
-// and the solution is the increment, added to the surface in FP64.
-constexpr int kAdiTile = 32 * 33;  // one [32][33] tile
-
-template <class T>
-__device__ inline void put_equation(T* A, T* B, T* C, T* F, int o, const Equation& e) {
-  if constexpr (sizeof(T) == sizeof(double)) {
-    A[o] = e.a; B[o] = e.bb; C[o] = e.c; F[o] = e.f;
-  } else {
-    const double r = e.f - (e.a * e.zm + e.bb * e.z0 + e.c * e.zp);
-    A[o] = (T)e.a; B[o] = (T)e.bb; C[o] = (T)e.c; F[o] = (T)r;
-  }
-}
-
-// One forward step of tridag for element t of a line: gam = c(t-1)/bet,
-// bet = b - a*gam, u = (f - a*u)/bet (t = 0: bet = b, u = f/bet, gam = 0).
-template <class T>
-__device__ inline bool thomas_step(bool first, T a, T b, T f, T& cprev, T c, T& bet, T& up, T& gam) {
-  if (first) {
-    bet = b;
-    if (bet == (T)0) return false;
-    up = f / bet;
-    gam = (T)0;
-  } else {
-    gam = cprev / bet;
-    bet = b - a * gam;
-    if (bet == (T)0) return false;
-    up = (f - a * up) / bet;
-  }
-  cprev = c;
-  return true;
-}
-
-// x pass: lines are rows j = 1..ny-2 (32 per block), elements i = 0..nx-1.
-// z: the surface (h); G, U: scratch [nn] (natural layout); zint: result on
-// rows 1..ny-2.
-template <class T>
-__global__ void __launch_bounds__(64) k_adi_rows(Bounds bd, double dt2, double dx2, double dy2,
-                                                 const double* __restrict__ K, const double* __restrict__ z,
-                                                 T* __restrict__ G, T* __restrict__ U, double* __restrict__ zint,
-                                                 int* __restrict__ err) {
-  extern __shared__ __align__(16) unsigned char adi_smem[];
-  T* eq = reinterpret_cast<T*>(adi_smem);  // [2 buffers][a, b, c, f][32 lines][33]
-  T* out = eq + 8 * kAdiTile;              // [2 buffers][gam, u][32 lines][33]
-  __shared__ int bad;
-  const int nx = bd.nx, ny = bd.ny;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int jb = 1 + blockIdx.x * 32;
-  const int nch = (nx + 31) / 32;
-  if (threadIdx.x == 0) bad = 0;
-  __syncthreads();
-  T bet = 0, up = 0, cprev = 0;
-  auto tile = [&](T* base, int buf, int which) { return base + (buf * 4 + which) * kAdiTile; };
-  auto otile = [&](int buf, int which) { return out + (buf * 2 + which) * kAdiTile; };
-  auto store_out = [&](int k) {  // warp 1: gam and u of chunk k, coalesced along the rows
-    const int i = k * 32 + lane;
-    if (i >= nx) return;
-    for (int r = 0; r < 32; ++r) {
-      const int j = jb + r;
-      if (j > ny - 2) break;
-      G[(size_t)j * nx + i] = otile(k & 1, 0)[r * 33 + lane];
-      U[(size_t)j * nx + i] = otile(k & 1, 1)[r * 33 + lane];
-    }
-  };
-  for (int k = 0; k <= nch; ++k) {
-    if (warp == 1) {
-      if (k < nch) {
-        const int i = k * 32 + lane;
-        if (i < nx)
-          for (int r = 0; r < 32; ++r) {
-            const int j = jb + r;
-            if (j > ny - 2) break;
-            put_equation(tile(eq, k & 1, 0), tile(eq, k & 1, 1), tile(eq, k & 1, 2), tile(eq, k & 1, 3),
-                         r * 33 + lane, x_equation(bd, dt2, dx2, dy2, K, z, i, j));
-          }
-      }
-      if (k >= 2) store_out(k - 2);
-    } else if (k >= 1 && jb + lane <= ny - 2 && !bad) {
-      const int kc = k - 1, i0 = kc * 32, tn = min(32, nx - i0);
-      const T* A = tile(eq, kc & 1, 0) + lane * 33;
-      const T* B = tile(eq, kc & 1, 1) + lane * 33;
-      const T* C = tile(eq, kc & 1, 2) + lane * 33;
-      const T* F = tile(eq, kc & 1, 3) + lane * 33;
-      T* og = otile(kc & 1, 0) + lane * 33;
-      T* ou = otile(kc & 1, 1) + lane * 33;
-      for (int t = 0; t < tn; ++t) {
-        T gam;
-        if (!thomas_step(i0 + t == 0, A[t], B[t], F[t], cprev, C[t], bet, up, gam)) {
-          bad = 1;
-          break;
-        }
-        og[t] = gam;
-        ou[t] = up;
-      }
-    }
-    __syncthreads();
-  }
-  if (warp == 1) store_out(nch - 1);
-  if (bad) {
-    if (threadIdx.x == 0) atomicExch(err, DEV_TRIDAG_ZERO);
-    return;
-  }
-  __threadfence_block();
-  __syncthreads();
-  // backward: u(t) = u(t) - gam(t+1)*u(t+1), chunks from the end; warp 1
-  // loads chunk k's gam and u into a tile, warp 0 substitutes chunk k+1's
-  // (loaded one iteration earlier) and leaves the solution in its tile,
-  // which warp 1 stores two iterations later
-  T gnext = 0;
-  auto ltile = [&](int buf, int which) { return eq + (buf * 2 + which) * kAdiTile; };  // reuse eq
-  auto store_res = [&](int k) {
-    const int i = k * 32 + lane;
-    if (i >= nx) return;
-    for (int r = 0; r < 32; ++r) {
-      const int j = jb + r;
-      if (j > ny - 2) break;
-      const size_t o = (size_t)j * nx + i;
-      const T v = ltile(k & 1, 1)[r * 33 + lane];
-      if constexpr (sizeof(T) == sizeof(double)) zint[o] = v;
-      else zint[o] = z[o] + (double)v;
-    }
-  };
-  for (int s = 0; s <= nch + 1; ++s) {
-    const int kl = nch - 1 - s;       // chunk loaded now
-    const int ks = nch - s;           // chunk substituted now
-    const int kw = nch + 1 - s;       // chunk stored now
-    if (warp == 1) {
-      if (kw < nch && kw >= 0) store_res(kw);
-      if (kl >= 0) {
-        const int i = kl * 32 + lane;
-        if (i < nx)
-          for (int r = 0; r < 32; ++r) {
-            const int j = jb + r;
-            if (j > ny - 2) break;
-            ltile(kl & 1, 0)[r * 33 + lane] = G[(size_t)j * nx + i];
-            ltile(kl & 1, 1)[r * 33 + lane] = U[(size_t)j * nx + i];
-          }
-      }
-    } else if (ks >= 0 && ks < nch && jb + lane <= ny - 2) {
-      const int i0 = ks * 32, tn = min(32, nx - i0);
-      const T* g = ltile(ks & 1, 0) + lane * 33;
-      T* u = ltile(ks & 1, 1) + lane * 33;
-      for (int t = tn - 1; t >= 0; --t) {
-        if (i0 + t == nx - 1) {
-          up = u[t];
-        } else {
-          up = u[t] - gnext * up;
-          u[t] = up;
-        }
-        gnext = g[t];
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// y pass: lines are columns i = 1..nx-2 (32 per block, lane = column),
-// elements j = 0..ny-1; z: the x pass result (zint); the backward sweep
-// applies Diffusion.f90:143-152 to those columns (etot, erate, h, b).
-template <class T>
-__global__ void __launch_bounds__(64) k_adi_cols(Bounds bd, double dt, double dt2, double dx2, double dy2,
-                                                 const double* __restrict__ K, const double* __restrict__ z,
-                                                 T* __restrict__ G, T* __restrict__ U, double* __restrict__ h,
-                                                 double* __restrict__ b, double* __restrict__ etot,
-                                                 double* __restrict__ erate, int* __restrict__ err) {
-  extern __shared__ __align__(16) unsigned char adi_smem[];
-  T* eq = reinterpret_cast<T*>(adi_smem);  // [2 buffers][a, b, c, f][32 elements][33]
-  __shared__ int bad;
-  const int nx = bd.nx, ny = bd.ny;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = 1 + blockIdx.x * 32 + lane;
-  const bool act = i <= nx - 2;
-  const int nch = (ny + 31) / 32;
-  if (threadIdx.x == 0) bad = 0;
-  __syncthreads();
-  T bet = 0, up = 0, cprev = 0;
-  auto tile = [&](int buf, int which) { return eq + (buf * 4 + which) * kAdiTile; };
-  for (int k = 0; k <= nch; ++k) {
-    if (warp == 1) {
-      if (k < nch && act)
-        for (int r = 0; r < 32; ++r) {
-          const int j = k * 32 + r;
-          if (j >= ny) break;
-          put_equation(tile(k & 1, 0), tile(k & 1, 1), tile(k & 1, 2), tile(k & 1, 3), r * 33 + lane,
-                       y_equation(bd, dt2, dx2, dy2, K, z, i, j));
-        }
-    } else if (k >= 1 && act && !bad) {
-      const int kc = k - 1, j0 = kc * 32, tn = min(32, ny - j0);
-      for (int t = 0; t < tn; ++t) {
-        const int o = t * 33 + lane;
-        T gam;
-        if (!thomas_step(j0 + t == 0, tile(kc & 1, 0)[o], tile(kc & 1, 1)[o], tile(kc & 1, 3)[o], cprev,
-                         tile(kc & 1, 2)[o], bet, up, gam)) {
-          bad = 1;
-          break;
-        }
-        const size_t g = (size_t)(j0 + t) * nx + i;
-        G[g] = gam;
-        U[g] = up;
-      }
-    }
-    __syncthreads();
-  }
-  if (bad) {
-    if (threadIdx.x == 0) atomicExch(err, DEV_TRIDAG_ZERO);
-    return;
-  }
-  __threadfence_block();
-  __syncthreads();
-  // backward with the finish fused: warp 1 prefetches chunk k's gam and u,
-  // warp 0 substitutes chunk k+1 and updates the nodes
-  T gnext = 0;
-  auto ltile = [&](int buf, int which) { return eq + (buf * 2 + which) * kAdiTile; };
-  for (int s = 0; s <= nch; ++s) {
-    const int kl = nch - 1 - s, ks = nch - s;
-    if (warp == 1) {
-      if (kl >= 0 && act)
-        for (int r = 0; r < 32; ++r) {
-          const int j = kl * 32 + r;
-          if (j >= ny) break;
-          const size_t g = (size_t)j * nx + i;
-          ltile(kl & 1, 0)[r * 33 + lane] = G[g];
-          ltile(kl & 1, 1)[r * 33 + lane] = U[g];
-        }
-    } else if (ks < nch && act) {
-      const int j0 = ks * 32, tn = min(32, ny - j0);
-      for (int t = tn - 1; t >= 0; --t) {
-        const int o = t * 33 + lane;
-        if (j0 + t != ny - 1) up = ltile(ks & 1, 1)[o] - gnext * up;
-        else up = ltile(ks & 1, 1)[o];
-        gnext = ltile(ks & 1, 0)[o];
-        const size_t k = (size_t)(j0 + t) * nx + i;
-        const double hk = h[k];
-        double zp;
-        if constexpr (sizeof(T) == sizeof(double)) zp = up;
-        else zp = z[k] + (double)up;
-        etot[k] = etot[k] + hk - zp;
-        erate[k] = erate[k] + (hk - zp) / dt;
-        h[k] = zp;
-        b[k] = fmin(zp, b[k]);
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// Diffusion.f90:143-152 on the edge columns i = 0 and nx-1 (zintp = h there)
-__global__ void k_adi_edge_cols(Bounds bd, double dt, double* __restrict__ h, double* __restrict__ b,
-                                double* __restrict__ etot, double* __restrict__ erate) {
-  const int nx = bd.nx, ny = bd.ny;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 2 * ny; q += gridDim.x * blockDim.x) {
-    const size_t k = (size_t)(q >> 1) * nx + ((q & 1) ? nx - 1 : 0);
-    const double hk = h[k], zp = hk;
+// mixed form of k_diff_finish: zintp = zint + the y-pass increment on columns
+// 1..nx-2, h elsewhere
+__global__ void k_diff_finish_m(Bounds bd, double dt, const float* __restrict__ dUy, const double* __restrict__ zint,
+                                double* __restrict__ h, double* __restrict__ b, double* __restrict__ etot,
+                                double* __restrict__ erate) {
+  const int nx = bd.nx, nn = nx * bd.ny;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const int i = k % nx;
+    const double hk = h[k];
+    const double zp = (i >= 1 && i <= nx - 2) ? zint[k] + (double)dUy[k] : hk;
     etot[k] = etot[k] + hk - zp;
     erate[k] = erate[k] + (hk - zp) / dt;
     h[k] = zp;
@@ -1583,44 +1334,64 @@ void thomas_lines(Ctx& c, int N, int L, int s0, int s1, const double* A, const d
   c.count_launch();
 }
 
-// ADI hillslope diffusion (Diffusion.f90:1-160): kdint, the x pass over the
-// rows and the y pass over the columns with the fused line solves, the node
-// updates fused into the y pass.  Plain form: the reference's arithmetic.
-// Mixed form: each line solved in FP32 for the increment of the surface
-// against the FP64 residual of the current surface, the increment added in
-// FP64.
-template <class T>
-static void diffusion_fused(Ctx& c) {
+// Mixed-precision ADI step: coefficients as in the plain form, each line
+// solved in FP32 for the increment of the surface against the FP64 residual
+// of the current surface, the increment added in FP64.
+static void diffusion_mixed(Ctx& c) {
   const int nx = c.nx, ny = c.ny, nn = c.nn;
   const double dt2 = c.dt / 2.0, dx2 = c.dx * c.dx, dy2 = c.dy * c.dy;
   double *K = c.dK, *Z = c.dZ;
-  T* G = reinterpret_cast<T*>(c.dA);
-  T* U = reinterpret_cast<T*>(c.dB);
-  const size_t rows_smem = 12 * kAdiTile * sizeof(T), cols_smem = 8 * kAdiTile * sizeof(T);
-  static std::once_flag attr_once;  // per element type, for every instance of the process
-  std::call_once(attr_once, [&] {
-    cudaFuncSetAttribute(k_adi_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows_smem);
-    cudaFuncSetAttribute(k_adi_cols<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cols_smem);
-  });
+  float *A = reinterpret_cast<float*>(c.dA), *B = reinterpret_cast<float*>(c.dB),
+        *C = reinterpret_cast<float*>(c.dC), *F = reinterpret_cast<float*>(c.dF),
+        *G = reinterpret_cast<float*>(c.dG);
   k_diff_kdint<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, c.kdsed, c.kd, c.h, c.b, K);
+  dim3 gx((nx + 127) / 128, ny - 2);
+  k_diff_xcoef<float><<<gx, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, c.h, A, B, C, F);
   stage_begin(c, KT_THOMAS_ROWS);
-  k_adi_rows<T><<<(ny - 2 + 31) / 32, 64, rows_smem, c.stream>>>(c.bd, dt2, dx2, dy2, K, c.h, G, U, Z, c.d_err);
+  k_thomas<float><<<(ny - 2 + 31) / 32, 32, 0, c.stream>>>(nx, ny, 1, ny - 1, A, B, C, F, G, c.d_err);
   stage_end(c, KT_THOMAS_ROWS);
-  // rows 0 and ny-1 keep h in the x pass
-  cudaMemcpyAsync(Z, c.h, sizeof(double) * nx, cudaMemcpyDeviceToDevice, c.stream);
-  cudaMemcpyAsync(Z + (size_t)(ny - 1) * nx, c.h + (size_t)(ny - 1) * nx, sizeof(double) * nx,
-                  cudaMemcpyDeviceToDevice, c.stream);
+  dim3 g2((nx + 31) / 32, (ny + 31) / 32);
+  k_diff_xgather<float><<<g2, dim3(32, 8), 0, c.stream>>>(c.bd, F, c.h, Z);
+  dim3 gy((nx + 127) / 128, ny);
+  k_diff_ycoef<float><<<gy, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, Z, A, B, C, F);
   stage_begin(c, KT_THOMAS_COLS);
-  k_adi_cols<T><<<(nx - 2 + 31) / 32, 64, cols_smem, c.stream>>>(c.bd, c.dt, dt2, dx2, dy2, K, Z, G, U, c.h, c.b,
-                                                                  c.etot, c.erate, c.d_err);
+  k_thomas<float><<<(nx - 2 + 31) / 32, 32, 0, c.stream>>>(ny, nx, 1, nx - 1, A, B, C, F, G, c.d_err);
   stage_end(c, KT_THOMAS_COLS);
-  k_adi_edge_cols<<<grid1d(2 * (size_t)ny), kBlock, 0, c.stream>>>(c.bd, c.dt, c.h, c.b, c.etot, c.erate);
-  c.count_launch(4);
+  k_diff_finish_m<<<grid1d(nn), kBlock, 0, c.stream>>>(c.bd, c.dt, F, Z, c.h, c.b, c.etot, c.erate);
+  c.count_launch(7);
 }
 
 void diffusion(Ctx& c) {
-  if (c.mixed) diffusion_fused<float>(c);
-  else diffusion_fused<double>(c);
+  if (c.mixed) {
+    diffusion_mixed(c);
+    return;
+  }
+  const int nx = c.nx, ny = c.ny, nn = c.nn;
+  const double dt2 = c.dt / 2.0, dx2 = c.dx * c.dx, dy2 = c.dy * c.dy;
+  double *K = c.dK, *A = c.dA, *B = c.dB, *C = c.dC, *F = c.dF, *G = c.dG, *Z = c.dZ;
+  k_diff_kdint<<<grid1d(nn), kBlock, 0, c.stream>>>(nn, c.kdsed, c.kd, c.h, c.b, K);
+  c.count_launch();
+  {
+    dim3 g((nx + 127) / 128, ny - 2);
+    k_diff_xcoef<double><<<g, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, c.h, A, B, C, F);
+    // systems are rows j=1..ny-2 with element i at [i*ny + j]
+    stage_begin(c, KT_THOMAS_ROWS);
+    k_thomas<double><<<(ny - 2 + 31) / 32, 32, 0, c.stream>>>(nx, ny, 1, ny - 1, A, B, C, F, G, c.d_err);
+    stage_end(c, KT_THOMAS_ROWS);
+    dim3 g2((nx + 31) / 32, (ny + 31) / 32);
+    k_diff_xgather<double><<<g2, dim3(32, 8), 0, c.stream>>>(c.bd, F, c.h, Z);
+    c.count_launch(3);
+  }
+  {
+    dim3 g((nx + 127) / 128, ny);
+    k_diff_ycoef<double><<<g, 128, 0, c.stream>>>(c.bd, dt2, dx2, dy2, K, Z, A, B, C, F);
+    stage_begin(c, KT_THOMAS_COLS);
+    k_thomas<double><<<(nx - 2 + 31) / 32, 32, 0, c.stream>>>(ny, nx, 1, nx - 1, A, B, C, F, G, c.d_err);
+    stage_end(c, KT_THOMAS_COLS);
+    c.count_launch(2);
+  }
+  k_diff_finish<<<grid1d(nn), kBlock, 0, c.stream>>>(c.bd, c.dt, F, c.h, c.b, c.etot, c.erate);
+  c.count_launch();
 }
 
 // The same ADI step on caller-supplied arrays: `scratch` holds 7*nx*ny
