@@ -317,8 +317,13 @@ int step_once(fsb::Ctx& c) {
     stage_end(c, ST_LOCMIN);
     if (!ok) { g_err = c.err; return 1; }
     stage_begin(c, ST_FILL);
-    fsb::build_chains(c);
-    fsb::fill_sweep(c);
+    // multiple flow with g = 0 fills lakes with the region-owned sweep; the
+    // single-flow sweeps and the sediment term use the chain schedule
+    c.chains_valid = false;
+    if (c.sfd || fsb::gs_active(c) || !fsb::region_fill(c)) {
+      fsb::ensure_chains(c);
+      fsb::fill_sweep(c);
+    }
     stage_end(c, ST_FILL);
     if (!c.sfd) {
       stage_begin(c, ST_MFD);
@@ -632,6 +637,7 @@ int fsb_copy_chi(fsb_ctx* h, double* dst, int where) {
     FSB_CUDA(cudaMemsetAsync(chi, 0, sizeof(double) * c.nn, c.stream));
   } else {
     const double a0 = (c.xl / (c.nx - 1)) * (c.yl / (c.ny - 1)) * 10.0;
+    fsb::ensure_chains(c);
     fsb::chi_chains(c, a0, c.m / c.n, chi);
   }
   return copy_out(c, chi, dst, where);
@@ -657,7 +663,10 @@ int fsb_get_fluxes(fsb_ctx* h, double* tectonic, double* erosion, double* bounda
   if (!c.routed)          // no stack yet: the flux is erate itself
     FSB_CUDA(cudaMemcpyAsync(flux, c.erate, sizeof(double) * c.nn, cudaMemcpyDeviceToDevice, c.stream));
   else if (c.sfd)
-    fsb::flux_chains(c, flux);
+    {
+      fsb::ensure_chains(c);
+      fsb::flux_chains(c, flux);
+    }
   else
     fsb::flux_mfd(c, flux);
   fsb::flux_sums(c, flux, c.red, c.red + 3 * 512);

@@ -661,6 +661,13 @@ void build_chains(Ctx& c) {
   c.ntickets_bu = c.h_cnt[19];
 }
 
+void ensure_chains(Ctx& c) {
+  if (!c.chains_valid) {
+    build_chains(c);
+    c.chains_valid = true;
+  }
+}
+
 static void next_epoch(Ctx& c) {
   c.epoch += 1;
   if (c.epoch == 0) {

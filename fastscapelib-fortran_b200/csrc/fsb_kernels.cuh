@@ -124,6 +124,7 @@ struct Ctx {
       *ch_sid = nullptr, *ch_hist = nullptr, *ch_goff = nullptr, *ch_tk_td = nullptr, *ch_tk_bu = nullptr;
   unsigned *ch_key = nullptr, *ch_skey = nullptr;
   int nchains = 0, ntickets_td = 0, ntickets_bu = 0, nroots = 0;
+  bool chains_valid = false;  // the chain schedule matches the current forest
   // last-arriver sweeps (multiple flow)
   int *la_queue = nullptr, *la_cnt = nullptr, *cnt_acc = nullptr, *cnt_spl = nullptr;
   void* mfd_line = nullptr;  // one 128-byte record per node (area, then stream power)
@@ -163,8 +164,8 @@ struct Ctx {
   // per-stage device timing (CUDA events on the instance's stream)
   // stages: uplift receivers stack locmin fill mfd accum spl diffusion advection;
   // then single kernels inside them: the area sweep, the stream-power sweep,
-  // the row and the column tridiagonal solves of the diffusion
-  static constexpr int kStages = 14;
+  // the row and the column tridiagonal solves of the diffusion, the lake fill
+  static constexpr int kStages = 15;
   bool profile = false;
   cudaEvent_t ev_begin[kStages] = {}, ev_end[kStages] = {};
   bool ev_pending[kStages] = {};
@@ -175,7 +176,7 @@ struct Ctx {
 };
 
 // per-stage / per-kernel CUDA events while profiling is on (fsb_api.cu)
-enum { KT_AREA_SWEEP = 10, KT_SPL_SWEEP = 11, KT_THOMAS_ROWS = 12, KT_THOMAS_COLS = 13 };
+enum { KT_AREA_SWEEP = 10, KT_SPL_SWEEP = 11, KT_THOMAS_ROWS = 12, KT_THOMAS_COLS = 13, KT_FILL_SWEEP = 14 };
 void stage_begin(Ctx& c, int s);
 void stage_end(Ctx& c, int s);
 
@@ -203,6 +204,7 @@ bool local_minima(Ctx& c);
 
 // chains (fsb_chains.cu)
 void build_chains(Ctx& c);          // heavy-first order + ticket lists of the current forest
+void ensure_chains(Ctx& c);         // build_chains unless the schedule is current
 void fill_chains(Ctx& c);
 void area_chains(Ctx& c);
 void spl_chains(Ctx& c, double* hnew);
@@ -215,6 +217,7 @@ void flux_mfd(Ctx& c, double* flux);                  // compute_fluxes' flux, m
 TileMap plan_tiles(int nx, int ny, int sms);
 bool region_accumulate(Ctx& c);
 bool region_stream_power(Ctx& c);
+bool region_fill(Ctx& c);  // hwater and lake_depth of the current forest (multiple flow)
 void thomas_lines(Ctx& c, int N, int L, int s0, int s1, const double* A, const double* B, const double* C, double* F,
                   double* G);
 void advect(Ctx& c);  // fsb_advect.cu

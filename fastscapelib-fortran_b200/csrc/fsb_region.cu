@@ -374,6 +374,50 @@ __global__ void k_spl_lines_t(Bounds bd, TileMap tm, int n_is_one, double kfsed,
   }
 }
 
+// Lake fill (FlowRouting.f90:73-89): the only input is rec(k); the
+// dependents are k's donors (the single-flow tree after LocalMinima),
+// largest priority first.  The value array starts as h.
+__global__ void k_fill_lines_t(int nx, int ny, TileMap tm, const int* __restrict__ rec, const int* __restrict__ ndon,
+                               const int* __restrict__ don, const double* __restrict__ h,
+                               const int* __restrict__ prio, RegionLine* __restrict__ line,
+                               double* __restrict__ val, unsigned char* __restrict__ cnt0, int* __restrict__ xcnt) {
+  const int nn = nx * ny;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const int gk = tm.g(k % nx, k / nx);
+    const int r = rec[k];
+    const int nd = ndon[k];
+    int dep[8];
+    unsigned pr[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      dep[t] = -1;
+      pr[t] = 0u;
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      if (t >= nd) break;
+      const int d = don[(size_t)k * 8 + t];
+      insert_by_priority(dep, pr, t, tm.g(d % nx, d / nx), prio16(prio[d]));
+    }
+    RegionLine L;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      L.c[t] = 0.0;
+      L.dep[t] = dep[t];
+      L.inp[t] = -1;
+    }
+    int x_in = 0;
+    if (r != k) {
+      L.inp[0] = tm.g(r % nx, r / nx);
+      x_in = (L.inp[0] >> tm.lr()) != (gk >> tm.lr());
+    }
+    line[gk] = L;
+    val[gk] = h[k];
+    cnt0[gk] = (unsigned char)(r != k ? 1 : 0);
+    xcnt[gk] = x_in;
+  }
+}
+
 // ---- node operations: one warp per node ------------------------------------------
 // A node is computed by a whole warp.  Lane t < 8 holds slot t of the node's
 // line (coefficient, input, dependent), loads input t and forms term t; the
@@ -387,11 +431,75 @@ constexpr unsigned FULL = 0xffffffffu;
 __device__ __forceinline__ double shfl_d(double v, int src) { return __shfl_sync(FULL, v, src); }
 __device__ __forceinline__ float shfl_f(float v, int src) { return __shfl_sync(FULL, v, src); }
 
+// Shared-memory cache of the values this CTA's nodes produced, direct-mapped
+// by local index.  A dependent that becomes ready usually reads inputs that
+// its neighbours produced shortly before; from this cache that is a
+// shared-memory access instead of an L2 round trip (global stores do not
+// bring the line into the consumer's L1).  Entries are written under a
+// sequence tag (invalidate, value, tag; CTA-scope fences between), and a
+// read counts only if the tag equals the node before and after the value is
+// read, so an entry being overwritten by another node is a miss, answered
+// from global memory, where every value is stored before its dependents are
+// released.
+template <class V> struct CacheSlot;
+template <> struct CacheSlot<double> { double v; int tag; int pad; };
+template <> struct CacheSlot<float> { float v; int tag; };
+template <> struct CacheSlot<double2> { double x, y; int tag; int pad; };
+constexpr int kCacheSlots = 2048;
+
+__device__ __forceinline__ void read_slot(volatile CacheSlot<double>* e, double& v) { v = e->v; }
+__device__ __forceinline__ void read_slot(volatile CacheSlot<float>* e, float& v) { v = e->v; }
+__device__ __forceinline__ void read_slot(volatile CacheSlot<double2>* e, double2& v) {
+  v.x = e->x;
+  v.y = e->y;
+}
+__device__ __forceinline__ void write_slot(volatile CacheSlot<double>* e, double v) { e->v = v; }
+__device__ __forceinline__ void write_slot(volatile CacheSlot<float>* e, float v) { e->v = v; }
+__device__ __forceinline__ void write_slot(volatile CacheSlot<double2>* e, double2 v) {
+  e->x = v.x;
+  e->y = v.y;
+}
+__device__ __forceinline__ float ld_l1(const float* p) { return ld_l1f(p); }
+__device__ __forceinline__ float ld_l2(const float* p) { return ld_l2f(p); }
+
+template <class V>
+struct ValueCache {
+  CacheSlot<V>* slot;
+  int mask, gbase, tile, lr;
+  __device__ bool get(int g, V& out) const {
+    const int l = g - gbase;
+    volatile CacheSlot<V>* e = slot + (l & mask);
+    if (e->tag != l) return false;
+    __threadfence_block();
+    read_slot(e, out);
+    __threadfence_block();
+    return e->tag == l;
+  }
+  __device__ void put(int g, V v) const {
+    const int l = g - gbase;
+    volatile CacheSlot<V>* e = slot + (l & mask);
+    e->tag = -1;
+    __threadfence_block();
+    write_slot(e, v);
+    __threadfence_block();
+    e->tag = l;
+  }
+  // an input's value: the cache, else global memory (L1 for this tile's
+  // nodes, L2 for other tiles', whose values arrive through the inbox)
+  __device__ V load(const V* arr, int q) const {
+    if ((q >> lr) != tile) return ld_l2(arr + q);
+    V v;
+    if (get(q, v)) return v;
+    return ld_l1(arr + q);
+  }
+};
+
 // a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115)
 struct AccRegionOp {
+  using Value = double;
   const RegionLine* line;
   double* val;
-  __device__ int run(int g, int lane, int tile, int lr) const {
+  __device__ int run(int g, int lane, const ValueCache<double>& vc) const {
     const int t = lane & 7;
     const RegionLine* L = line + g;
     const double c = __ldg(&L->c[t]);
@@ -399,7 +507,7 @@ struct AccRegionOp {
     const int q = __ldg(&L->inp[t]);
     const bool mine = lane < 8 && q >= 0;
     double x = 0.0;
-    if (mine) x = (q >> lr) == tile ? ld_l1(val + q) : ld_l2(val + q);
+    if (mine) x = vc.load(val, q);
     if (lane < 8 && d >= 0) prefetch_l1(line + d);
     const double term = x * c;
     const unsigned present = __ballot_sync(FULL, mine);
@@ -409,7 +517,38 @@ struct AccRegionOp {
       const double v = shfl_d(term, s);
       if ((present >> s) & 1u) acc = acc + v;
     }
-    if (lane == 0) st_global(val + g, acc);
+    if (lane == 0) {
+      vc.put(g, acc);
+      st_global(val + g, acc);
+    }
+    return lane < 8 ? d : -1;
+  }
+};
+
+// hwater(k) = hwater(rec) + 1e-8 where hwater(rec) > h(k), else h(k)
+// (FlowRouting.f90:80-86, sequential rounding along every path)
+struct FillRegionOp {
+  using Value = double;
+  const RegionLine* line;
+  double* val;
+  __device__ int run(int g, int lane, const ValueCache<double>& vc) const {
+    const int t = lane & 7;
+    const RegionLine* L = line + g;
+    const int d = __ldg(&L->dep[t]);
+    const int q = __ldg(&L->inp[0]);
+    if (lane < 8 && d >= 0) prefetch_l1(line + d);
+    const double hk = ld_l1(val + g);  // h(k), stored by the line builder
+    double v = hk;
+    if (q >= 0) {
+      double hr = 0.0;
+      if (lane == 0) hr = vc.load(val, q);
+      hr = shfl_d(hr, 0);
+      v = hr > hk ? hr + 1.0e-8 : hk;
+    }
+    if (lane == 0) {
+      vc.put(g, v);
+      st_global(val + g, v);
+    }
     return lane < 8 ? d : -1;
   }
 };
@@ -438,13 +577,14 @@ struct RegionPow {
 // (StreamPowerLaw.f90:92-177): hw[g] = (new h, water); each Newton
 // iteration evaluates the eight receivers' powers in parallel, one per lane
 struct SplRegionOp {
+  using Value = double2;
   const RegionLine* line;
   double2* hw;
   RegionPow np;
   double omega;
   int n_is_one;
   int* err;
-  __device__ int run(int g, int lane, int tile, int lr) const {
+  __device__ int run(int g, int lane, const ValueCache<double2>& vc) const {
     const int t = lane & 7;
     const RegionLine* L = line + g;
     const double c = __ldg(&L->c[t]);
@@ -459,9 +599,9 @@ struct SplRegionOp {
     const unsigned present = __ballot_sync(FULL, mine);
     double hq = 0.0, wr = 0.0;
     if (rg >= 0) {
-      if (mine) hq = (q >> lr) == tile ? ld_l1(hw + q).x : ld_l2(hw + q).x;
+      if (mine) hq = vc.load(hw, q).x;
       double w = 0.0;
-      if (lane == 0) w = (rg >> lr) == tile ? ld_l1(hw + rg).y : ld_l2(hw + rg).y;
+      if (lane == 0) w = vc.load(hw, rg).y;
       wr = shfl_d(w, 0);
     }
     if (lane < 8 && d >= 0) prefetch_l1(line + d);
@@ -547,16 +687,21 @@ struct SplRegionOp {
       }
       wk = fmax(wr, hk);
     }
-    if (lane == 0) st_global(hw + g, make_double2(hk, wk));
+    if (lane == 0) {
+      const double2 v = make_double2(hk, wk);
+      vc.put(g, v);
+      st_global(hw + g, v);
+    }
     return lane < 8 ? d : -1;
   }
 };
 
 // Mixed precision: the area in FP32 (values, weights, sums)
 struct AccRegionOpF {
+  using Value = float;
   const RegionLineF* line;
   float* val;
-  __device__ int run(int g, int lane, int tile, int lr) const {
+  __device__ int run(int g, int lane, const ValueCache<float>& vc) const {
     const int t = lane & 7;
     const RegionLineF* L = line + g;
     const float c = __ldg(&L->c[t]);
@@ -564,7 +709,7 @@ struct AccRegionOpF {
     const int q = __ldg(&L->inp[t]);
     const bool mine = lane < 8 && q >= 0;
     float x = 0.0f;
-    if (mine) x = (q >> lr) == tile ? ld_l1f(val + q) : ld_l2f(val + q);
+    if (mine) x = vc.load(val, q);
     if (lane < 8 && d >= 0) prefetch_l1(line + d);
     const float term = x * c;
     const unsigned present = __ballot_sync(FULL, mine);
@@ -574,7 +719,10 @@ struct AccRegionOpF {
       const float v = shfl_f(term, s);
       if ((present >> s) & 1u) acc = acc + v;
     }
-    if (lane == 0) st_globalf(val + g, acc);
+    if (lane == 0) {
+      vc.put(g, acc);
+      st_globalf(val + g, acc);
+    }
     return lane < 8 ? d : -1;
   }
 };
@@ -587,6 +735,7 @@ struct AccRegionOpF {
 // d (x = max(0, ht - hq + d), :146-162) with the reference's tolerance and
 // relaxation.
 struct SplRegionOpM {
+  using Value = double2;
   const RegionLineF* line;
   double2* hw;
   float n;
@@ -594,7 +743,7 @@ struct SplRegionOpM {
   float omega;
   int n_is_one;
   int* err;
-  __device__ int run(int g, int lane, int tile, int lr) const {
+  __device__ int run(int g, int lane, const ValueCache<double2>& vc) const {
     const int t = lane & 7;
     const RegionLineF* L = line + g;
     const float c = __ldg(&L->c[t]);
@@ -609,9 +758,9 @@ struct SplRegionOpM {
     const unsigned present = __ballot_sync(FULL, mine);
     double hq = 0.0, wr = 0.0;
     if (rg >= 0) {
-      if (mine) hq = (q >> lr) == tile ? ld_l1(hw + q).x : ld_l2(hw + q).x;
+      if (mine) hq = vc.load(hw, q).x;
       double w = 0.0;
-      if (lane == 0) w = (rg >> lr) == tile ? ld_l1(hw + rg).y : ld_l2(hw + rg).y;
+      if (lane == 0) w = vc.load(hw, rg).y;
       wr = shfl_d(w, 0);
     }
     if (lane < 8 && dp >= 0) prefetch_l1(line + dp);
@@ -705,7 +854,11 @@ struct SplRegionOpM {
       }
       wk = fmax(wr, hk);
     }
-    if (lane == 0) st_global(hw + g, make_double2(hk, wk));
+    if (lane == 0) {
+      const double2 v = make_double2(hk, wk);
+      vc.put(g, v);
+      st_global(hw + g, v);
+    }
     return lane < 8 ? dp : -1;
   }
 };
@@ -729,6 +882,9 @@ __global__ void __launch_bounds__(kRegionThreads, 2)
   const int R = 1 << lr;
   unsigned* cnt = reinterpret_cast<unsigned*>(smem);                  // R bytes
   unsigned short* q = reinterpret_cast<unsigned short*>(smem + R);    // R entries
+  const int nslots = min(R, kCacheSlots);
+  using V = typename Op::Value;
+  CacheSlot<V>* slots = reinterpret_cast<CacheSlot<V>*>(smem + 3 * R);  // nslots entries
   __shared__ int qhead, qtail, ndone, stop;
   const int tile = blockIdx.x;
   const int gbase = tile << lr;
@@ -745,7 +901,9 @@ __global__ void __launch_bounds__(kRegionThreads, 2)
   for (int w = threadIdx.x; w < R / 4; w += blockDim.x)
     cnt[w] = reinterpret_cast<const unsigned*>(cnt0 + gbase)[w];
   for (int l = threadIdx.x; l < R; l += blockDim.x) q[l] = kQEmpty;
+  for (int l = threadIdx.x; l < nslots; l += blockDim.x) slots[l].tag = -1;
   __syncthreads();
+  const ValueCache<V> vc{slots, nslots - 1, gbase, tile, lr};
   for (int l = threadIdx.x; l < R; l += blockDim.x)
     if (cnt0[gbase + l] == 0) q[atomicAdd(&qtail, 1)] = (unsigned short)l;
   __syncthreads();
@@ -823,7 +981,7 @@ __global__ void __launch_bounds__(kRegionThreads, 2)
       cur = got;
       __threadfence_block();  // acquire: the producers' values
     }
-    const int d = op.run(gbase + cur, lane, tile, lr);
+    const int d = op.run(gbase + cur, lane, vc);
     __syncwarp();
     __threadfence_block();  // release: the node's value before its dependents' counters
     bool ready = false;
@@ -862,6 +1020,18 @@ __global__ void k_untile_area(int nx, int ny, TileMap tm, const T* __restrict__ 
     a[k] = (double)val[tm.g(k % nx, k / nx)];
 }
 
+// hwater and lake_depth (FlowRouting.f90:87-88) in natural order
+__global__ void k_fill_finish_t(int nx, int ny, TileMap tm, const double* __restrict__ val,
+                                const double* __restrict__ h, double* __restrict__ hwater,
+                                double* __restrict__ lake_depth) {
+  const int nn = nx * ny;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const double v = val[tm.g(k % nx, k / nx)];
+    hwater[k] = v;
+    lake_depth[k] = v - h[k];
+  }
+}
+
 // StreamPowerLaw.f90:380-393 with g == 0: b=min(h,b), etot=etot+ht-h,
 // erate=(ht-h)/dt, Sedflux=ht-h, from the tile-major (h, water) pairs
 __global__ void k_spl_finish_t(int nx, int ny, TileMap tm, double dt, const double2* __restrict__ hw,
@@ -879,16 +1049,22 @@ __global__ void k_spl_finish_t(int nx, int ny, TileMap tm, double dt, const doub
 }
 
 
-size_t region_smem(const TileMap& tm) { return (size_t)3 << tm.lr(); }
+template <class Op>
+size_t region_smem(const TileMap& tm) {
+  const size_t R = (size_t)1 << tm.lr();
+  return 3 * R + std::min(R, (size_t)kCacheSlots) * sizeof(CacheSlot<typename Op::Value>);
+}
 
 // whether every tile's CTA of this sweep kernel can be co-resident
 template <class Op>
 bool region_fits(const TileMap& tm) {
-  const size_t smem = region_smem(tm);
+  const size_t smem = region_smem<Op>(tm);
   auto kern = k_region_sweep<Op>;
   // the permitted maximum covers every plan (3 bytes per node, 32768 nodes per
-  // tile), so instances with different plans never undo each other's setting
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * 32768) != cudaSuccess) {
+  // tile, and the value cache), so instances with different plans never undo
+  // each other's setting
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           3 * 32768 + kCacheSlots * (int)sizeof(CacheSlot<typename Op::Value>)) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
@@ -909,7 +1085,7 @@ bool region_usable(Ctx& c) {
     c.region_state = (region_fits<AccRegionOp>(c.tmap) &&
                       region_fits<SplRegionOp>(c.tmap) &&
                       region_fits<AccRegionOpF>(c.tmap) &&
-                      region_fits<SplRegionOpM>(c.tmap))
+                      region_fits<SplRegionOpM>(c.tmap) && region_fits<FillRegionOp>(c.tmap))
                          ? 1
                          : -1;
   return c.region_state > 0;
@@ -919,7 +1095,7 @@ template <class Op>
 bool launch_region(Ctx& c, Op op) {
   const TileMap& tm = c.tmap;
   const int tiles = tm.tiles();
-  const size_t smem = region_smem(tm);
+  const size_t smem = region_smem<Op>(tm);
   auto kern = k_region_sweep<Op>;
   cudaMemsetAsync(c.rl_inbox, 0xff, sizeof(int) * (size_t)tiles * c.rl_icap, c.stream);
   cudaMemsetAsync(c.rl_itail, 0, sizeof(unsigned) * (size_t)tiles, c.stream);
@@ -932,6 +1108,7 @@ bool launch_region(Ctx& c, Op op) {
   TileMap tmv = tm;
   void* args[] = {&op, &tmv, &cnt0, &xcnt, &inbox, &icap, &itail, &err};
   const int timer = std::is_same<Op, AccRegionOp>::value || std::is_same<Op, AccRegionOpF>::value ? KT_AREA_SWEEP
+                    : std::is_same<Op, FillRegionOp>::value                                       ? KT_FILL_SWEEP
                                                                                                   : KT_SPL_SWEEP;
   stage_begin(c, timer);
   const cudaError_t e =
@@ -1022,6 +1199,20 @@ bool region_stream_power(Ctx& c) {
   }
   k_spl_finish_t<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, c.dt, hw, c.h, c.b, c.etot, c.erate,
                                                         c.sedflux);
+  c.count_launch();
+  return true;
+}
+
+bool region_fill(Ctx& c) {
+  if (!region_usable(c)) return false;
+  const TileMap& tm = c.tmap;
+  RegionLine* line = static_cast<RegionLine*>(c.rl_line);
+  cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)tm.padded(), c.stream);
+  k_fill_lines_t<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, c.rec, c.ndon, c.don, c.h, c.size, line,
+                                                        c.rl_val, c.rl_cnt0, c.rl_xcnt);
+  c.count_launch();
+  if (!launch_region<FillRegionOp>(c, FillRegionOp{line, c.rl_val})) return false;
+  k_fill_finish_t<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, c.rl_val, c.h, c.hwater, c.lake_depth);
   c.count_launch();
   return true;
 }

@@ -235,6 +235,7 @@ int stream_power_gs(Ctx& c) {
   }
   double* vol = c.dZ;
   double* up = reinterpret_cast<double*>(c.ch_val);
+  ensure_chains(c);
   lake_volume_chains(c, sill, contrib, vol, up);
   k_gs_finish<<<grid1d(nn), kBlock, 0, st>>>(nn, c.dt, hcur, c.water, sill, lsed, vol, c.h, c.b, c.etot, c.erate,
                                             c.sedflux);
