@@ -32,7 +32,8 @@ namespace fsb {
 
 namespace {
 
-constexpr int kRegionThreads = 256;       // 8 warps: one inbox poller + 7 workers
+// threads of a sweep CTA: warp 0 polls the inbox, the others compute nodes;
+// each op says how many (its register use decides what two CTAs per SM allow)
 constexpr unsigned short kQEmpty = 0xFFFF;
 constexpr unsigned long long kRegionTimeLimitNs = 4000000000ull;  // a sweep giving up: 4 s
 
@@ -497,6 +498,7 @@ struct ValueCache {
 // a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115)
 struct AccRegionOp {
   using Value = double;
+  static constexpr int kThreads = 512;
   const RegionLine* line;
   double* val;
   __device__ int run(int g, int lane, const ValueCache<double>& vc) const {
@@ -529,6 +531,7 @@ struct AccRegionOp {
 // (FlowRouting.f90:80-86, sequential rounding along every path)
 struct FillRegionOp {
   using Value = double;
+  static constexpr int kThreads = 512;
   const RegionLine* line;
   double* val;
   __device__ int run(int g, int lane, const ValueCache<double>& vc) const {
@@ -576,8 +579,10 @@ struct RegionPow {
 // implicit stream power law over the multiple receivers with g == 0
 // (StreamPowerLaw.f90:92-177): hw[g] = (new h, water); each Newton
 // iteration evaluates the eight receivers' powers in parallel, one per lane
+template <bool HALF3>
 struct SplRegionOp {
   using Value = double2;
+  static constexpr int kThreads = HALF3 ? 512 : 256;
   const RegionLine* line;
   double2* hw;
   RegionPow np;
@@ -622,7 +627,7 @@ struct SplRegionOp {
               }
             }
             hk = f / df;
-          } else if (np.half3) {  // n = 1.5: the receivers' square roots in parallel
+          } else if constexpr (HALF3) {  // n = 1.5: the receivers' square roots in parallel
             const double tolp = 1.0e-3;
             double errp = 2.0 * tolp;
             int guard = 0;
@@ -699,6 +704,7 @@ struct SplRegionOp {
 // Mixed precision: the area in FP32 (values, weights, sums)
 struct AccRegionOpF {
   using Value = float;
+  static constexpr int kThreads = 512;
   const RegionLineF* line;
   float* val;
   __device__ int run(int g, int lane, const ValueCache<float>& vc) const {
@@ -734,8 +740,10 @@ struct AccRegionOpF {
 // StreamPowerLaw.f90:108-118 rewritten for the increment; otherwise Newton on
 // d (x = max(0, ht - hq + d), :146-162) with the reference's tolerance and
 // relaxation.
+template <bool HALF3>
 struct SplRegionOpM {
   using Value = double2;
+  static constexpr int kThreads = HALF3 ? 512 : 256;
   const RegionLineF* line;
   double2* hw;
   float n;
@@ -782,7 +790,7 @@ struct SplRegionOpM {
               }
             }
             d = -num / den;
-          } else if (half3) {  // n = 1.5: the receivers' square roots in parallel
+          } else if constexpr (HALF3) {  // n = 1.5: the receivers' square roots in parallel
             const float tolp = 1.0e-3f;
             float errp = 2.0f * tolp;
             int guard = 0;
@@ -874,7 +882,7 @@ struct SplRegionOpM {
 // are done; every wait is bounded by a 4 s limit, after which the sweep
 // reports DEV_SPIN_LIMIT.
 template <class Op>
-__global__ void __launch_bounds__(kRegionThreads, 2)
+__global__ void __launch_bounds__(Op::kThreads, 2)
     k_region_sweep(Op op, TileMap tm, const unsigned char* __restrict__ cnt0, int* xcnt, int* inbox, int icap,
                    unsigned* itail, int* err) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1072,7 +1080,7 @@ bool region_fits(const TileMap& tm) {
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kRegionThreads, smem) != cudaSuccess) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Op::kThreads, smem) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
@@ -1083,9 +1091,10 @@ bool region_usable(Ctx& c) {
   if (!c.region_enabled || c.tmap.ntx == 0) return false;
   if (c.region_state == 0)
     c.region_state = (region_fits<AccRegionOp>(c.tmap) &&
-                      region_fits<SplRegionOp>(c.tmap) &&
+                      region_fits<SplRegionOp<true>>(c.tmap) && region_fits<SplRegionOp<false>>(c.tmap) &&
                       region_fits<AccRegionOpF>(c.tmap) &&
-                      region_fits<SplRegionOpM>(c.tmap) && region_fits<FillRegionOp>(c.tmap))
+                      region_fits<SplRegionOpM<true>>(c.tmap) && region_fits<SplRegionOpM<false>>(c.tmap) &&
+                      region_fits<FillRegionOp>(c.tmap))
                          ? 1
                          : -1;
   return c.region_state > 0;
@@ -1112,7 +1121,7 @@ bool launch_region(Ctx& c, Op op) {
                                                                                                   : KT_SPL_SWEEP;
   stage_begin(c, timer);
   const cudaError_t e =
-      cudaLaunchCooperativeKernel((const void*)kern, dim3(tiles), dim3(kRegionThreads), args, smem, c.stream);
+      cudaLaunchCooperativeKernel((const void*)kern, dim3(tiles), dim3(Op::kThreads), args, smem, c.stream);
   stage_end(c, timer);
   c.count_launch();
   if (e != cudaSuccess) {  // e.g. the GPU is shared and the tiles no longer fit: queue engine
@@ -1185,8 +1194,13 @@ bool region_stream_power(Ctx& c) {
                                                                 c.mnrec, c.mwrec, c.mlrec, c.h, c.b, c.kf, c.a,
                                                                 c.size, line, hw, c.rl_cnt0, c.rl_xcnt, c.d_err);
     c.count_launch();
-    SplRegionOpM op{line, hw, (float)c.n, c.n == 1.5, (float)(0.875 / c.n), n1, c.d_err};
-    if (!launch_region<SplRegionOpM>(c, op)) return false;
+    if (c.n == 1.5) {
+      SplRegionOpM<true> op{line, hw, (float)c.n, 1, (float)(0.875 / c.n), n1, c.d_err};
+      if (!launch_region<SplRegionOpM<true>>(c, op)) return false;
+    } else {
+      SplRegionOpM<false> op{line, hw, (float)c.n, 0, (float)(0.875 / c.n), n1, c.d_err};
+      if (!launch_region<SplRegionOpM<false>>(c, op)) return false;
+    }
   } else {
     RegionLine* line = static_cast<RegionLine*>(c.rl_line);
     k_spl_lines_t<double><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, tm, n1, c.kfsed, c.dt, c.m, c.n, c.rec,
@@ -1194,8 +1208,13 @@ bool region_stream_power(Ctx& c) {
                                                                  c.a, c.size, line, hw, c.rl_cnt0, c.rl_xcnt,
                                                                  c.d_err);
     c.count_launch();
-    SplRegionOp op{line, hw, RegionPow{c.n, c.n == 1.5}, 0.875 / c.n, n1, c.d_err};
-    if (!launch_region<SplRegionOp>(c, op)) return false;
+    if (c.n == 1.5) {
+      SplRegionOp<true> op{line, hw, RegionPow{c.n, 1}, 0.875 / c.n, n1, c.d_err};
+      if (!launch_region<SplRegionOp<true>>(c, op)) return false;
+    } else {
+      SplRegionOp<false> op{line, hw, RegionPow{c.n, 0}, 0.875 / c.n, n1, c.d_err};
+      if (!launch_region<SplRegionOp<false>>(c, op)) return false;
+    }
   }
   k_spl_finish_t<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, c.dt, hw, c.h, c.b, c.etot, c.erate,
                                                         c.sedflux);
