@@ -117,7 +117,7 @@ size_t layout(fsb::Ctx& c, char* base) {
   c.pos = L.take<int>(N); c.size = L.take<int>(N);
   c.mrec = L.take<int>(8 * N); c.mnrec = L.take<int>(N); c.mstack = L.take<int>(N); c.mdmask = L.take<int>(N);
   c.mwrec = L.take<double>(8 * N); c.mlrec = L.take<double>(8 * N);
-  c.ltab = L.take<double>(16);
+  c.ltab = L.take<double>(48);  // 9 lengths; their n-th powers at +16 (double) and +32 (float)
   c.rec_pre = L.take<int>(N); c.stack_pre = L.take<int>(N); c.basins = L.take<int>(N);
   c.length_pre = L.take<double>(N);
   c.s_flag = L.take<int>(N + 1); c.s_scan = L.take<int>(N + 1); c.s_roots = L.take<int>(N);
@@ -317,13 +317,9 @@ int step_once(fsb::Ctx& c) {
     stage_end(c, ST_LOCMIN);
     if (!ok) { g_err = c.err; return 1; }
     stage_begin(c, ST_FILL);
-    // multiple flow with g = 0 fills lakes with the region-owned sweep; the
-    // single-flow sweeps and the sediment term use the chain schedule
-    c.chains_valid = false;
-    if (c.sfd || fsb::gs_active(c) || !fsb::region_fill(c)) {
-      fsb::ensure_chains(c);
-      fsb::fill_sweep(c);
-    }
+    c.chains_valid = false;  // a new forest
+    fsb::ensure_chains(c);
+    fsb::fill_sweep(c);
     stage_end(c, ST_FILL);
     if (!c.sfd) {
       stage_begin(c, ST_MFD);

@@ -693,8 +693,10 @@ static int chain_blocks(int ntickets) {
 void fill_chains(Ctx& c) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_td, c.nchains, c.ntickets_td, c.nn};
+  stage_begin(c, KT_FILL);
   k_fill_chains<<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.h, c.hwater, c.lake_depth, c.ticket,
                                                     c.done, c.epoch, c.d_err);
+  stage_end(c, KT_FILL);
   c.count_launch();
 }
 

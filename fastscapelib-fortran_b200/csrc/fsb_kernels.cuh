@@ -133,7 +133,7 @@ struct Ctx {
   // region-owned sweeps (fsb_region.cu): tile plan and tile-major buffers
   TileMap tmap{};
   bool region_enabled = true;  // use them when the plan and a cooperative launch allow
-  int region_state = 0;        // 0 unchecked, 1 usable, -1 not usable on this device
+  signed char region_ok[8] = {};  // per sweep op: 0 unchecked, 1 usable, -1 not on this device
   void* rl_line = nullptr;     // one 128-byte line per tile-major slot
   double* rl_val = nullptr;    // 2 doubles per slot: area, or (h, water)
   unsigned char* rl_cnt0 = nullptr;  // initial counters, one byte per slot
@@ -165,6 +165,7 @@ struct Ctx {
   // stages: uplift receivers stack locmin fill mfd accum spl diffusion advection;
   // then single kernels inside them: the area sweep, the stream-power sweep,
   // the row and the column tridiagonal solves of the diffusion, the lake fill
+  // sweep
   static constexpr int kStages = 15;
   bool profile = false;
   cudaEvent_t ev_begin[kStages] = {}, ev_end[kStages] = {};
@@ -176,7 +177,7 @@ struct Ctx {
 };
 
 // per-stage / per-kernel CUDA events while profiling is on (fsb_api.cu)
-enum { KT_AREA_SWEEP = 10, KT_SPL_SWEEP = 11, KT_THOMAS_ROWS = 12, KT_THOMAS_COLS = 13, KT_FILL_SWEEP = 14 };
+enum { KT_AREA_SWEEP = 10, KT_SPL_SWEEP = 11, KT_THOMAS_ROWS = 12, KT_THOMAS_COLS = 13, KT_FILL = 14 };
 void stage_begin(Ctx& c, int s);
 void stage_end(Ctx& c, int s);
 
@@ -217,7 +218,6 @@ void flux_mfd(Ctx& c, double* flux);                  // compute_fluxes' flux, m
 TileMap plan_tiles(int nx, int ny, int sms);
 bool region_accumulate(Ctx& c);
 bool region_stream_power(Ctx& c);
-bool region_fill(Ctx& c);  // hwater and lake_depth of the current forest (multiple flow)
 void thomas_lines(Ctx& c, int N, int L, int s0, int s1, const double* A, const double* B, const double* C, double* F,
                   double* G);
 void advect(Ctx& c);  // fsb_advect.cu

@@ -32,8 +32,12 @@ namespace fsb {
 
 namespace {
 
-// threads of a sweep CTA: warp 0 polls the inbox, the others compute nodes;
-// each op says how many (its register use decides what two CTAs per SM allow)
+// Co-resident sweep CTAs per SM the tile plan counts on.  The threads of a
+// sweep CTA (warp 0 polls the inbox, the others compute nodes) are the op's
+// kThreads: 512 where its registers allow two such CTAs per SM -- more
+// worker warps per tile measured faster at 2049^2 (stream-power sweep 32 ->
+// 16 ms against 256 threads).
+constexpr int kRegionCtasPerSm = 2;
 constexpr unsigned short kQEmpty = 0xFFFF;
 constexpr unsigned long long kRegionTimeLimitNs = 4000000000ull;  // a sweep giving up: 4 s
 
@@ -280,6 +284,7 @@ __global__ void k_spl_lines_t(Bounds bd, TileMap tm, int n_is_one, double kfsed,
                               const double* __restrict__ mlrec, const double* __restrict__ h,
                               const double* __restrict__ b, const double* __restrict__ kf,
                               const double* __restrict__ a, const int* __restrict__ prio,
+                              const double* __restrict__ ltab, const T* __restrict__ lpow,
                               RegionLineT<T>* __restrict__ line, double2* __restrict__ hw,
                               unsigned char* __restrict__ cnt0, int* __restrict__ xcnt, int* err) {
   const int nx = bd.nx, ny = bd.ny, nn = nx * ny;
@@ -312,12 +317,16 @@ __global__ void k_spl_lines_t(Bounds bd, TileMap tm, int n_is_one, double kfsed,
       if (n_is_one ? (htk >= h[q]) : (htk > h[q])) {
         const double w = mwrec[o + t], l = mlrec[o + t];
         if (!is_neighbour(i, j, q, nx, ny)) atomicExch(err, DEV_NOT_ADJACENT);
+        // l^n from the table of the nine neighbour lengths (l is one of them)
+        T ln = 0;
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+          if (__ldg(&ltab[e]) == l) ln = __ldg(&lpow[e]);
         if constexpr (sizeof(T) == sizeof(double)) {
-          set_at(fact, nq, n_is_one ? kk * pow(ak * w, m) / l : kk * pow(ak * w, m) / pow(l, n));
+          set_at(fact, nq, n_is_one ? kk * pow(ak * w, m) / l : kk * pow(ak * w, m) / ln);
         } else {  // mixed precision: the erosion factor in FP32
           const float kf32 = (float)kk, aw32 = (float)(ak * w), l32 = (float)l;
-          set_at(fact, nq, n_is_one ? kf32 * powf(aw32, (float)m) / l32
-                                    : kf32 * powf(aw32, (float)m) / powf(l32, (float)n));
+          set_at(fact, nq, n_is_one ? kf32 * powf(aw32, (float)m) / l32 : kf32 * powf(aw32, (float)m) / ln);
         }
         set_at(inp, nq, tm.g(q % nx, q / nx));
         set_at(qv, nq++, q);
@@ -375,47 +384,14 @@ __global__ void k_spl_lines_t(Bounds bd, TileMap tm, int n_is_one, double kfsed,
   }
 }
 
-// Lake fill (FlowRouting.f90:73-89): the only input is rec(k); the
-// dependents are k's donors (the single-flow tree after LocalMinima),
-// largest priority first.  The value array starts as h.
-__global__ void k_fill_lines_t(int nx, int ny, TileMap tm, const int* __restrict__ rec, const int* __restrict__ ndon,
-                               const int* __restrict__ don, const double* __restrict__ h,
-                               const int* __restrict__ prio, RegionLine* __restrict__ line,
-                               double* __restrict__ val, unsigned char* __restrict__ cnt0, int* __restrict__ xcnt) {
-  const int nn = nx * ny;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
-    const int gk = tm.g(k % nx, k / nx);
-    const int r = rec[k];
-    const int nd = ndon[k];
-    int dep[8];
-    unsigned pr[8];
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      dep[t] = -1;
-      pr[t] = 0u;
-    }
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      if (t >= nd) break;
-      const int d = don[(size_t)k * 8 + t];
-      insert_by_priority(dep, pr, t, tm.g(d % nx, d / nx), prio16(prio[d]));
-    }
-    RegionLine L;
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      L.c[t] = 0.0;
-      L.dep[t] = dep[t];
-      L.inp[t] = -1;
-    }
-    int x_in = 0;
-    if (r != k) {
-      L.inp[0] = tm.g(r % nx, r / nx);
-      x_in = (L.inp[0] >> tm.lr()) != (gk >> tm.lr());
-    }
-    line[gk] = L;
-    val[gk] = h[k];
-    cnt0[gk] = (unsigned char)(r != k ? 1 : 0);
-    xcnt[gk] = x_in;
+// l^n for the nine neighbour lengths of find_receiver / find_mult_rec, with
+// the same pow the per-node expression used (so the factors are unchanged)
+__global__ void k_length_pow(const double* __restrict__ ltab, double n, double* __restrict__ lpow,
+                             float* __restrict__ lpowf) {
+  const int e = threadIdx.x;
+  if (e < 9) {
+    lpow[e] = pow(ltab[e], n);
+    lpowf[e] = powf((float)ltab[e], (float)n);
   }
 }
 
@@ -432,76 +408,29 @@ constexpr unsigned FULL = 0xffffffffu;
 __device__ __forceinline__ double shfl_d(double v, int src) { return __shfl_sync(FULL, v, src); }
 __device__ __forceinline__ float shfl_f(float v, int src) { return __shfl_sync(FULL, v, src); }
 
-// Shared-memory cache of the values this CTA's nodes produced, direct-mapped
-// by local index.  A dependent that becomes ready usually reads inputs that
-// its neighbours produced shortly before; from this cache that is a
-// shared-memory access instead of an L2 round trip (global stores do not
-// bring the line into the consumer's L1).  Entries are written under a
-// sequence tag (invalidate, value, tag; CTA-scope fences between), and a
-// read counts only if the tag equals the node before and after the value is
-// read, so an entry being overwritten by another node is a miss, answered
-// from global memory, where every value is stored before its dependents are
-// released.
-template <class V> struct CacheSlot;
-template <> struct CacheSlot<double> { double v; int tag; int pad; };
-template <> struct CacheSlot<float> { float v; int tag; };
-template <> struct CacheSlot<double2> { double x, y; int tag; int pad; };
-constexpr int kCacheSlots = 2048;
-
-__device__ __forceinline__ void read_slot(volatile CacheSlot<double>* e, double& v) { v = e->v; }
-__device__ __forceinline__ void read_slot(volatile CacheSlot<float>* e, float& v) { v = e->v; }
-__device__ __forceinline__ void read_slot(volatile CacheSlot<double2>* e, double2& v) {
-  v.x = e->x;
-  v.y = e->y;
-}
-__device__ __forceinline__ void write_slot(volatile CacheSlot<double>* e, double v) { e->v = v; }
-__device__ __forceinline__ void write_slot(volatile CacheSlot<float>* e, float v) { e->v = v; }
-__device__ __forceinline__ void write_slot(volatile CacheSlot<double2>* e, double2 v) {
-  e->x = v.x;
-  e->y = v.y;
-}
 __device__ __forceinline__ float ld_l1(const float* p) { return ld_l1f(p); }
 __device__ __forceinline__ float ld_l2(const float* p) { return ld_l2f(p); }
 
-template <class V>
-struct ValueCache {
-  CacheSlot<V>* slot;
-  int mask, gbase, tile, lr;
-  __device__ bool get(int g, V& out) const {
-    const int l = g - gbase;
-    volatile CacheSlot<V>* e = slot + (l & mask);
-    if (e->tag != l) return false;
-    __threadfence_block();
-    read_slot(e, out);
-    __threadfence_block();
-    return e->tag == l;
-  }
-  __device__ void put(int g, V v) const {
-    const int l = g - gbase;
-    volatile CacheSlot<V>* e = slot + (l & mask);
-    e->tag = -1;
-    __threadfence_block();
-    write_slot(e, v);
-    __threadfence_block();
-    e->tag = l;
-  }
-  // an input's value: the cache, else global memory (L1 for this tile's
-  // nodes, L2 for other tiles', whose values arrive through the inbox)
+// An input's value: this tile's nodes through L1, other tiles' (which arrive
+// through the inbox, after an acquire at GPU scope) from L2.  Measured on
+// B200: a shared-memory cache of produced values in front of these loads
+// was slower (its fences and the L1 capacity it took cost more than the
+// round trips it saved).
+struct TileLoc {
+  int tile, lr;
+  template <class V>
   __device__ V load(const V* arr, int q) const {
-    if ((q >> lr) != tile) return ld_l2(arr + q);
-    V v;
-    if (get(q, v)) return v;
-    return ld_l1(arr + q);
+    return (q >> lr) == tile ? ld_l1(arr + q) : ld_l2(arr + q);
   }
 };
 
 // a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115)
 struct AccRegionOp {
   using Value = double;
-  static constexpr int kThreads = 512;
+  static constexpr int kThreads = 512, kId = 0;
   const RegionLine* line;
   double* val;
-  __device__ int run(int g, int lane, const ValueCache<double>& vc) const {
+  __device__ int run(int g, int lane, const TileLoc& vc) const {
     const int t = lane & 7;
     const RegionLine* L = line + g;
     const double c = __ldg(&L->c[t]);
@@ -511,6 +440,7 @@ struct AccRegionOp {
     double x = 0.0;
     if (mine) x = vc.load(val, q);
     if (lane < 8 && d >= 0) prefetch_l1(line + d);
+    if (lane >= 8 && lane < 16 && d >= 0) prefetch_l1(val + d);  // the dependent's own entry
     const double term = x * c;
     const unsigned present = __ballot_sync(FULL, mine);
     double acc = ld_l1(val + g);  // dx*dy*precip(k), stored by the line builder
@@ -520,37 +450,7 @@ struct AccRegionOp {
       if ((present >> s) & 1u) acc = acc + v;
     }
     if (lane == 0) {
-      vc.put(g, acc);
       st_global(val + g, acc);
-    }
-    return lane < 8 ? d : -1;
-  }
-};
-
-// hwater(k) = hwater(rec) + 1e-8 where hwater(rec) > h(k), else h(k)
-// (FlowRouting.f90:80-86, sequential rounding along every path)
-struct FillRegionOp {
-  using Value = double;
-  static constexpr int kThreads = 512;
-  const RegionLine* line;
-  double* val;
-  __device__ int run(int g, int lane, const ValueCache<double>& vc) const {
-    const int t = lane & 7;
-    const RegionLine* L = line + g;
-    const int d = __ldg(&L->dep[t]);
-    const int q = __ldg(&L->inp[0]);
-    if (lane < 8 && d >= 0) prefetch_l1(line + d);
-    const double hk = ld_l1(val + g);  // h(k), stored by the line builder
-    double v = hk;
-    if (q >= 0) {
-      double hr = 0.0;
-      if (lane == 0) hr = vc.load(val, q);
-      hr = shfl_d(hr, 0);
-      v = hr > hk ? hr + 1.0e-8 : hk;
-    }
-    if (lane == 0) {
-      vc.put(g, v);
-      st_global(val + g, v);
     }
     return lane < 8 ? d : -1;
   }
@@ -582,14 +482,14 @@ struct RegionPow {
 template <bool HALF3>
 struct SplRegionOp {
   using Value = double2;
-  static constexpr int kThreads = HALF3 ? 512 : 256;
+  static constexpr int kThreads = HALF3 ? 512 : 256, kId = HALF3 ? 1 : 2;
   const RegionLine* line;
   double2* hw;
   RegionPow np;
   double omega;
   int n_is_one;
   int* err;
-  __device__ int run(int g, int lane, const ValueCache<double2>& vc) const {
+  __device__ int run(int g, int lane, const TileLoc& vc) const {
     const int t = lane & 7;
     const RegionLine* L = line + g;
     const double c = __ldg(&L->c[t]);
@@ -610,6 +510,7 @@ struct SplRegionOp {
       wr = shfl_d(w, 0);
     }
     if (lane < 8 && d >= 0) prefetch_l1(line + d);
+    if (lane >= 8 && lane < 16 && d >= 0) prefetch_l1(hw + d);  // the dependent's (ht, rec)
     double hk = ht, wk = ht;
     if (rg >= 0) {
       const double elev = ht;
@@ -694,7 +595,6 @@ struct SplRegionOp {
     }
     if (lane == 0) {
       const double2 v = make_double2(hk, wk);
-      vc.put(g, v);
       st_global(hw + g, v);
     }
     return lane < 8 ? d : -1;
@@ -704,10 +604,10 @@ struct SplRegionOp {
 // Mixed precision: the area in FP32 (values, weights, sums)
 struct AccRegionOpF {
   using Value = float;
-  static constexpr int kThreads = 512;
+  static constexpr int kThreads = 512, kId = 3;
   const RegionLineF* line;
   float* val;
-  __device__ int run(int g, int lane, const ValueCache<float>& vc) const {
+  __device__ int run(int g, int lane, const TileLoc& vc) const {
     const int t = lane & 7;
     const RegionLineF* L = line + g;
     const float c = __ldg(&L->c[t]);
@@ -717,6 +617,7 @@ struct AccRegionOpF {
     float x = 0.0f;
     if (mine) x = vc.load(val, q);
     if (lane < 8 && d >= 0) prefetch_l1(line + d);
+    if (lane >= 8 && lane < 16 && d >= 0) prefetch_l1(val + d);  // the dependent's own entry
     const float term = x * c;
     const unsigned present = __ballot_sync(FULL, mine);
     float acc = ld_l1f(val + g);
@@ -726,7 +627,6 @@ struct AccRegionOpF {
       if ((present >> s) & 1u) acc = acc + v;
     }
     if (lane == 0) {
-      vc.put(g, acc);
       st_globalf(val + g, acc);
     }
     return lane < 8 ? d : -1;
@@ -743,7 +643,7 @@ struct AccRegionOpF {
 template <bool HALF3>
 struct SplRegionOpM {
   using Value = double2;
-  static constexpr int kThreads = HALF3 ? 512 : 256;
+  static constexpr int kThreads = HALF3 ? 512 : 256, kId = HALF3 ? 4 : 5;
   const RegionLineF* line;
   double2* hw;
   float n;
@@ -751,7 +651,7 @@ struct SplRegionOpM {
   float omega;
   int n_is_one;
   int* err;
-  __device__ int run(int g, int lane, const ValueCache<double2>& vc) const {
+  __device__ int run(int g, int lane, const TileLoc& vc) const {
     const int t = lane & 7;
     const RegionLineF* L = line + g;
     const float c = __ldg(&L->c[t]);
@@ -772,6 +672,7 @@ struct SplRegionOpM {
       wr = shfl_d(w, 0);
     }
     if (lane < 8 && dp >= 0) prefetch_l1(line + dp);
+    if (lane >= 8 && lane < 16 && dp >= 0) prefetch_l1(hw + dp);  // the dependent's (ht, rec)
     double hk = ht, wk = ht;
     if (rg >= 0) {
       if (ht > wr) {
@@ -864,7 +765,6 @@ struct SplRegionOpM {
     }
     if (lane == 0) {
       const double2 v = make_double2(hk, wk);
-      vc.put(g, v);
       st_global(hw + g, v);
     }
     return lane < 8 ? dp : -1;
@@ -882,7 +782,7 @@ struct SplRegionOpM {
 // are done; every wait is bounded by a 4 s limit, after which the sweep
 // reports DEV_SPIN_LIMIT.
 template <class Op>
-__global__ void __launch_bounds__(Op::kThreads, 2)
+__global__ void __launch_bounds__(Op::kThreads, kRegionCtasPerSm)
     k_region_sweep(Op op, TileMap tm, const unsigned char* __restrict__ cnt0, int* xcnt, int* inbox, int icap,
                    unsigned* itail, int* err) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -890,9 +790,6 @@ __global__ void __launch_bounds__(Op::kThreads, 2)
   const int R = 1 << lr;
   unsigned* cnt = reinterpret_cast<unsigned*>(smem);                  // R bytes
   unsigned short* q = reinterpret_cast<unsigned short*>(smem + R);    // R entries
-  const int nslots = min(R, kCacheSlots);
-  using V = typename Op::Value;
-  CacheSlot<V>* slots = reinterpret_cast<CacheSlot<V>*>(smem + 3 * R);  // nslots entries
   __shared__ int qhead, qtail, ndone, stop;
   const int tile = blockIdx.x;
   const int gbase = tile << lr;
@@ -909,9 +806,8 @@ __global__ void __launch_bounds__(Op::kThreads, 2)
   for (int w = threadIdx.x; w < R / 4; w += blockDim.x)
     cnt[w] = reinterpret_cast<const unsigned*>(cnt0 + gbase)[w];
   for (int l = threadIdx.x; l < R; l += blockDim.x) q[l] = kQEmpty;
-  for (int l = threadIdx.x; l < nslots; l += blockDim.x) slots[l].tag = -1;
   __syncthreads();
-  const ValueCache<V> vc{slots, nslots - 1, gbase, tile, lr};
+  const TileLoc vc{tile, lr};
   for (int l = threadIdx.x; l < R; l += blockDim.x)
     if (cnt0[gbase + l] == 0) q[atomicAdd(&qtail, 1)] = (unsigned short)l;
   __syncthreads();
@@ -1028,18 +924,6 @@ __global__ void k_untile_area(int nx, int ny, TileMap tm, const T* __restrict__ 
     a[k] = (double)val[tm.g(k % nx, k / nx)];
 }
 
-// hwater and lake_depth (FlowRouting.f90:87-88) in natural order
-__global__ void k_fill_finish_t(int nx, int ny, TileMap tm, const double* __restrict__ val,
-                                const double* __restrict__ h, double* __restrict__ hwater,
-                                double* __restrict__ lake_depth) {
-  const int nn = nx * ny;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
-    const double v = val[tm.g(k % nx, k / nx)];
-    hwater[k] = v;
-    lake_depth[k] = v - h[k];
-  }
-}
-
 // StreamPowerLaw.f90:380-393 with g == 0: b=min(h,b), etot=etot+ht-h,
 // erate=(ht-h)/dt, Sedflux=ht-h, from the tile-major (h, water) pairs
 __global__ void k_spl_finish_t(int nx, int ny, TileMap tm, double dt, const double2* __restrict__ hw,
@@ -1059,8 +943,7 @@ __global__ void k_spl_finish_t(int nx, int ny, TileMap tm, double dt, const doub
 
 template <class Op>
 size_t region_smem(const TileMap& tm) {
-  const size_t R = (size_t)1 << tm.lr();
-  return 3 * R + std::min(R, (size_t)kCacheSlots) * sizeof(CacheSlot<typename Op::Value>);
+  return (size_t)3 << tm.lr();
 }
 
 // whether every tile's CTA of this sweep kernel can be co-resident
@@ -1069,10 +952,8 @@ bool region_fits(const TileMap& tm) {
   const size_t smem = region_smem<Op>(tm);
   auto kern = k_region_sweep<Op>;
   // the permitted maximum covers every plan (3 bytes per node, 32768 nodes per
-  // tile, and the value cache), so instances with different plans never undo
-  // each other's setting
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           3 * 32768 + kCacheSlots * (int)sizeof(CacheSlot<typename Op::Value>)) != cudaSuccess) {
+  // tile), so instances with different plans never undo each other's setting
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * 32768) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
@@ -1087,17 +968,14 @@ bool region_fits(const TileMap& tm) {
   return per_sm * sms >= tm.tiles();
 }
 
+// whether the sweep of op Op can run on the instance's tile plan (checked
+// once per instance and op)
+template <class Op>
 bool region_usable(Ctx& c) {
   if (!c.region_enabled || c.tmap.ntx == 0) return false;
-  if (c.region_state == 0)
-    c.region_state = (region_fits<AccRegionOp>(c.tmap) &&
-                      region_fits<SplRegionOp<true>>(c.tmap) && region_fits<SplRegionOp<false>>(c.tmap) &&
-                      region_fits<AccRegionOpF>(c.tmap) &&
-                      region_fits<SplRegionOpM<true>>(c.tmap) && region_fits<SplRegionOpM<false>>(c.tmap) &&
-                      region_fits<FillRegionOp>(c.tmap))
-                         ? 1
-                         : -1;
-  return c.region_state > 0;
+  signed char& st = c.region_ok[Op::kId];
+  if (st == 0) st = region_fits<Op>(c.tmap) ? 1 : -1;
+  return st > 0;
 }
 
 template <class Op>
@@ -1117,7 +995,6 @@ bool launch_region(Ctx& c, Op op) {
   TileMap tmv = tm;
   void* args[] = {&op, &tmv, &cnt0, &xcnt, &inbox, &icap, &itail, &err};
   const int timer = std::is_same<Op, AccRegionOp>::value || std::is_same<Op, AccRegionOpF>::value ? KT_AREA_SWEEP
-                    : std::is_same<Op, FillRegionOp>::value                                       ? KT_FILL_SWEEP
                                                                                                   : KT_SPL_SWEEP;
   stage_begin(c, timer);
   const cudaError_t e =
@@ -1126,7 +1003,7 @@ bool launch_region(Ctx& c, Op op) {
   c.count_launch();
   if (e != cudaSuccess) {  // e.g. the GPU is shared and the tiles no longer fit: queue engine
     cudaGetLastError();
-    c.region_state = -1;
+    c.region_ok[Op::kId] = -1;
     return false;
   }
   return true;
@@ -1136,12 +1013,12 @@ bool launch_region(Ctx& c, Op op) {
 
 // Tile plan: the smallest tiles of 2^a x 2^b nodes (32 x 32 at least, 32768
 // nodes at most, width >= height) whose count fits the co-resident CTAs
-// (two per SM); none fits -> the queue engine runs.
+// (kRegionCtasPerSm per SM); none fits -> the queue engine runs.
 TileMap plan_tiles(int nx, int ny, int sms) {
   TileMap tm{};
   tm.nx = nx;
   tm.ny = ny;
-  const int max_ctas = 2 * std::max(1, sms);
+  const int max_ctas = kRegionCtasPerSm * std::max(1, sms);
   static const int cand[][2] = {{5, 5}, {6, 5}, {6, 6}, {7, 6}, {7, 7}, {8, 7}};
   for (const auto& cd : cand) {
     const int ntx = (nx + (1 << cd[0]) - 1) >> cd[0], nty = (ny + (1 << cd[1]) - 1) >> cd[1];
@@ -1157,7 +1034,7 @@ TileMap plan_tiles(int nx, int ny, int sms) {
 }
 
 bool region_accumulate(Ctx& c) {
-  if (!region_usable(c)) return false;
+  if (c.mixed ? !region_usable<AccRegionOpF>(c) : !region_usable<AccRegionOp>(c)) return false;
   const TileMap& tm = c.tmap;
   cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)tm.padded(), c.stream);  // padding slots never run
   if (c.mixed) {
@@ -1183,16 +1060,24 @@ bool region_accumulate(Ctx& c) {
 }
 
 bool region_stream_power(Ctx& c) {
-  if (!region_usable(c)) return false;
+  const bool h3 = c.n == 1.5;
+  const bool ok = c.mixed ? (h3 ? region_usable<SplRegionOpM<true>>(c) : region_usable<SplRegionOpM<false>>(c))
+                          : (h3 ? region_usable<SplRegionOp<true>>(c) : region_usable<SplRegionOp<false>>(c));
+  if (!ok) return false;
   const TileMap& tm = c.tmap;
   const int n1 = fabs(c.n - 1.0) < DBL_MIN;
   double2* hw = reinterpret_cast<double2*>(c.rl_val);
   cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)tm.padded(), c.stream);
+  double* lpow = c.ltab + 16;
+  float* lpowf = reinterpret_cast<float*>(c.ltab + 32);
+  k_length_pow<<<1, 32, 0, c.stream>>>(c.ltab, c.n, lpow, lpowf);
+  c.count_launch();
   if (c.mixed) {
     RegionLineF* line = static_cast<RegionLineF*>(c.rl_line);
     k_spl_lines_t<float><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, tm, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec,
                                                                 c.mnrec, c.mwrec, c.mlrec, c.h, c.b, c.kf, c.a,
-                                                                c.size, line, hw, c.rl_cnt0, c.rl_xcnt, c.d_err);
+                                                                c.size, c.ltab, lpowf, line, hw, c.rl_cnt0,
+                                                                c.rl_xcnt, c.d_err);
     c.count_launch();
     if (c.n == 1.5) {
       SplRegionOpM<true> op{line, hw, (float)c.n, 1, (float)(0.875 / c.n), n1, c.d_err};
@@ -1205,8 +1090,8 @@ bool region_stream_power(Ctx& c) {
     RegionLine* line = static_cast<RegionLine*>(c.rl_line);
     k_spl_lines_t<double><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, tm, n1, c.kfsed, c.dt, c.m, c.n, c.rec,
                                                                  c.mrec, c.mnrec, c.mwrec, c.mlrec, c.h, c.b, c.kf,
-                                                                 c.a, c.size, line, hw, c.rl_cnt0, c.rl_xcnt,
-                                                                 c.d_err);
+                                                                 c.a, c.size, c.ltab, lpow, line, hw, c.rl_cnt0,
+                                                                 c.rl_xcnt, c.d_err);
     c.count_launch();
     if (c.n == 1.5) {
       SplRegionOp<true> op{line, hw, RegionPow{c.n, 1}, 0.875 / c.n, n1, c.d_err};
@@ -1218,20 +1103,6 @@ bool region_stream_power(Ctx& c) {
   }
   k_spl_finish_t<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, c.dt, hw, c.h, c.b, c.etot, c.erate,
                                                         c.sedflux);
-  c.count_launch();
-  return true;
-}
-
-bool region_fill(Ctx& c) {
-  if (!region_usable(c)) return false;
-  const TileMap& tm = c.tmap;
-  RegionLine* line = static_cast<RegionLine*>(c.rl_line);
-  cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)tm.padded(), c.stream);
-  k_fill_lines_t<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, c.rec, c.ndon, c.don, c.h, c.size, line,
-                                                        c.rl_val, c.rl_cnt0, c.rl_xcnt);
-  c.count_launch();
-  if (!launch_region<FillRegionOp>(c, FillRegionOp{line, c.rl_val})) return false;
-  k_fill_finish_t<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, c.rl_val, c.h, c.hwater, c.lake_depth);
   c.count_launch();
   return true;
 }

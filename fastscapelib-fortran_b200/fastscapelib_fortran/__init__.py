@@ -123,7 +123,7 @@ _sig("fsb_batch_destroy", _vp)
 STAGES = ("uplift", "receivers", "stack", "local_minima", "lake_fill", "mfd_receivers",
           "drainage_area", "stream_power", "diffusion", "advection",
           # single kernels inside the stages above
-          "k_area_sweep", "k_spl_sweep", "k_thomas_rows", "k_thomas_cols", "k_fill_sweep")
+          "k_area_sweep", "k_spl_sweep", "k_thomas_rows", "k_thomas_cols", "k_fill_chains")
 
 
 def _check(rc: int) -> None:

@@ -183,8 +183,8 @@ long long fsb_launch_count(fsb_ctx* c);
    fill, 5 multiple-flow receivers, 6 drainage area, 7 stream power law,
    8 diffusion, 9 advection; then single kernels inside them: 10 the
    multiple-flow area sweep, 11 the multiple-flow stream-power sweep, 12 and
-   13 the row and column tridiagonal solves of the diffusion, 14 the
-   multiple-flow lake fill sweep.
+   13 the row and column tridiagonal solves of the diffusion, 14 the lake
+   fill sweep.
    fsb_stage_times returns accumulated milliseconds and call counts for the
    first n of these and optionally resets them. */
 int fsb_set_profile(fsb_ctx* c, int on);
