@@ -256,6 +256,25 @@ def stage_bytes(stage, rbar, nconn_per_node, sfd):
     return table[stage]
 
 
+def measured_traffic(kernel, nn):
+    """DRAM bytes per launch of `kernel` (dram__bytes_read.sum + _write.sum),
+    scaled to nn nodes from the per-node figure of the ncu capture committed in
+    profiles/kernel_traffic.json -- but only while the kernel's source file is
+    the one that capture measured (SHA-256 recorded beside the figure)."""
+    import hashlib
+    path = os.path.join(ROOT, "profiles", "kernel_traffic.json")
+    if not os.path.exists(path):
+        return None, "no capture committed"
+    rec = json.load(open(path)).get(kernel)
+    if rec is None:
+        return None, "no capture of this kernel"
+    src = os.path.join(ROOT, rec["source"])
+    sha = hashlib.sha256(open(src, "rb").read()).hexdigest()
+    if sha != rec["source_sha256"]:
+        return None, f"capture of an earlier {rec['source']} (source changed since)"
+    return rec["bytes_per_node"] * nn, f"{rec['capture']}, scaled by nodes"
+
+
 def run_gpu(args):
     import numpy as np
     import torch
@@ -347,20 +366,22 @@ def run_gpu(args):
         mnrec = g.copy_int("mnrec")
         rbar = float(mnrec.mean())
         dbg_nconn = g.locmin_debug()["nconn"]
-        top = max(((k, v) for k, v in stages.items() if not k.startswith("k_")),
-                  key=lambda kv: kv[1][0])
-        name, (tot_ms, calls) = top
+        # the dominant single kernel among the timed ones, with the algorithmic
+        # bytes of the stage it carries (the sweep kernels do that stage's work)
+        kstage = {"k_spl_sweep": "stream_power", "k_area_sweep": "drainage_area",
+                  "k_fill_chains": "lake_fill", "k_thomas_rows": "diffusion", "k_thomas_cols": "diffusion"}
+        ktimes = {k: v for k, v in stages.items() if k in kstage and v[1]}
+        name, (tot_ms, calls) = max(ktimes.items(), key=lambda kv: kv[1][0] / max(kv[1][1], 1))
         per_launch_ms = tot_ms / max(calls, 1)
-        bpn = stage_bytes(name, rbar, dbg_nconn / wl.nn, wl.p < -1.5)
+        bpn = stage_bytes(kstage[name], rbar, dbg_nconn / wl.nn, wl.p < -1.5)
+        if name.startswith("k_thomas"):
+            bpn /= 2.0  # one of the two line passes of the diffusion
         achieved = bpn * wl.nn / (per_launch_ms / 1e3) / 1e9
         peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
         peak, peak_src = 6650.0, "fallback"
         if os.path.exists(peaks_path):
             peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
-        traffic = None
-        tpath = os.path.join(ROOT, "profiles", "dram_traffic.json")
-        if os.path.exists(tpath):
-            traffic = json.load(open(tpath)).get(name)
+        traffic, traffic_note = measured_traffic(name, wl.nn)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -371,7 +392,8 @@ def run_gpu(args):
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
                          "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "bytes_per_node": bpn},
+                         "traffic": traffic, "traffic_source": traffic_note,
+                         "bytes_per_node": bpn, "launch_ms": per_launch_ms},
             "stages_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()
                                    if not k.startswith("k_")},
             "kernels_ms_per_launch": {k: v[0] / max(v[1], 1) for k, v in stages.items()

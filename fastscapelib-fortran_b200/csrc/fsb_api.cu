@@ -162,10 +162,16 @@ size_t layout(fsb::Ctx& c, char* base) {
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaGetLastError();
-    c.tmap = fsb::plan_tiles(c.nx, c.ny, sms);
-    const size_t P = (size_t)std::max(0ll, c.tmap.padded());
-    const int T = c.tmap.tiles();
-    c.rl_icap = c.tmap.ntx ? 2 * ((1 << c.tmap.ltx) + (1 << c.tmap.lty)) + 16 : 0;
+    c.ntplans = fsb::plan_tiles(c.nx, c.ny, sms, c.tplans, fsb::Ctx::kMaxPlans);
+    for (auto& t : c.tplan_of) t = fsb::TileMap{};
+    size_t P = 0;
+    int T = 0;
+    c.rl_icap = 0;
+    for (int i = 0; i < c.ntplans; ++i) {  // buffers for the largest of the candidate plans
+      P = std::max(P, (size_t)c.tplans[i].padded());
+      T = std::max(T, c.tplans[i].tiles());
+      c.rl_icap = std::max(c.rl_icap, 2 * ((1 << c.tplans[i].ltx) + (1 << c.tplans[i].lty)) + 16);
+    }
     c.rl_line = L.take<double>(16 * P);
     c.rl_val = L.take<double>(2 * P);
     c.rl_cnt0 = L.take<unsigned char>(P);

@@ -131,7 +131,10 @@ struct Ctx {
   double* hw = nullptr;      // (elevation, water surface) pairs of the stream-power sweep
   double* slots = nullptr;   // kSlotStride input slots per node of the multiple-flow sweeps
   // region-owned sweeps (fsb_region.cu): tile plan and tile-major buffers
-  TileMap tmap{};
+  static constexpr int kMaxPlans = 3;
+  TileMap tplans[kMaxPlans] = {};  // candidate plans (smallest tiles first)
+  int ntplans = 0;
+  TileMap tplan_of[8] = {};        // per sweep op: the tuned plan (ntx == 0: not yet)
   bool region_enabled = true;  // use them when the plan and a cooperative launch allow
   signed char region_ok[8] = {};  // per sweep op: 0 unchecked, 1 usable, -1 not on this device
   void* rl_line = nullptr;     // one 128-byte line per tile-major slot
@@ -215,7 +218,7 @@ void flux_mfd(Ctx& c, double* flux);                  // compute_fluxes' flux, m
 // tridiagonal systems s0..s1-1, element t of system s at [t*L + s], F solved in place
 // region-owned multiple-flow sweeps (fsb_region.cu); false: not usable, the
 // queue engine of fsb_flow.cu runs instead
-TileMap plan_tiles(int nx, int ny, int sms);
+int plan_tiles(int nx, int ny, int sms, TileMap* out, int max_plans);
 bool region_accumulate(Ctx& c);
 bool region_stream_power(Ctx& c);
 void thomas_lines(Ctx& c, int N, int L, int s0, int s1, const double* A, const double* B, const double* C, double* F,

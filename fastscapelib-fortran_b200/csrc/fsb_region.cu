@@ -24,6 +24,9 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <type_traits>
 
 #include "fsb_kernels.cuh"
@@ -968,19 +971,22 @@ bool region_fits(const TileMap& tm) {
   return per_sm * sms >= tm.tiles();
 }
 
-// whether the sweep of op Op can run on the instance's tile plan (checked
-// once per instance and op)
+// whether the sweep of op Op can run on one of the instance's tile plans
+// (checked once per instance and op)
 template <class Op>
 bool region_usable(Ctx& c) {
-  if (!c.region_enabled || c.tmap.ntx == 0) return false;
+  if (!c.region_enabled || c.ntplans == 0) return false;
   signed char& st = c.region_ok[Op::kId];
-  if (st == 0) st = region_fits<Op>(c.tmap) ? 1 : -1;
+  if (st == 0) {
+    st = -1;
+    for (int i = 0; i < c.ntplans; ++i)
+      if (region_fits<Op>(c.tplans[i])) st = 1;
+  }
   return st > 0;
 }
 
 template <class Op>
-bool launch_region(Ctx& c, Op op) {
-  const TileMap& tm = c.tmap;
+bool launch_region(Ctx& c, Op op, const TileMap& tm) {
   const int tiles = tm.tiles();
   const size_t smem = region_smem<Op>(tm);
   auto kern = k_region_sweep<Op>;
@@ -1001,62 +1007,146 @@ bool launch_region(Ctx& c, Op op) {
       cudaLaunchCooperativeKernel((const void*)kern, dim3(tiles), dim3(Op::kThreads), args, smem, c.stream);
   stage_end(c, timer);
   c.count_launch();
-  if (e != cudaSuccess) {  // e.g. the GPU is shared and the tiles no longer fit: queue engine
+  if (e != cudaSuccess) {  // e.g. the GPU is shared and the tiles no longer fit
     cudaGetLastError();
-    c.region_ok[Op::kId] = -1;
     return false;
   }
   return true;
 }
 
+// ---- the tile-plan tuner ------------------------------------------------------
+// The tile shape decides how a sweep's work is split between co-resident CTAs
+// and how often its critical path crosses a tile boundary; which shape is
+// fastest depends on the grid.  The first sweep of an op on an instance
+// whose grid size has not been seen by the process runs once on each
+// candidate plan (the smallest tiles that fit the co-resident CTAs and up
+// to two coarser ones), timed with CUDA events, and keeps the fastest, also
+// for every later instance of that grid size.  Every run is a complete,
+// correct sweep: a node's arithmetic does not depend on the plan, so each
+// run gives the same values and the last one's output is used.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, std::pair<int, int>> g_tuned;  // (nx, ny, op) -> (ltx, lty)
+
+// Runs run(plan) on the op's tuned plan, tuning first where needed; returns
+// the plan of the last complete run, or nullptr when no plan could run.
+template <class Op, class Run>
+const TileMap* run_tuned(Ctx& c, Run run) {
+  TileMap& chosen = c.tplan_of[Op::kId];
+  if (chosen.ntx == 0) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(std::make_tuple(c.nx, c.ny, Op::kId));
+    if (it != g_tuned.end())
+      for (int i = 0; i < c.ntplans; ++i)
+        if (c.tplans[i].ltx == it->second.first && c.tplans[i].lty == it->second.second) chosen = c.tplans[i];
+  }
+  if (chosen.ntx != 0) {
+    if (run(chosen)) return &chosen;
+    c.region_ok[Op::kId] = -1;  // the queue engine runs from now on
+    return nullptr;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const TileMap* last = nullptr;
+  float best_ms = 0.f;
+  int best = -1;
+  for (int i = 0; i < c.ntplans; ++i) {
+    if (!region_fits<Op>(c.tplans[i])) continue;
+    cudaEventRecord(e0, c.stream);
+    const bool ok = run(c.tplans[i]);
+    cudaEventRecord(e1, c.stream);
+    float ms = 0.f;
+    if (!ok || cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    last = &c.tplans[i];
+    if (best < 0 || ms < best_ms) {
+      best = i;
+      best_ms = ms;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (best < 0) c.region_ok[Op::kId] = -1;  // no plan ran: the queue engine from now on
+  if (best >= 0) {
+    chosen = c.tplans[best];
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[std::make_tuple(c.nx, c.ny, Op::kId)] = std::make_pair(chosen.ltx, chosen.lty);
+  }
+  return last;
+}
+
 }  // namespace
 
-// Tile plan: the smallest tiles of 2^a x 2^b nodes (32 x 32 at least, 32768
-// nodes at most, width >= height) whose count fits the co-resident CTAs
-// (kRegionCtasPerSm per SM); none fits -> the queue engine runs.
-TileMap plan_tiles(int nx, int ny, int sms) {
-  TileMap tm{};
-  tm.nx = nx;
-  tm.ny = ny;
+// Tile plans: tiles of 2^a x 2^b nodes (32 x 32 at least, 32768 nodes at
+// most, width >= height) whose count fits the co-resident CTAs
+// (kRegionCtasPerSm per SM) -- the smallest such tiles and up to two coarser
+// ones, for the tuner.  None fits -> the queue engine runs.
+int plan_tiles(int nx, int ny, int sms, TileMap* out, int max_plans) {
   const int max_ctas = kRegionCtasPerSm * std::max(1, sms);
   static const int cand[][2] = {{5, 5}, {6, 5}, {6, 6}, {7, 6}, {7, 7}, {8, 7}};
+  int n = 0;
   for (const auto& cd : cand) {
     const int ntx = (nx + (1 << cd[0]) - 1) >> cd[0], nty = (ny + (1 << cd[1]) - 1) >> cd[1];
-    if (ntx * nty <= max_ctas) {
+    if (ntx * nty <= max_ctas && n < max_plans) {
+      TileMap& tm = out[n++];
+      tm.nx = nx;
+      tm.ny = ny;
       tm.ltx = cd[0];
       tm.lty = cd[1];
       tm.ntx = ntx;
       tm.nty = nty;
-      return tm;
     }
   }
-  return tm;  // ntx == 0: no plan
+  return n;
 }
 
 bool region_accumulate(Ctx& c) {
-  if (c.mixed ? !region_usable<AccRegionOpF>(c) : !region_usable<AccRegionOp>(c)) return false;
-  const TileMap& tm = c.tmap;
-  cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)tm.padded(), c.stream);  // padding slots never run
   if (c.mixed) {
+    if (!region_usable<AccRegionOpF>(c)) return false;
     RegionLineF* line = static_cast<RegionLineF*>(c.rl_line);
     float* val = reinterpret_cast<float*>(c.rl_val);
-    k_acc_lines_t<float><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, tm, c.dx * c.dy, c.mrec, c.mnrec, c.mwrec,
-                                                                c.precip, c.size, line, val, c.rl_cnt0, c.rl_xcnt,
-                                                                c.d_err);
-    c.count_launch();
-    if (!launch_region<AccRegionOpF>(c, AccRegionOpF{line, val})) return false;
-    k_untile_area<float><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, val, c.a);
+    const TileMap* tm = run_tuned<AccRegionOpF>(c, [&](const TileMap& p) {
+      cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)p.padded(), c.stream);  // padding slots never run
+      k_acc_lines_t<float><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, p, c.dx * c.dy, c.mrec, c.mnrec, c.mwrec,
+                                                                  c.precip, c.size, line, val, c.rl_cnt0, c.rl_xcnt,
+                                                                  c.d_err);
+      c.count_launch();
+      return launch_region<AccRegionOpF>(c, AccRegionOpF{line, val}, p);
+    });
+    if (!tm) return false;
+    k_untile_area<float><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, *tm, val, c.a);
   } else {
+    if (!region_usable<AccRegionOp>(c)) return false;
     RegionLine* line = static_cast<RegionLine*>(c.rl_line);
-    k_acc_lines_t<double><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, tm, c.dx * c.dy, c.mrec, c.mnrec, c.mwrec,
-                                                                 c.precip, c.size, line, c.rl_val, c.rl_cnt0,
-                                                                 c.rl_xcnt, c.d_err);
-    c.count_launch();
-    if (!launch_region<AccRegionOp>(c, AccRegionOp{line, c.rl_val})) return false;
-    k_untile_area<double><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, c.rl_val, c.a);
+    const TileMap* tm = run_tuned<AccRegionOp>(c, [&](const TileMap& p) {
+      cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)p.padded(), c.stream);
+      k_acc_lines_t<double><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, p, c.dx * c.dy, c.mrec, c.mnrec, c.mwrec,
+                                                                   c.precip, c.size, line, c.rl_val, c.rl_cnt0,
+                                                                   c.rl_xcnt, c.d_err);
+      c.count_launch();
+      return launch_region<AccRegionOp>(c, AccRegionOp{line, c.rl_val}, p);
+    });
+    if (!tm) return false;
+    k_untile_area<double><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, *tm, c.rl_val, c.a);
   }
   c.count_launch();
   return true;
+}
+
+template <class Op, class T>
+static const TileMap* spl_sweep(Ctx& c, const Op& op, RegionLineT<T>* line, const T* lpow) {
+  const int n1 = fabs(c.n - 1.0) < DBL_MIN;
+  double2* hw = reinterpret_cast<double2*>(c.rl_val);
+  return run_tuned<Op>(c, [&](const TileMap& p) {
+    cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)p.padded(), c.stream);
+    k_spl_lines_t<T><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, p, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec,
+                                                            c.mnrec, c.mwrec, c.mlrec, c.h, c.b, c.kf, c.a, c.size,
+                                                            c.ltab, lpow, line, hw, c.rl_cnt0, c.rl_xcnt, c.d_err);
+    c.count_launch();
+    return launch_region<Op>(c, op, p);
+  });
 }
 
 bool region_stream_power(Ctx& c) {
@@ -1064,44 +1154,28 @@ bool region_stream_power(Ctx& c) {
   const bool ok = c.mixed ? (h3 ? region_usable<SplRegionOpM<true>>(c) : region_usable<SplRegionOpM<false>>(c))
                           : (h3 ? region_usable<SplRegionOp<true>>(c) : region_usable<SplRegionOp<false>>(c));
   if (!ok) return false;
-  const TileMap& tm = c.tmap;
   const int n1 = fabs(c.n - 1.0) < DBL_MIN;
   double2* hw = reinterpret_cast<double2*>(c.rl_val);
-  cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)tm.padded(), c.stream);
   double* lpow = c.ltab + 16;
   float* lpowf = reinterpret_cast<float*>(c.ltab + 32);
   k_length_pow<<<1, 32, 0, c.stream>>>(c.ltab, c.n, lpow, lpowf);
   c.count_launch();
+  const TileMap* tm;
   if (c.mixed) {
     RegionLineF* line = static_cast<RegionLineF*>(c.rl_line);
-    k_spl_lines_t<float><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, tm, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec,
-                                                                c.mnrec, c.mwrec, c.mlrec, c.h, c.b, c.kf, c.a,
-                                                                c.size, c.ltab, lpowf, line, hw, c.rl_cnt0,
-                                                                c.rl_xcnt, c.d_err);
-    c.count_launch();
-    if (c.n == 1.5) {
-      SplRegionOpM<true> op{line, hw, (float)c.n, 1, (float)(0.875 / c.n), n1, c.d_err};
-      if (!launch_region<SplRegionOpM<true>>(c, op)) return false;
-    } else {
-      SplRegionOpM<false> op{line, hw, (float)c.n, 0, (float)(0.875 / c.n), n1, c.d_err};
-      if (!launch_region<SplRegionOpM<false>>(c, op)) return false;
-    }
+    if (h3)
+      tm = spl_sweep(c, SplRegionOpM<true>{line, hw, (float)c.n, 1, (float)(0.875 / c.n), n1, c.d_err}, line, lpowf);
+    else
+      tm = spl_sweep(c, SplRegionOpM<false>{line, hw, (float)c.n, 0, (float)(0.875 / c.n), n1, c.d_err}, line, lpowf);
   } else {
     RegionLine* line = static_cast<RegionLine*>(c.rl_line);
-    k_spl_lines_t<double><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, tm, n1, c.kfsed, c.dt, c.m, c.n, c.rec,
-                                                                 c.mrec, c.mnrec, c.mwrec, c.mlrec, c.h, c.b, c.kf,
-                                                                 c.a, c.size, c.ltab, lpow, line, hw, c.rl_cnt0,
-                                                                 c.rl_xcnt, c.d_err);
-    c.count_launch();
-    if (c.n == 1.5) {
-      SplRegionOp<true> op{line, hw, RegionPow{c.n, 1}, 0.875 / c.n, n1, c.d_err};
-      if (!launch_region<SplRegionOp<true>>(c, op)) return false;
-    } else {
-      SplRegionOp<false> op{line, hw, RegionPow{c.n, 0}, 0.875 / c.n, n1, c.d_err};
-      if (!launch_region<SplRegionOp<false>>(c, op)) return false;
-    }
+    if (h3)
+      tm = spl_sweep(c, SplRegionOp<true>{line, hw, RegionPow{c.n, 1}, 0.875 / c.n, n1, c.d_err}, line, lpow);
+    else
+      tm = spl_sweep(c, SplRegionOp<false>{line, hw, RegionPow{c.n, 0}, 0.875 / c.n, n1, c.d_err}, line, lpow);
   }
-  k_spl_finish_t<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, tm, c.dt, hw, c.h, c.b, c.etot, c.erate,
+  if (!tm) return false;
+  k_spl_finish_t<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, *tm, c.dt, hw, c.h, c.b, c.etot, c.erate,
                                                         c.sedflux);
   c.count_launch();
   return true;
