@@ -58,9 +58,16 @@ def parse():
     ap.add_argument("--workers", type=int, default=32, help="batch worker streams")
     ap.add_argument("--grids", type=int, default=256, help="batched: number of grids")
     ap.add_argument("--job-steps", type=int, default=100, help="batched: steps per grid")
-    ap.add_argument("--requests", type=int, default=12, help="served: requests per rate")
-    ap.add_argument("--step-scale", type=float, default=0.2,
-                    help="served: scale of the 20..400 steps per request")
+    ap.add_argument("--requests", type=int, default=100, help="served: requests per rate")
+    ap.add_argument("--probe-requests", type=int, default=24,
+                    help="served: requests submitted at once to measure the capacity")
+    ap.add_argument("--loads", default="0.5,0.7,0.85,1.0,1.2",
+                    help="served: arrival rates as fractions of the measured capacity")
+    ap.add_argument("--precision", default="fp64", help="served/batched: fp64, mixed or fp64,mixed")
+    ap.add_argument("--mixed-loads", default=None,
+                    help="served: loads for the mixed form (default: --loads)")
+    ap.add_argument("--step-scale", type=float, default=1.0,
+                    help="served: scale of the 20..400 steps per request (1 = as specified)")
     ap.add_argument("--max-side", type=int, default=4097, help="served: largest grid side")
     ap.add_argument("--mem-budget", type=float, default=150e9, help="device bytes for jobs")
     return ap.parse_args()
@@ -482,24 +489,32 @@ def run_batched(args):
     # starts last and runs alone at the end
     wls.sort(key=lambda w: -w.nn * w.nsteps)
     node_steps = sum(w.nn * w.nsteps for w in wls)
+    forms = {}
+    precs = args.precision.split(",")
+    clocks = ClockSampler(0, clocks_path("clocks_batched.csv"))
     with fs.Batch(workers=args.workers, mem_budget=int(args.mem_budget)) as b:
-        # warm-up: one small job per worker (library, streams, memory pool)
-        b.run([w.job() for w in W.uneven_d8(args.workers, seed=999, nsteps=max(args.warmup, 1),
-                                            lo=129, hi=257)])
-        jobs = [w.job() for w in wls]
-        clocks = ClockSampler(0, clocks_path("clocks_batched.csv"))
-        t0 = time.perf_counter()
-        b.run(jobs)
-        wall = time.perf_counter() - t0
-        clk = clocks.stop()
-    lat = np.array([j.t_end - j.t_submit for j in jobs])
+        for prec in precs:
+            # warm-up: one small job per worker (library, streams, memory pool)
+            b.run([w.job(precision=prec) for w in W.uneven_d8(args.workers, seed=999,
+                                                              nsteps=max(args.warmup, 1),
+                                                              lo=129, hi=257)])
+            jobs = [w.job(precision=prec) for w in wls]
+            t0 = time.perf_counter()
+            b.run(jobs)
+            wall = time.perf_counter() - t0
+            lat = np.array([j.t_end - j.t_submit for j in jobs])
+            forms[prec] = {"value": node_steps / wall, "wall_s": wall,
+                           "job_latency_s": {"p50": float(np.percentile(lat, 50)),
+                                             "p99": float(np.percentile(lat, 99))}}
+    clk = clocks.stop()
     sides = np.array([w.nx for w in wls])
-    value = node_steps / wall
+    value = forms[precs[0]]["value"]
+    lat = np.array([forms[precs[0]]["job_latency_s"]["p50"], forms[precs[0]]["job_latency_s"]["p99"]])
     line = {
-        "metric": "node-steps/s, 256 uneven single-flow grids run concurrently (FP64)",
+        "metric": "node-steps/s, 256 uneven single-flow grids run concurrently",
         "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.job_steps, "warmup": args.warmup,
         "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
+        "dtype": args.precision, "data": "synthetic",
         "config": {"workload": f"uneven_d8 x{len(wls)} (sides {sides.min()}..{sides.max()}, "
                                f"{args.job_steps} steps each, bc=1111, p=-2, per-grid kf,m,n,kd,U)",
                    "grids": len(wls), "total_nodes": int(sum(w.nn for w in wls)),
@@ -509,7 +524,7 @@ def run_batched(args):
         "e2e": {"value": value, "unit": UNIT,
                 "h2d_bytes_per_step": int(sum(4 * 8 * w.nn for w in wls)) // args.job_steps,
                 "d2h_bytes_per_step": int(sum(8 * w.nn for w in wls)) // args.job_steps},
-        "job_latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "job_latency_s": {"p50": float(lat[0]), "p99": float(lat[1])}, "forms": forms,
         "clocks": clk, "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
@@ -530,12 +545,12 @@ def run_served(args):
     def requests(seed):
         return W.served_mfd(args.requests, seed=seed, hi=args.max_side, steps=steps)
 
-    def serve(b, reqs, rate, rng):
+    def serve(b, reqs, rate, rng, prec="fp64"):
         """Submits at Poisson arrival times; returns (latencies, node-steps/s)."""
         gaps = rng.exponential(1.0 / rate, len(reqs)) if rate > 0 else np.zeros(len(reqs))
         arrivals = np.cumsum(gaps) - gaps[0]
         ids = [None] * len(reqs)
-        jobs = [r.job() for r in reqs]
+        jobs = [r.job(precision=prec) for r in reqs]
         t0 = time.perf_counter()
 
         def submitter():
@@ -554,36 +569,44 @@ def run_served(args):
         lat = np.array([j.t_end - j.t_submit for j in jobs])
         return lat, sum(r.nn * r.nsteps for r in reqs) / span
 
-    levels = []
+    forms = {}
+    clocks = ClockSampler(0, clocks_path("clocks_served.csv"))
     with fs.Batch(workers=args.workers, mem_budget=int(args.mem_budget)) as b:
-        b.run([w.job() for w in W.served_mfd(args.workers, seed=999, hi=513, steps=(2, 2))])
-        # capacity: all requests of a probe set at once
-        probe = requests(777)
-        lat, thr = serve(b, probe, 0.0, np.random.default_rng(0))
-        work = np.mean([r.nn * r.nsteps for r in probe])
-        mu = thr / work  # requests per second the GPU completes when saturated
-        clocks = ClockSampler(0, clocks_path("clocks_served.csv"))
-        for lv, frac in enumerate((0.2, 0.4, 0.6, 0.8, 0.95)):
-            rate = frac * mu
-            lat, thr = serve(b, requests(1000 + lv), rate, np.random.default_rng(lv))
-            levels.append({"rate_per_s": rate, "load": frac, "requests": len(lat),
-                           "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-                           "node_steps_per_s": thr})
-        clk = clocks.stop()
-    top = levels[-1]
+        for prec in args.precision.split(","):
+            b.run([w.job(precision=prec) for w in W.served_mfd(args.workers, seed=999, hi=513,
+                                                                steps=(2, 2))])
+            # capacity: a probe set of requests submitted at once
+            probe = W.served_mfd(args.probe_requests, seed=777, hi=args.max_side, steps=steps)
+            _, thr = serve(b, probe, 0.0, np.random.default_rng(0), prec)
+            work = np.mean([r.nn * r.nsteps for r in probe])
+            mu = thr / work  # requests per second the GPU completes when saturated
+            loads = args.loads if prec == "fp64" or not args.mixed_loads else args.mixed_loads
+            levels = []
+            for lv, frac in enumerate(float(x) for x in loads.split(",")):
+                rate = frac * mu
+                lat, thr = serve(b, requests(1000 + lv), rate, np.random.default_rng(lv), prec)
+                levels.append({"rate_per_s": rate, "load": frac, "requests": len(lat),
+                               "p50_s": float(np.percentile(lat, 50)),
+                               "p99_s": float(np.percentile(lat, 99)),
+                               "max_s": float(lat.max()), "node_steps_per_s": thr})
+            forms[prec] = {"capacity_req_per_s": mu, "probe_node_steps_per_s": mu * work,
+                           "levels": levels}
+    clk = clocks.stop()
+    first = forms[args.precision.split(",")[0]]
+    top = max(first["levels"], key=lambda lv: lv["node_steps_per_s"])
     line = {
-        "metric": "served multiple-flow requests: p50/p99 latency (s) and node-steps/s (FP64)",
+        "metric": "served multiple-flow requests: p50/p99 latency (s) and node-steps/s",
         "value": top["node_steps_per_s"], "unit": UNIT, "n_gpus": 1, "steps": None,
         "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"served_mfd: sides 257..{args.max_side}, steps {steps[0]}..{steps[1]}, "
-                               f"{args.requests} Poisson requests per rate, rates = "
-                               f"(0.2..0.95) x saturated capacity {mu:.3f}/s",
-                   "workers": args.workers, "mem_budget": args.mem_budget,
+        "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+        "config": {"workload": f"served_mfd: sides log-uniform 257..{args.max_side} (odd), steps "
+                               f"uniform {steps[0]}..{steps[1]}, p=1.1, n=1.5, bc=1010, "
+                               f"{args.requests} Poisson requests per rate",
+                   "loads": args.loads, "workers": args.workers, "mem_budget": args.mem_budget,
                    "timing": "host wall clock from each arrival to its result"},
         "e2e": {"value": top["node_steps_per_s"], "unit": UNIT, "h2d_bytes_per_step": None,
                 "d2h_bytes_per_step": None},
-        "capacity_req_per_s": mu, "levels": levels, "clocks": clk,
+        "forms": forms, "clocks": clk,
     }
     print(json.dumps(line), flush=True)
 
