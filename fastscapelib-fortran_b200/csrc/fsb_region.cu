@@ -1028,9 +1028,19 @@ bool launch_region(Ctx& c, Op op, const TileMap& tm) {
 // to two coarser ones), timed with CUDA events, and keeps the plan with the
 // fastest run, also for every later instance of that grid size.  Every run is a complete,
 // correct sweep: a node's arithmetic does not depend on the plan, so each
-// run gives the same values and the last one's output is used.
+// run gives the same values and the last one's output is used.  A cached
+// choice applies to a later grid of the same size class when its candidate
+// list holds that tile shape.
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int>, std::pair<int, int>> g_tuned;  // (nx, ny, op) -> (ltx, lty)
+// (size class, aspect class, op) -> (ltx, lty); a size class spans a factor
+// sqrt(2) in nodes, so a stream of requests of many sizes (the served form)
+// tunes once per class, not once per size
+std::map<std::tuple<int, int, int>, std::pair<int, int>> g_tuned;
+std::tuple<int, int, int> tune_key(const Ctx& c, int op) {
+  const int size_class = (int)std::floor(2.0 * std::log2((double)c.nx * (double)c.ny));
+  const int aspect_class = (int)std::lround(std::log2((double)c.nx / (double)c.ny));
+  return std::make_tuple(size_class * 64 + aspect_class, 0, op);
+}
 
 // Runs run(plan) on the op's tuned plan, tuning first where needed; returns
 // the plan of the last complete run, or nullptr when no plan could run.
@@ -1039,7 +1049,7 @@ const TileMap* run_tuned(Ctx& c, Run run) {
   TileMap& chosen = c.tplan_of[Op::kId];
   if (chosen.ntx == 0) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tuned.find(std::make_tuple(c.nx, c.ny, Op::kId));
+    auto it = g_tuned.find(tune_key(c, Op::kId));
     if (it != g_tuned.end())
       for (int i = 0; i < c.ntplans; ++i)
         if (c.tplans[i].ltx == it->second.first && c.tplans[i].lty == it->second.second) chosen = c.tplans[i];
@@ -1082,7 +1092,7 @@ const TileMap* run_tuned(Ctx& c, Run run) {
   if (best >= 0) {
     chosen = c.tplans[best];
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tuned[std::make_tuple(c.nx, c.ny, Op::kId)] = std::make_pair(chosen.ltx, chosen.lty);
+    g_tuned[tune_key(c, Op::kId)] = std::make_pair(chosen.ltx, chosen.lty);
   }
   return last;
 }
