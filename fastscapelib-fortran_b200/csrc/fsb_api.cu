@@ -164,6 +164,7 @@ size_t layout(fsb::Ctx& c, char* base) {
     cudaGetLastError();
     c.ntplans = fsb::plan_tiles(c.nx, c.ny, sms, c.tplans, fsb::Ctx::kMaxPlans);
     for (auto& t : c.tplan_of) t = fsb::TileMap{};
+    for (auto& f : c.tform_of) f = 0;
     size_t P = 0;
     int T = 0;
     c.rl_icap = 0;

@@ -135,6 +135,7 @@ struct Ctx {
   TileMap tplans[kMaxPlans] = {};  // candidate plans (smallest tiles first)
   int ntplans = 0;
   TileMap tplan_of[8] = {};        // per sweep op: the tuned plan (ntx == 0: not yet)
+  int tform_of[8] = {};            // per sweep op: the tuned kernel form (0: one node per warp)
   bool region_enabled = true;  // use them when the plan and a cooperative launch allow
   signed char region_ok[8] = {};  // per sweep op: 0 unchecked, 1 usable, -1 not on this device
   void* rl_line = nullptr;     // one 128-byte line per tile-major slot

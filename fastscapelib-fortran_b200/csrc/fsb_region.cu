@@ -398,18 +398,21 @@ __global__ void k_length_pow(const double* __restrict__ ltab, double n, double* 
   }
 }
 
-// ---- node operations: one warp per node ------------------------------------------
-// A node is computed by a whole warp.  Lane t < 8 holds slot t of the node's
-// line (coefficient, input, dependent), loads input t and forms term t; the
-// node's sums then run over the terms in slot order -- the order of the
-// queue engine in fsb_flow.cu -- with every lane doing the same scalar
-// arithmetic on shuffled terms, so the warp never diverges and the loops over
-// eight slots become one instruction each.  Lane 0 stores the node's value.
-// run() returns the dependent in this lane's slot (-1 for none, and for lanes
-// 8..31).
+// ---- node operations: a warp segment per node -------------------------------------
+// A node is computed by a segment of W = 32 / NPW lanes of a warp (NPW nodes
+// per warp).  Lane t < 8 of the segment holds slot t of the node's line
+// (coefficient, input, dependent), loads input t and forms term t; the
+// node's sums then run over the present slots in slot order -- the order of
+// the queue engine in fsb_flow.cu -- with every lane of the segment doing the
+// same scalar arithmetic on shuffled terms (all eight shuffles issued
+// unconditionally, absent slots masked in the adds: an early exit from the
+// loop serialised the shuffles and measured slower).  All segments of a warp execute
+// the same instruction stream: a segment without a node, or whose node needs
+// fewer Newton iterations, runs along without effect, so warp-collective
+// shuffles and ballots stay convergent.  Lane 0 of a segment stores the
+// node's value.  run() returns the dependent in this lane's slot (-1 for
+// none).
 constexpr unsigned FULL = 0xffffffffu;
-__device__ __forceinline__ double shfl_d(double v, int src) { return __shfl_sync(FULL, v, src); }
-__device__ __forceinline__ float shfl_f(float v, int src) { return __shfl_sync(FULL, v, src); }
 
 __device__ __forceinline__ float ld_l1(const float* p) { return ld_l1f(p); }
 __device__ __forceinline__ float ld_l2(const float* p) { return ld_l2f(p); }
@@ -427,38 +430,72 @@ struct TileLoc {
   }
 };
 
-// a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115)
-struct AccRegionOp {
-  using Value = double;
-  static constexpr int kThreads = 512, kId = 0;
-  const RegionLine* line;
-  double* val;
-  __device__ int run(int g, int lane, const TileLoc& vc) const {
-    const int t = lane & 7;
-    const RegionLine* L = line + g;
-    const double c = __ldg(&L->c[t]);
-    const int d = __ldg(&L->dep[t]);
-    const int q = __ldg(&L->inp[t]);
-    const bool mine = lane < 8 && q >= 0;
-    double x = 0.0;
-    if (mine) x = vc.load(val, q);
-    if (lane < 8 && d >= 0) prefetch_l1(line + d);
-    if (lane >= 8 && lane < 16 && d >= 0) prefetch_l1(val + d);  // the dependent's own entry
-    const double term = x * c;
-    const unsigned present = __ballot_sync(FULL, mine);
-    const int npres = __popc(present);  // slots fill from 0: the present ones are 0..npres-1
-    double acc = ld_l1(val + g);  // dx*dy*precip(k), stored by the line builder
-#pragma unroll
-    for (int s = 0; s < 8; ++s) {
-      if (s >= npres) break;
-      acc = acc + shfl_d(term, s);
+// A lane's segment: its lane within the segment and the segment's first lane.
+struct Seg {
+  int sl, base;
+  __device__ double shfl(double v, int s) const { return __shfl_sync(FULL, v, base + s); }
+  __device__ float shfl(float v, int s) const { return __shfl_sync(FULL, v, base + s); }
+  // bit t: predicate of lane t (< 8) of this segment
+  __device__ unsigned slots(bool p) const { return (__ballot_sync(FULL, p) >> base) & 0xffu; }
+};
+
+// The slot fields of a node's line for this lane (nothing for an idle segment).
+template <class T>
+struct Slot {
+  T c = 0;
+  int d = -1, q = -1;
+  bool owner = false;  // lane < 8 of the segment: the slot is this lane's
+  __device__ Slot(const RegionLineT<T>* line, int g, const Seg& sg) {
+    if (g >= 0) {  // lanes 8.. of a wide segment read the same slots (one line, coalesced)
+      const RegionLineT<T>* L = line + g;
+      const int t = sg.sl & 7;
+      c = __ldg(&L->c[t]);
+      d = __ldg(&L->dep[t]);
+      q = __ldg(&L->inp[t]);
+      owner = sg.sl < 8;
     }
-    if (lane == 0) {
-      st_global(val + g, acc);
-    }
-    return lane < 8 ? d : -1;
+  }
+  // the dependent's line (lanes 0-7) and its own entry (lanes 8-15, or the
+  // same lanes in 8-lane segments) into L1
+  template <class E>
+  __device__ void prefetch(const void* lines, const E* entries, const Seg& sg, int w) const {
+    if (d < 0) return;
+    if (sg.sl < 8) prefetch_l1(reinterpret_cast<const RegionLineT<T>*>(lines) + d);
+    if (w > 8 ? (sg.sl >= 8 && sg.sl < 16) : true) prefetch_l1(entries + d);
   }
 };
+
+// a(k) = dx*dy*precip(k) + sum over donors of a(d)*w(d->k) (FlowRouting.f90:109-115)
+template <class T, int NPW>
+struct AccRegionOpT {
+  using Value = T;
+  static constexpr int kThreads = 512, kNpw = NPW, kId = sizeof(T) == sizeof(double) ? 0 : 3;
+  const RegionLineT<T>* line;
+  T* val;
+  __device__ int run(int g, const Seg& sg, const TileLoc& vc) const {
+    const Slot<T> sl(line, g, sg);
+    const bool mine = sl.owner && sl.q >= 0;
+    T x = 0;
+    if (mine) x = vc.load(val, sl.q);
+    sl.prefetch(line, val, sg, 32 / NPW);
+    const T term = x * sl.c;
+    const unsigned present = sg.slots(mine);
+    const int npres = __popc(present);  // slots fill from 0: the present ones are 0..npres-1
+    T acc = g >= 0 ? ld_l1(val + g) : T(0);  // dx*dy*precip(k), stored by the line builder
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+      const T v = sg.shfl(term, s);
+      if (s < npres) acc = acc + v;
+    }
+    if (g >= 0 && sg.sl == 0) {
+      if constexpr (sizeof(T) == sizeof(double)) st_global(val + g, acc);
+      else st_globalf(val + g, acc);
+    }
+    return sl.owner ? sl.d : -1;
+  }
+};
+template <int NPW> using AccRegionOpN = AccRegionOpT<double, NPW>;
+template <int NPW> using AccRegionOpFN = AccRegionOpT<float, NPW>;
 
 // x^n and x^(n-1) for the Newton update (as NewtonPow in fsb_flow.cu): for
 // n = 1.5 as x*sqrt(x) and sqrt(x); otherwise x*x^(n-1) with one pow for x > 0.
@@ -481,159 +518,127 @@ struct RegionPow {
 };
 
 // implicit stream power law over the multiple receivers with g == 0
-// (StreamPowerLaw.f90:92-177): hw[g] = (new h, water); each Newton
-// iteration evaluates the eight receivers' powers in parallel, one per lane
-template <bool HALF3>
-struct SplRegionOp {
+// (StreamPowerLaw.f90:92-177): hw[g] = (new h, water).  For n = 1.5 each
+// Newton iteration evaluates the receivers' x*sqrt(x) in parallel, one per
+// lane; for other n lane 0 of the segment iterates with pow (a shuffle in a
+// loop with pow does not compile).
+template <bool HALF3, int NPW>
+struct SplRegionOpN {
   using Value = double2;
-  static constexpr int kThreads = HALF3 ? 512 : 256, kId = HALF3 ? 1 : 2;
+  static constexpr int kThreads = HALF3 ? 512 : 256, kNpw = NPW, kId = HALF3 ? 1 : 2;
   const RegionLine* line;
   double2* hw;
   RegionPow np;
   double omega;
   int n_is_one;
   int* err;
-  __device__ int run(int g, int lane, const TileLoc& vc) const {
-    const int t = lane & 7;
-    const RegionLine* L = line + g;
-    const double c = __ldg(&L->c[t]);
-    const int d = __ldg(&L->dep[t]);
-    const int q = __ldg(&L->inp[t]);
-    const double2 self = ld_l1(hw + g);
-    int rg;
-    bool has_mrec;
-    unpack_meta(self.y, rg, has_mrec);
-    const double ht = self.x;
-    const bool mine = lane < 8 && q >= 0;
-    const unsigned present = __ballot_sync(FULL, mine);
-    const int npres = __popc(present);  // slots fill from 0: the present ones are 0..npres-1
-    double hq = 0.0, wr = 0.0;
-    if (rg >= 0) {
-      if (mine) hq = vc.load(hw, q).x;
-      double w = 0.0;
-      if (lane == 0) w = vc.load(hw, rg).y;
-      wr = shfl_d(w, 0);
+  __device__ int run(int g, const Seg& sg, const TileLoc& vc) const {
+    const Slot<double> sl(line, g, sg);
+    int rg = -1;
+    bool has_mrec = false;
+    double ht = 0.0;
+    if (g >= 0) {
+      const double2 self = ld_l1(hw + g);
+      unpack_meta(self.y, rg, has_mrec);
+      ht = self.x;
     }
-    if (lane < 8 && d >= 0) prefetch_l1(line + d);
-    if (lane >= 8 && lane < 16 && d >= 0) prefetch_l1(hw + d);  // the dependent's (ht, rec)
-    double hk = ht, wk = ht;
+    const bool mine = sl.owner && sl.q >= 0;
+    const unsigned present = sg.slots(mine);
+    const int npres = __popc(present);
+    double hq = 0.0, w = 0.0;
     if (rg >= 0) {
-      const double elev = ht;
-      if (elev > wr) {
-        if (has_mrec) {
-          if (n_is_one) {
-            const double tf = c * hq;
-            double f = elev, df = 1.0;
+      if (mine) hq = vc.load(hw, sl.q).x;
+      if (sg.sl == 0) w = vc.load(hw, rg).y;
+    }
+    const double wr = sg.shfl(w, 0);
+    sl.prefetch(line, hw, sg, 32 / NPW);  // the dependent's line and own entry (ht, rec)
+    const double elev = ht;
+    const bool solve = rg >= 0 && elev > wr && has_mrec;
+    double hk = ht;
+    if (n_is_one) {
+      const double tf = sl.c * hq;
+      double f = elev, df = 1.0;
 #pragma unroll
-            for (int s = 0; s < 8; ++s) {
-              if (s >= npres) break;
-              const double a = shfl_d(tf, s), b = shfl_d(c, s);
-              f = f + a;
-              df = df + b;
-            }
-            hk = f / df;
-          } else if constexpr (HALF3) {  // n = 1.5: the receivers' square roots in parallel
-            const double tolp = 1.0e-3;
-            double errp = 2.0 * tolp;
-            int guard = 0;
-            while (errp > tolp) {
-              if (++guard > kNewtonLimit) {
-                if (lane == 0) atomicExch(err, DEV_NEWTON_LIMIT);
-                break;
-              }
-              const double x = fmax(0.0, hk - hq);
-              const double r = sqrt(x);
-              const double tf = c * (x * r), tdf = c * np.n * r;
-              double f = hk - elev, df = 1.0;
+      for (int s = 0; s < 8; ++s) {
+        const double a = sg.shfl(tf, s), b = sg.shfl(sl.c, s);
+        if (s < npres) {
+          f = f + a;
+          df = df + b;
+        }
+      }
+      if (solve) hk = f / df;
+    } else if constexpr (HALF3) {
+      const double tolp = 1.0e-3;
+      bool go = solve;
+      int guard = 0;
+      while (__any_sync(FULL, go)) {
+        if (go && ++guard > kNewtonLimit) {
+          if (sg.sl == 0) atomicExch(err, DEV_NEWTON_LIMIT);
+          go = false;
+        }
+        const double x = fmax(0.0, hk - hq);
+        const double r = sqrt(x);
+        const double tf = sl.c * (x * r), tdf = sl.c * np.n * r;
+        double f = hk - elev, df = 1.0;
 #pragma unroll
-              for (int s = 0; s < 8; ++s) {
-                if (s >= npres) break;
-                const double a = shfl_d(tf, s), b = shfl_d(tdf, s);
-                f = f + a;
-                df = df + b;
-              }
-              const double hn = hk - f / df;
-              errp = fabs(hn - hk);
-              hk = hk * (1.0 - omega) + hn * omega;
-            }
-          } else {  // other n: the slots gathered to lane 0, which iterates with pow
-            double fs[8], qs[8];
-#pragma unroll
-            for (int s = 0; s < 8; ++s) {
-              fs[s] = shfl_d(c, s);
-              qs[s] = shfl_d(hq, s);
-            }
-            if (lane == 0) {
-              const double tolp = 1.0e-3;
-              double errp = 2.0 * tolp;
-              int guard = 0;
-              while (errp > tolp) {
-                if (++guard > kNewtonLimit) {
-                  atomicExch(err, DEV_NEWTON_LIMIT);
-                  break;
-                }
-                double f = hk - elev, df = 1.0;
-#pragma unroll
-                for (int s = 0; s < 8; ++s)
-                  if (s < npres) {
-                    const double x = fmax(0.0, hk - qs[s]);
-                    double pn, pn1;
-                    np.eval(x, pn, pn1);
-                    f = f + fs[s] * pn;
-                    df = df + fs[s] * np.n * pn1;
-                  }
-                const double hn = hk - f / df;
-                errp = fabs(hn - hk);
-                hk = hk * (1.0 - omega) + hn * omega;
-              }
-            }
-            hk = shfl_d(hk, 0);
+        for (int s = 0; s < 8; ++s) {
+          const double a = sg.shfl(tf, s), b = sg.shfl(tdf, s);
+          if (s < npres) {
+            f = f + a;
+            df = df + b;
           }
         }
+        if (go) {
+          const double hn = hk - f / df;
+          const double errp = fabs(hn - hk);
+          hk = hk * (1.0 - omega) + hn * omega;
+          go = errp > tolp;
+        }
+      }
+    } else {
+      double fs[8], qs[8];
+#pragma unroll
+      for (int s = 0; s < 8; ++s) {
+        fs[s] = sg.shfl(sl.c, s);
+        qs[s] = sg.shfl(hq, s);
+      }
+      if (sg.sl == 0 && solve) {
+        const double tolp = 1.0e-3;
+        double errp = 2.0 * tolp;
+        int guard = 0;
+        while (errp > tolp) {
+          if (++guard > kNewtonLimit) {
+            atomicExch(err, DEV_NEWTON_LIMIT);
+            break;
+          }
+          double f = hk - elev, df = 1.0;
+#pragma unroll
+          for (int s = 0; s < 8; ++s)
+            if (s < npres) {
+              const double x = fmax(0.0, hk - qs[s]);
+              double pn, pn1;
+              np.eval(x, pn, pn1);
+              f = f + fs[s] * pn;
+              df = df + fs[s] * np.n * pn1;
+            }
+          const double hn = hk - f / df;
+          errp = fabs(hn - hk);
+          hk = hk * (1.0 - omega) + hn * omega;
+        }
+      }
+      hk = sg.shfl(hk, 0);
+    }
+    double wk = ht;
+    if (rg >= 0) {
+      if (elev > wr) {
         if (hk < wr) hk = wr;
       } else {
         hk = elev;
       }
       wk = fmax(wr, hk);
     }
-    if (lane == 0) {
-      const double2 v = make_double2(hk, wk);
-      st_global(hw + g, v);
-    }
-    return lane < 8 ? d : -1;
-  }
-};
-
-// Mixed precision: the area in FP32 (values, weights, sums)
-struct AccRegionOpF {
-  using Value = float;
-  static constexpr int kThreads = 512, kId = 3;
-  const RegionLineF* line;
-  float* val;
-  __device__ int run(int g, int lane, const TileLoc& vc) const {
-    const int t = lane & 7;
-    const RegionLineF* L = line + g;
-    const float c = __ldg(&L->c[t]);
-    const int d = __ldg(&L->dep[t]);
-    const int q = __ldg(&L->inp[t]);
-    const bool mine = lane < 8 && q >= 0;
-    float x = 0.0f;
-    if (mine) x = vc.load(val, q);
-    if (lane < 8 && d >= 0) prefetch_l1(line + d);
-    if (lane >= 8 && lane < 16 && d >= 0) prefetch_l1(val + d);  // the dependent's own entry
-    const float term = x * c;
-    const unsigned present = __ballot_sync(FULL, mine);
-    const int npres = __popc(present);  // slots fill from 0: the present ones are 0..npres-1
-    float acc = ld_l1f(val + g);
-#pragma unroll
-    for (int s = 0; s < 8; ++s) {
-      if (s >= npres) break;
-      acc = acc + shfl_f(term, s);
-    }
-    if (lane == 0) {
-      st_globalf(val + g, acc);
-    }
-    return lane < 8 ? d : -1;
+    if (g >= 0 && sg.sl == 0) st_global(hw + g, make_double2(hk, wk));
+    return sl.owner ? sl.d : -1;
   }
 };
 
@@ -644,10 +649,10 @@ struct AccRegionOpF {
 // StreamPowerLaw.f90:108-118 rewritten for the increment; otherwise Newton on
 // d (x = max(0, ht - hq + d), :146-162) with the reference's tolerance and
 // relaxation.
-template <bool HALF3>
-struct SplRegionOpM {
+template <bool HALF3, int NPW>
+struct SplRegionOpMN {
   using Value = double2;
-  static constexpr int kThreads = HALF3 ? 512 : 256, kId = HALF3 ? 4 : 5;
+  static constexpr int kThreads = HALF3 ? 512 : 256, kNpw = NPW, kId = HALF3 ? 4 : 5;
   const RegionLineF* line;
   double2* hw;
   float n;
@@ -655,135 +660,140 @@ struct SplRegionOpM {
   float omega;
   int n_is_one;
   int* err;
-  __device__ int run(int g, int lane, const TileLoc& vc) const {
-    const int t = lane & 7;
-    const RegionLineF* L = line + g;
-    const float c = __ldg(&L->c[t]);
-    const int dp = __ldg(&L->dep[t]);
-    const int q = __ldg(&L->inp[t]);
-    const double2 self = ld_l1(hw + g);
-    int rg;
-    bool has_mrec;
-    unpack_meta(self.y, rg, has_mrec);
-    const double ht = self.x;
-    const bool mine = lane < 8 && q >= 0;
-    const unsigned present = __ballot_sync(FULL, mine);
-    const int npres = __popc(present);  // slots fill from 0: the present ones are 0..npres-1
-    double hq = 0.0, wr = 0.0;
-    if (rg >= 0) {
-      if (mine) hq = vc.load(hw, q).x;
-      double w = 0.0;
-      if (lane == 0) w = vc.load(hw, rg).y;
-      wr = shfl_d(w, 0);
+  __device__ int run(int g, const Seg& sg, const TileLoc& vc) const {
+    const Slot<float> sl(line, g, sg);
+    int rg = -1;
+    bool has_mrec = false;
+    double ht = 0.0;
+    if (g >= 0) {
+      const double2 self = ld_l1(hw + g);
+      unpack_meta(self.y, rg, has_mrec);
+      ht = self.x;
     }
-    if (lane < 8 && dp >= 0) prefetch_l1(line + dp);
-    if (lane >= 8 && lane < 16 && dp >= 0) prefetch_l1(hw + dp);  // the dependent's (ht, rec)
+    const bool mine = sl.owner && sl.q >= 0;
+    const unsigned present = sg.slots(mine);
+    const int npres = __popc(present);
+    double hq = 0.0, w = 0.0;
+    if (rg >= 0) {
+      if (mine) hq = vc.load(hw, sl.q).x;
+      if (sg.sl == 0) w = vc.load(hw, rg).y;
+    }
+    const double wr = sg.shfl(w, 0);
+    sl.prefetch(line, hw, sg, 32 / NPW);
+    const bool solve = rg >= 0 && ht > wr && has_mrec;
+    const float dist = mine ? (float)(ht - hq) : 0.0f;
+    float d = 0.0f;
+    if (n_is_one) {
+      const float tf = sl.c * dist;
+      float num = 0.0f, den = 1.0f;
+#pragma unroll
+      for (int s = 0; s < 8; ++s) {
+        const float a = sg.shfl(tf, s), b = sg.shfl(sl.c, s);
+        if (s < npres) {
+          num = num + a;
+          den = den + b;
+        }
+      }
+      d = -num / den;
+    } else if constexpr (HALF3) {
+      const float tolp = 1.0e-3f;
+      bool go = solve;
+      int guard = 0;
+      while (__any_sync(FULL, go)) {
+        if (go && ++guard > kNewtonLimit) {
+          if (sg.sl == 0) atomicExch(err, DEV_NEWTON_LIMIT);
+          go = false;
+        }
+        const float x = fmaxf(0.0f, dist + d);
+        const float r = sqrtf(x);
+        const float tf = sl.c * (x * r), tdf = sl.c * n * r;
+        float f = d, df = 1.0f;
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+          const float a = sg.shfl(tf, s), b = sg.shfl(tdf, s);
+          if (s < npres) {
+            f = f + a;
+            df = df + b;
+          }
+        }
+        if (go) {
+          const float dn = d - f / df;
+          const float errp = fabsf(dn - d);
+          d = d * (1.0f - omega) + dn * omega;
+          go = errp > tolp;
+        }
+      }
+    } else {
+      float fs[8], ds[8];
+#pragma unroll
+      for (int s = 0; s < 8; ++s) {
+        fs[s] = sg.shfl(sl.c, s);
+        ds[s] = sg.shfl(dist, s);
+      }
+      if (sg.sl == 0 && solve) {
+        const float tolp = 1.0e-3f;
+        float errp = 2.0f * tolp;
+        int guard = 0;
+        while (errp > tolp) {
+          if (++guard > kNewtonLimit) {
+            atomicExch(err, DEV_NEWTON_LIMIT);
+            break;
+          }
+          float f = d, df = 1.0f;
+#pragma unroll
+          for (int s = 0; s < 8; ++s)
+            if (s < npres) {
+              const float x = fmaxf(0.0f, ds[s] + d);
+              float pn, pn1;
+              if (x > 0.0f) {
+                pn1 = powf(x, n - 1.0f);
+                pn = x * pn1;
+              } else {
+                pn = powf(x, n);
+                pn1 = powf(x, n - 1.0f);
+              }
+              f = f + fs[s] * pn;
+              df = df + fs[s] * n * pn1;
+            }
+          const float dn = d - f / df;
+          errp = fabsf(dn - d);
+          d = d * (1.0f - omega) + dn * omega;
+        }
+      }
+      d = sg.shfl(d, 0);
+    }
     double hk = ht, wk = ht;
     if (rg >= 0) {
       if (ht > wr) {
-        if (has_mrec) {
-          const float dist = mine ? (float)(ht - hq) : 0.0f;
-          float d = 0.0f;
-          if (n_is_one) {
-            const float tf = c * dist;
-            float num = 0.0f, den = 1.0f;
-#pragma unroll
-            for (int s = 0; s < 8; ++s) {
-              if (s >= npres) break;
-              const float a = shfl_f(tf, s), b = shfl_f(c, s);
-              num = num + a;
-              den = den + b;
-            }
-            d = -num / den;
-          } else if constexpr (HALF3) {  // n = 1.5: the receivers' square roots in parallel
-            const float tolp = 1.0e-3f;
-            float errp = 2.0f * tolp;
-            int guard = 0;
-            while (errp > tolp) {
-              if (++guard > kNewtonLimit) {
-                if (lane == 0) atomicExch(err, DEV_NEWTON_LIMIT);
-                break;
-              }
-              const float x = fmaxf(0.0f, dist + d);
-              const float r = sqrtf(x);
-              const float tf = c * (x * r), tdf = c * n * r;
-              float f = d, df = 1.0f;
-#pragma unroll
-              for (int s = 0; s < 8; ++s) {
-                if (s >= npres) break;
-                const float a = shfl_f(tf, s), b = shfl_f(tdf, s);
-                f = f + a;
-                df = df + b;
-              }
-              const float dn = d - f / df;
-              errp = fabsf(dn - d);
-              d = d * (1.0f - omega) + dn * omega;
-            }
-          } else {  // other n: the slots gathered to lane 0, which iterates with powf
-            float fs[8], ds[8];
-#pragma unroll
-            for (int s = 0; s < 8; ++s) {
-              fs[s] = shfl_f(c, s);
-              ds[s] = shfl_f(dist, s);
-            }
-            if (lane == 0) {
-              const float tolp = 1.0e-3f;
-              float errp = 2.0f * tolp;
-              int guard = 0;
-              while (errp > tolp) {
-                if (++guard > kNewtonLimit) {
-                  atomicExch(err, DEV_NEWTON_LIMIT);
-                  break;
-                }
-                float f = d, df = 1.0f;
-#pragma unroll
-                for (int s = 0; s < 8; ++s)
-                  if (s < npres) {
-                    const float x = fmaxf(0.0f, ds[s] + d);
-                    float pn, pn1;
-                    if (x > 0.0f) {
-                      pn1 = powf(x, n - 1.0f);
-                      pn = x * pn1;
-                    } else {
-                      pn = powf(x, n);
-                      pn1 = powf(x, n - 1.0f);
-                    }
-                    f = f + fs[s] * pn;
-                    df = df + fs[s] * n * pn1;
-                  }
-                const float dn = d - f / df;
-                errp = fabsf(dn - d);
-                d = d * (1.0f - omega) + dn * omega;
-              }
-            }
-            d = shfl_f(d, 0);
-          }
-          hk = ht + (double)d;
-        }
+        if (has_mrec) hk = ht + (double)d;
         if (hk < wr) hk = wr;
       } else {
         hk = ht;
       }
       wk = fmax(wr, hk);
     }
-    if (lane == 0) {
-      const double2 v = make_double2(hk, wk);
-      st_global(hw + g, v);
-    }
-    return lane < 8 ? dp : -1;
+    if (g >= 0 && sg.sl == 0) st_global(hw + g, make_double2(hk, wk));
+    return sl.owner ? sl.d : -1;
   }
 };
+
+// Nodes per warp: each sweep runs as two kernels, one node per warp (the
+// shortest latency per node, best where the critical path dominates) and four
+// per warp (8-lane segments, more nodes in flight, best on large grids); the
+// tuner below picks one per grid size class.  Single-node ops (n != 1.5 SPL)
+// have one form.
+constexpr int kNpwWide = 4;
 
 // ---- the sweep kernel ------------------------------------------------------------
 // One CTA per tile.  Shared memory: the tile's counters (bytes, four per word)
 // and its ready queue (local indices, filled once each, never wrapped).
-// Warp 0's lane 0 polls the tile's inbox; each other warp computes one node
-// at a time: after a node, its lanes release the node's dependents (one per
-// lane), the warp continues with the first one made ready (they come largest
-// priority first) and queues the others.  An idle warp claims the next queue
-// slot and waits for it to be filled.  A CTA ends when all nodes of its tile
-// are done; every wait is bounded by a 4 s limit, after which the sweep
-// reports DEV_SPIN_LIMIT.
+// Warp 0's lane 0 polls the tile's inbox; every other warp computes up to
+// NPW nodes at a time, one per segment: after a node, its lanes release the
+// node's dependents (one per lane), the segment continues with the first one
+// made ready (they come largest priority first) and queues the others.  A
+// segment without a node claims the next queue slot and waits for it to be
+// filled.  A CTA ends when all nodes of its tile are done; every wait is
+// bounded by a 4 s limit, after which the sweep reports DEV_SPIN_LIMIT.
 template <class Op>
 __global__ void __launch_bounds__(Op::kThreads, kRegionCtasPerSm)
     k_region_sweep(Op op, TileMap tm, const unsigned char* __restrict__ cnt0, int* xcnt, int* inbox, int icap,
@@ -864,36 +874,39 @@ __global__ void __launch_bounds__(Op::kThreads, kRegionCtasPerSm)
       __nanosleep(64);
     }
   }
+  constexpr int W = 32 / Op::kNpw;  // lanes per node
+  const Seg sg{lane % W, lane - lane % W};
+  const unsigned segmask = (W == 32 ? 0xffffffffu : ((1u << W) - 1u)) << sg.base;
   int cur = -1, slot = -1, ticks = 0, back = 32;
   for (;;) {
-    if (cur < 0) {
-      int got = -1, quit = 0;
-      if (lane == 0) {
-        if (slot < 0) slot = atomicAdd(&qhead, 1);
-        if (slot < R) {
-          const unsigned short v = *(volatile unsigned short*)&q[slot];
-          if (v != kQEmpty) {
-            got = v;
-            slot = -1;
-          }
+    // segments without a node try their queue slot (the segment's lane 0)
+    int got = -1;
+    if (cur < 0 && sg.sl == 0) {
+      if (slot < 0) slot = atomicAdd(&qhead, 1);
+      if (slot < R) {
+        const unsigned short v = *(volatile unsigned short*)&q[slot];
+        if (v != kQEmpty) {
+          got = v;
+          slot = -1;
         }
-        if (got < 0) quit = *(volatile int*)&ndone >= count || should_stop(ticks);
       }
-      got = __shfl_sync(FULL, got, 0);
-      if (got < 0) {
-        if (__shfl_sync(FULL, quit, 0)) return;
-        // idle warps back off (32 ns doubling to 512 ns): polling warps take
-        // issue slots from the busy ones (stream-power sweep at 2049^2:
-        // 15.9 -> 15.3 ms against a constant 32 ns)
-        __nanosleep(back);
-        if (back < 512) back <<= 1;
-        continue;
-      }
-      back = 32;
-      cur = got;
-      __threadfence_block();  // acquire: the producers' values
     }
-    const int d = op.run(gbase + cur, lane, vc);
+    got = __shfl_sync(FULL, got, sg.base);
+    if (cur < 0) cur = got;
+    if (!__any_sync(FULL, cur >= 0)) {
+      int quit = 0;
+      if (lane == 0) quit = *(volatile int*)&ndone >= count || should_stop(ticks);
+      if (__shfl_sync(FULL, quit, 0)) return;
+      // idle warps back off (32 ns doubling to 512 ns): polling warps take
+      // issue slots from the busy ones (stream-power sweep at 2049^2:
+      // 15.9 -> 15.3 ms against a constant 32 ns)
+      __nanosleep(back);
+      if (back < 512) back <<= 1;
+      continue;
+    }
+    back = 32;
+    __threadfence_block();  // acquire: the producers' values
+    const int d = op.run(cur >= 0 ? gbase + cur : -1, sg, vc);
     __syncwarp();
     __threadfence_block();  // release: the node's value before its dependents' counters
     bool ready = false;
@@ -911,16 +924,13 @@ __global__ void __launch_bounds__(Op::kThreads, kRegionCtasPerSm)
         }
       }
     }
-    const unsigned rm = __ballot_sync(FULL, ready);
-    int nxt = -1;
-    if (rm) {
-      const int first = __ffs(rm) - 1;
-      nxt = __shfl_sync(FULL, d - gbase, first);
-      if (ready && lane != first) push(d - gbase);
-      __threadfence_block();  // acquire for the continuation
-    }
-    if (lane == 0) atomicAdd(&ndone, 1);
-    cur = nxt;
+    const unsigned rm = __ballot_sync(FULL, ready) & segmask;
+    const int first = rm ? __ffs(rm) - 1 : lane;
+    const int nxt_l = __shfl_sync(FULL, d - gbase, first);
+    if (ready && lane != first) push(d - gbase);
+    if (rm) __threadfence_block();  // acquire for the continuation
+    if (sg.sl == 0 && cur >= 0) atomicAdd(&ndone, 1);
+    cur = rm ? nxt_l : -1;
   }
 }
 
@@ -1005,8 +1015,7 @@ bool launch_region(Ctx& c, Op op, const TileMap& tm) {
   int* err = c.d_err;
   TileMap tmv = tm;
   void* args[] = {&op, &tmv, &cnt0, &xcnt, &inbox, &icap, &itail, &err};
-  const int timer = std::is_same<Op, AccRegionOp>::value || std::is_same<Op, AccRegionOpF>::value ? KT_AREA_SWEEP
-                                                                                                  : KT_SPL_SWEEP;
+  const int timer = Op::kId == 0 || Op::kId == 3 ? KT_AREA_SWEEP : KT_SPL_SWEEP;
   stage_begin(c, timer);
   const cudaError_t e =
       cudaLaunchCooperativeKernel((const void*)kern, dim3(tiles), dim3(Op::kThreads), args, smem, c.stream);
@@ -1021,42 +1030,50 @@ bool launch_region(Ctx& c, Op op, const TileMap& tm) {
 
 // ---- the tile-plan tuner ------------------------------------------------------
 // The tile shape decides how a sweep's work is split between co-resident CTAs
-// and how often its critical path crosses a tile boundary; which shape is
-// fastest depends on the grid.  The first sweep of an op on an instance
-// whose grid size has not been seen by the process runs twice on each
-// candidate plan (the smallest tiles that fit the co-resident CTAs and up
-// to two coarser ones), timed with CUDA events, and keeps the plan with the
-// fastest run, also for every later instance of that grid size.  Every run is a complete,
-// correct sweep: a node's arithmetic does not depend on the plan, so each
-// run gives the same values and the last one's output is used.  A cached
-// choice applies to a later grid of the same size class when its candidate
-// list holds that tile shape.
+// and how often its critical path crosses a tile boundary, and the nodes per
+// warp trade latency per node for nodes in flight; which pair is fastest
+// depends on the grid.  The first sweep of an op on an instance whose grid
+// size class has not been seen by the process runs twice on each candidate
+// (every candidate plan -- the smallest tiles that fit the co-resident CTAs
+// and up to two coarser ones -- with each form of the kernel), timed with
+// CUDA events, and keeps the fastest, also for every later instance of that
+// size class.  Every run is a complete, correct sweep: a node's arithmetic
+// depends neither on the plan nor on the form, so each run gives the same
+// values and the last one's output is used.  A cached choice applies to a
+// later grid of the same size class when its candidate list holds that tile
+// shape.
 std::mutex g_tune_mu;
-// (size class, aspect class, op) -> (ltx, lty); a size class spans a factor
-// sqrt(2) in nodes, so a stream of requests of many sizes (the served form)
-// tunes once per class, not once per size
-std::map<std::tuple<int, int, int>, std::pair<int, int>> g_tuned;
+// (size class, aspect class, op) -> (ltx, lty, form); a size class spans a
+// factor sqrt(2) in nodes, so a stream of requests of many sizes (the served
+// form) tunes once per class, not once per size
+std::map<std::tuple<int, int, int>, std::tuple<int, int, int>> g_tuned;
 std::tuple<int, int, int> tune_key(const Ctx& c, int op) {
   const int size_class = (int)std::floor(2.0 * std::log2((double)c.nx * (double)c.ny));
   const int aspect_class = (int)std::lround(std::log2((double)c.nx / (double)c.ny));
   return std::make_tuple(size_class * 64 + aspect_class, 0, op);
 }
 
-// Runs run(plan) on the op's tuned plan, tuning first where needed; returns
-// the plan of the last complete run, or nullptr when no plan could run.
-template <class Op, class Run>
-const TileMap* run_tuned(Ctx& c, Run run) {
-  TileMap& chosen = c.tplan_of[Op::kId];
+// Runs run(plan, form) on op id's tuned plan and form (0 <= form < nforms),
+// tuning first where needed; fits(plan, form) says whether the form's CTAs
+// are co-resident on the plan.  Returns the plan of the last complete run, or
+// nullptr when no plan could run.
+template <class Fits, class Run>
+const TileMap* run_tuned(Ctx& c, int id, int nforms, Fits fits, Run run) {
+  TileMap& chosen = c.tplan_of[id];
+  int& form = c.tform_of[id];
   if (chosen.ntx == 0) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tuned.find(tune_key(c, Op::kId));
-    if (it != g_tuned.end())
+    auto it = g_tuned.find(tune_key(c, id));
+    if (it != g_tuned.end() && std::get<2>(it->second) < nforms)
       for (int i = 0; i < c.ntplans; ++i)
-        if (c.tplans[i].ltx == it->second.first && c.tplans[i].lty == it->second.second) chosen = c.tplans[i];
+        if (c.tplans[i].ltx == std::get<0>(it->second) && c.tplans[i].lty == std::get<1>(it->second)) {
+          chosen = c.tplans[i];
+          form = std::get<2>(it->second);
+        }
   }
   if (chosen.ntx != 0) {
-    if (run(chosen)) return &chosen;
-    c.region_ok[Op::kId] = -1;  // the queue engine runs from now on
+    if (fits(chosen, form) && run(chosen, form)) return &chosen;
+    c.region_ok[id] = -1;  // the queue engine runs from now on
     return nullptr;
   }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1064,37 +1081,87 @@ const TileMap* run_tuned(Ctx& c, Run run) {
   cudaEventCreate(&e1);
   const TileMap* last = nullptr;
   float best_ms = 0.f;
-  int best = -1;
-  for (int i = 0; i < c.ntplans; ++i) {
-    if (!region_fits<Op>(c.tplans[i])) continue;
-    float plan_ms = -1.f;  // the better of two runs of each candidate
-    for (int rep = 0; rep < 2; ++rep) {
-      cudaEventRecord(e0, c.stream);
-      const bool ok = run(c.tplans[i]);
-      cudaEventRecord(e1, c.stream);
-      float ms = 0.f;
-      if (!ok || cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
-        cudaGetLastError();
-        plan_ms = -1.f;
-        break;
+  int best = -1, best_form = 0;
+  for (int i = 0; i < c.ntplans; ++i)
+    for (int f = 0; f < nforms; ++f) {
+      if (!fits(c.tplans[i], f)) continue;
+      float cand_ms = -1.f;  // the better of two runs of each candidate
+      for (int rep = 0; rep < 2; ++rep) {
+        cudaEventRecord(e0, c.stream);
+        const bool ok = run(c.tplans[i], f);
+        cudaEventRecord(e1, c.stream);
+        float ms = 0.f;
+        if (!ok || cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+          cudaGetLastError();
+          cand_ms = -1.f;
+          break;
+        }
+        last = &c.tplans[i];
+        if (cand_ms < 0.f || ms < cand_ms) cand_ms = ms;
       }
-      last = &c.tplans[i];
-      if (plan_ms < 0.f || ms < plan_ms) plan_ms = ms;
+      if (cand_ms >= 0.f && (best < 0 || cand_ms < best_ms)) {
+        best = i;
+        best_form = f;
+        best_ms = cand_ms;
+      }
     }
-    if (plan_ms >= 0.f && (best < 0 || plan_ms < best_ms)) {
-      best = i;
-      best_ms = plan_ms;
-    }
-  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (best < 0) c.region_ok[Op::kId] = -1;  // no plan ran: the queue engine from now on
+  if (best < 0) c.region_ok[id] = -1;  // no plan ran: the queue engine from now on
   if (best >= 0) {
     chosen = c.tplans[best];
+    form = best_form;
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tuned[tune_key(c, Op::kId)] = std::make_pair(chosen.ltx, chosen.lty);
+    g_tuned[tune_key(c, id)] = std::make_tuple(chosen.ltx, chosen.lty, form);
   }
   return last;
+}
+
+// area sweep of value type T on plan p with NPW nodes per warp
+template <class T, int NPW>
+bool acc_run(Ctx& c, const TileMap& p) {
+  using Op = AccRegionOpT<T, NPW>;
+  RegionLineT<T>* line = static_cast<RegionLineT<T>*>(c.rl_line);
+  T* val = reinterpret_cast<T*>(c.rl_val);
+  cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)p.padded(), c.stream);  // padding slots never run
+  k_acc_lines_t<T><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, p, c.dx * c.dy, c.mrec, c.mnrec, c.mwrec, c.precip,
+                                                          c.size, line, val, c.rl_cnt0, c.rl_xcnt, c.d_err);
+  c.count_launch();
+  return launch_region<Op>(c, Op{line, val}, p);
+}
+
+template <class T>
+bool region_accumulate_t(Ctx& c) {
+  using Op1 = AccRegionOpT<T, 1>;
+  using OpW = AccRegionOpT<T, kNpwWide>;
+  if (!region_usable<Op1>(c)) return false;
+  const TileMap* tm = run_tuned(
+      c, Op1::kId, 2, [&](const TileMap& p, int f) { return f ? region_fits<OpW>(p) : region_fits<Op1>(p); },
+      [&](const TileMap& p, int f) { return f ? acc_run<T, kNpwWide>(c, p) : acc_run<T, 1>(c, p); });
+  if (!tm) return false;
+  k_untile_area<T><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, *tm, reinterpret_cast<T*>(c.rl_val), c.a);
+  c.count_launch();
+  return true;
+}
+
+// stream-power sweep: op1 (one node per warp) and opw (its wide form, the
+// same type where the op has one form only: nforms = 1)
+template <class Op1, class OpW, class T>
+const TileMap* spl_sweep(Ctx& c, const Op1& op1, const OpW& opw, int nforms, RegionLineT<T>* line,
+                         const T* lpow) {
+  const int n1 = fabs(c.n - 1.0) < DBL_MIN;
+  double2* hw = reinterpret_cast<double2*>(c.rl_val);
+  return run_tuned(
+      c, Op1::kId, nforms, [&](const TileMap& p, int f) { return f ? region_fits<OpW>(p) : region_fits<Op1>(p); },
+      [&](const TileMap& p, int f) {
+        cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)p.padded(), c.stream);
+        k_spl_lines_t<T><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, p, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec,
+                                                                c.mnrec, c.mwrec, c.mlrec, c.h, c.b, c.kf, c.a,
+                                                                c.size, c.ltab, lpow, line, hw, c.rl_cnt0,
+                                                                c.rl_xcnt, c.d_err);
+        c.count_launch();
+        return f ? launch_region<OpW>(c, opw, p) : launch_region<Op1>(c, op1, p);
+      });
 }
 
 }  // namespace
@@ -1123,56 +1190,13 @@ int plan_tiles(int nx, int ny, int sms, TileMap* out, int max_plans) {
 }
 
 bool region_accumulate(Ctx& c) {
-  if (c.mixed) {
-    if (!region_usable<AccRegionOpF>(c)) return false;
-    RegionLineF* line = static_cast<RegionLineF*>(c.rl_line);
-    float* val = reinterpret_cast<float*>(c.rl_val);
-    const TileMap* tm = run_tuned<AccRegionOpF>(c, [&](const TileMap& p) {
-      cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)p.padded(), c.stream);  // padding slots never run
-      k_acc_lines_t<float><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, p, c.dx * c.dy, c.mrec, c.mnrec, c.mwrec,
-                                                                  c.precip, c.size, line, val, c.rl_cnt0, c.rl_xcnt,
-                                                                  c.d_err);
-      c.count_launch();
-      return launch_region<AccRegionOpF>(c, AccRegionOpF{line, val}, p);
-    });
-    if (!tm) return false;
-    k_untile_area<float><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, *tm, val, c.a);
-  } else {
-    if (!region_usable<AccRegionOp>(c)) return false;
-    RegionLine* line = static_cast<RegionLine*>(c.rl_line);
-    const TileMap* tm = run_tuned<AccRegionOp>(c, [&](const TileMap& p) {
-      cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)p.padded(), c.stream);
-      k_acc_lines_t<double><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, p, c.dx * c.dy, c.mrec, c.mnrec, c.mwrec,
-                                                                   c.precip, c.size, line, c.rl_val, c.rl_cnt0,
-                                                                   c.rl_xcnt, c.d_err);
-      c.count_launch();
-      return launch_region<AccRegionOp>(c, AccRegionOp{line, c.rl_val}, p);
-    });
-    if (!tm) return false;
-    k_untile_area<double><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, *tm, c.rl_val, c.a);
-  }
-  c.count_launch();
-  return true;
-}
-
-template <class Op, class T>
-static const TileMap* spl_sweep(Ctx& c, const Op& op, RegionLineT<T>* line, const T* lpow) {
-  const int n1 = fabs(c.n - 1.0) < DBL_MIN;
-  double2* hw = reinterpret_cast<double2*>(c.rl_val);
-  return run_tuned<Op>(c, [&](const TileMap& p) {
-    cudaMemsetAsync(c.rl_cnt0, 0xff, (size_t)p.padded(), c.stream);
-    k_spl_lines_t<T><<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.bd, p, n1, c.kfsed, c.dt, c.m, c.n, c.rec, c.mrec,
-                                                            c.mnrec, c.mwrec, c.mlrec, c.h, c.b, c.kf, c.a, c.size,
-                                                            c.ltab, lpow, line, hw, c.rl_cnt0, c.rl_xcnt, c.d_err);
-    c.count_launch();
-    return launch_region<Op>(c, op, p);
-  });
+  return c.mixed ? region_accumulate_t<float>(c) : region_accumulate_t<double>(c);
 }
 
 bool region_stream_power(Ctx& c) {
   const bool h3 = c.n == 1.5;
-  const bool ok = c.mixed ? (h3 ? region_usable<SplRegionOpM<true>>(c) : region_usable<SplRegionOpM<false>>(c))
-                          : (h3 ? region_usable<SplRegionOp<true>>(c) : region_usable<SplRegionOp<false>>(c));
+  const bool ok = c.mixed ? (h3 ? region_usable<SplRegionOpMN<true, 1>>(c) : region_usable<SplRegionOpMN<false, 1>>(c))
+                          : (h3 ? region_usable<SplRegionOpN<true, 1>>(c) : region_usable<SplRegionOpN<false, 1>>(c));
   if (!ok) return false;
   const int n1 = fabs(c.n - 1.0) < DBL_MIN;
   double2* hw = reinterpret_cast<double2*>(c.rl_val);
@@ -1181,18 +1205,24 @@ bool region_stream_power(Ctx& c) {
   k_length_pow<<<1, 32, 0, c.stream>>>(c.ltab, c.n, lpow, lpowf);
   c.count_launch();
   const TileMap* tm;
+  const double omega = 0.875 / c.n;
   if (c.mixed) {
     RegionLineF* line = static_cast<RegionLineF*>(c.rl_line);
+    const float nf = (float)c.n, of = (float)omega;
     if (h3)
-      tm = spl_sweep(c, SplRegionOpM<true>{line, hw, (float)c.n, 1, (float)(0.875 / c.n), n1, c.d_err}, line, lpowf);
+      tm = spl_sweep(c, SplRegionOpMN<true, 1>{line, hw, nf, 1, of, n1, c.d_err},
+                     SplRegionOpMN<true, kNpwWide>{line, hw, nf, 1, of, n1, c.d_err}, 2, line, lpowf);
     else
-      tm = spl_sweep(c, SplRegionOpM<false>{line, hw, (float)c.n, 0, (float)(0.875 / c.n), n1, c.d_err}, line, lpowf);
+      tm = spl_sweep(c, SplRegionOpMN<false, 1>{line, hw, nf, 0, of, n1, c.d_err},
+                     SplRegionOpMN<false, 1>{line, hw, nf, 0, of, n1, c.d_err}, 1, line, lpowf);
   } else {
     RegionLine* line = static_cast<RegionLine*>(c.rl_line);
     if (h3)
-      tm = spl_sweep(c, SplRegionOp<true>{line, hw, RegionPow{c.n, 1}, 0.875 / c.n, n1, c.d_err}, line, lpow);
+      tm = spl_sweep(c, SplRegionOpN<true, 1>{line, hw, RegionPow{c.n, 1}, omega, n1, c.d_err},
+                     SplRegionOpN<true, kNpwWide>{line, hw, RegionPow{c.n, 1}, omega, n1, c.d_err}, 2, line, lpow);
     else
-      tm = spl_sweep(c, SplRegionOp<false>{line, hw, RegionPow{c.n, 0}, 0.875 / c.n, n1, c.d_err}, line, lpow);
+      tm = spl_sweep(c, SplRegionOpN<false, 1>{line, hw, RegionPow{c.n, 0}, omega, n1, c.d_err},
+                     SplRegionOpN<false, 1>{line, hw, RegionPow{c.n, 0}, omega, n1, c.d_err}, 1, line, lpow);
   }
   if (!tm) return false;
   k_spl_finish_t<<<grid1d(c.nn), kBlock, 0, c.stream>>>(c.nx, c.ny, *tm, c.dt, hw, c.h, c.b, c.etot, c.erate,
