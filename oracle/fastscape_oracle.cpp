@@ -37,6 +37,16 @@ namespace {
 typedef std::vector<double> dvec;
 typedef std::vector<int> ivec;
 
+// Diagnostic of the n = 1.5 powers (off unless fso_pow15_diag(1) is called):
+// every multiple-flow Newton solve is repeated with x**1.5 and x**0.5 taken
+// as x*sqrt(x) and sqrt(x), the GPU's evaluation, on the same inputs; the
+// reference's result is kept and the differences are counted.
+struct Pow15Diag {
+  bool on = false;
+  long long solves = 0, iters = 0, iter_diff = 0, h_diff = 0;
+  double max_rel = 0.0;
+} g_pow15;
+
 // Fortran tiny(1d0)
 const double TINY = DBL_MIN;
 
@@ -702,7 +712,10 @@ void stream_power_law(Ctx& c) {
                 const double omega = 0.875 / c.n, tolp = 1.e-3;
                 double errp = 2.0 * tolp;
                 const double h0 = elev[ijk];
+                const double hstart = c.h[ijk];
+                long long it = 0;
                 while (errp > tolp) {
+                  ++it;
                   double f = c.h[ijk] - h0, df = 1.0;
                   for (int k = 0; k < nr; ++k)
                     if (ht[ijk] > ht[mr[k]]) {
@@ -714,6 +727,31 @@ void stream_power_law(Ctx& c) {
                   const double hn = c.h[ijk] - f / df;
                   errp = std::fabs(hn - c.h[ijk]);
                   c.h[ijk] = c.h[ijk] * (1.0 - omega) + hn * omega;
+                }
+                if (g_pow15.on && c.n == 1.5) {  // the same solve with x*sqrt(x), sqrt(x)
+                  double hb = hstart, eb = 2.0 * tolp;
+                  long long itb = 0;
+                  while (eb > tolp && itb < 100000) {
+                    ++itb;
+                    double f = hb - h0, df = 1.0;
+                    for (int k = 0; k < nr; ++k)
+                      if (ht[ijk] > ht[mr[k]]) {
+                        const double fact = kfint[ijk] * c.dt * std::pow(c.a[ijk] * mw[k], c.m) / std::pow(ml[k], c.n);
+                        const double x = std::max(0.0, hb - c.h[mr[k]]);
+                        const double r = std::sqrt(x);
+                        f = f + fact * (x * r);
+                        df = df + fact * c.n * r;
+                      }
+                    const double hn = hb - f / df;
+                    eb = std::fabs(hn - hb);
+                    hb = hb * (1.0 - omega) + hn * omega;
+                  }
+                  g_pow15.solves += 1;
+                  g_pow15.iters += it;
+                  g_pow15.iter_diff += itb != it;
+                  g_pow15.h_diff += hb != c.h[ijk];
+                  const double rel = std::fabs(hb - c.h[ijk]) / std::max(std::fabs(c.h[ijk]), 1.0);
+                  if (rel > g_pow15.max_rel) g_pow15.max_rel = rel;
                 }
               }
             }
@@ -945,6 +983,24 @@ extern "C" {
 const char* fso_last_error() { return C->err.c_str(); }
 
 // FastScape_Init -- FastScape_api.f90:146 -> FastScape_ctx.f90:40-53
+// on != 0: start the n = 1.5 power diagnostic (counters reset); out (may be
+// null) receives solves, total iterations, solves whose iteration count
+// differs, solves whose result differs, and the largest relative difference
+int fso_pow15_diag(int on, double* out) {
+  if (out) {
+    out[0] = (double)g_pow15.solves;
+    out[1] = (double)g_pow15.iters;
+    out[2] = (double)g_pow15.iter_diff;
+    out[3] = (double)g_pow15.h_diff;
+    out[4] = g_pow15.max_rel;
+  }
+  if (on >= 0) {
+    g_pow15 = Pow15Diag();
+    g_pow15.on = on != 0;
+  }
+  return 0;
+}
+
 int fso_init() {
   g_ctx = Ctx();
   return 0;

@@ -48,6 +48,7 @@ def lib():
         L.fso_set_nx_ny.argtypes = [ctypes.c_int, ctypes.c_int]
         L.fso_set_xl_yl.argtypes = [ctypes.c_double, ctypes.c_double]
         L.fso_set_dt.argtypes = [ctypes.c_double]
+        L.fso_pow15_diag.argtypes = [ctypes.c_int, ctypes.c_void_p]
         L.fso_set_erosional_parameters.argtypes = [
             _F64P, ctypes.c_double, ctypes.c_double, ctypes.c_double, _F64P,
             ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double]
@@ -188,6 +189,16 @@ def copy_slots(name: str) -> np.ndarray:
     out = np.empty((_nn(), 8), dtype=dt)
     _check(lib().fso_copy_slots(fid, out.ctypes.data))
     return out
+
+
+def pow15_diag(on=None) -> dict:
+    """Counters of the n = 1.5 power diagnostic (every multiple-flow Newton
+    solve repeated with x*sqrt(x) and sqrt(x) for x**1.5 and x**0.5).
+    on=True/False starts/stops it (and resets the counters); None reads."""
+    out = np.zeros(5, dtype=np.float64)
+    lib().fso_pow15_diag(-1 if on is None else int(bool(on)), out.ctypes.data)
+    return {"solves": int(out[0]), "iterations": int(out[1]), "iteration_count_differs": int(out[2]),
+            "result_differs": int(out[3]), "max_rel_diff": float(out[4])}
 
 
 def locmin_debug() -> dict:
