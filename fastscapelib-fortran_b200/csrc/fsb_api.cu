@@ -123,6 +123,10 @@ size_t layout(fsb::Ctx& c, char* base) {
   c.s_flag = L.take<int>(N + 1); c.s_scan = L.take<int>(N + 1); c.s_roots = L.take<int>(N);
   c.s_root_rank = L.take<int>(N);
   c.s_list_a = L.take<unsigned long long>(2 * N); c.s_list_b = L.take<unsigned long long>(2 * N);
+  c.s_rank_sa = L.take<unsigned long long>(fsb::rank_splitter_cap(2 * N));
+  c.s_rank_sb = L.take<unsigned long long>(fsb::rank_splitter_cap(2 * N));
+  c.s_rank_nheads = L.take<unsigned>(1);
+  c.s_rank_pred = L.take<unsigned char>(2 * N + fsb::kRankStride);  // whole 16-byte flag groups
   c.ht_key = L.take<unsigned long long>(hcap); c.ht_wmin = L.take<unsigned long long>(hcap);
   c.ht_first = L.take<unsigned>(hcap); c.ht_best = L.take<unsigned>(hcap);
   c.e_b1 = L.take<int>(E); c.e_b2 = L.take<int>(E); c.e_n1 = L.take<int>(E); c.e_n2 = L.take<int>(E);

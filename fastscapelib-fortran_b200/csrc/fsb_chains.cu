@@ -105,6 +105,40 @@ __global__ void k_hf_offsets(int nn, const int* __restrict__ rec, const int* __r
   }
 }
 
+// Path sums of the heavy-first offsets over the receiver forest without
+// pointer jumping: node k's subtree is the interval [pos(k), pos(k) + size(k))
+// of the DFS preorder, so adding w(k) at pos(k) and subtracting it at
+// pos(k) + size(k) makes the prefix sum at pos(k) the sum over k's ancestors
+// and k.  w = (light flag << 27) | offset: offsets sum to a heavy-first
+// position (< nn <= 2^27) and light flags to a light depth (< 32), so the
+// two fields never carry into each other; the marks wrap modulo 2^32 and
+// cancel exactly.
+constexpr int kPathOffBits = 27;
+
+__global__ void k_path_marks(int nn, const unsigned long long* __restrict__ val, const int* __restrict__ pos,
+                             const int* __restrict__ size, unsigned* __restrict__ marks, int* __restrict__ err) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const unsigned long long v = val[k];
+    const unsigned w = ((unsigned)(v >> 32) << kPathOffBits) | (unsigned)v;
+    const int p = pos[k], e = p + size[k];
+    if (p < 0 || e > nn || e <= p) {
+      atomicExch(err, DEV_STACK_ERROR);
+      continue;
+    }
+    atomicAdd(&marks[p], w);
+    atomicAdd(&marks[e], 0u - w);
+  }
+}
+
+// after an exclusive scan of the marks: the path sum of k (light depth in the high word)
+__global__ void k_path_take(int nn, const int* __restrict__ pos, const unsigned* __restrict__ scan,
+                            unsigned long long* __restrict__ out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const unsigned s = scan[pos[k] + 1];
+    out[k] = ((unsigned long long)(s >> kPathOffBits) << 32) | (s & ((1u << kPathOffBits) - 1u));
+  }
+}
+
 // one synchronous pointer-jumping round of the path sums
 __global__ void k_path_jump(int nn, const unsigned long long* __restrict__ vin, const int* __restrict__ nin,
                             unsigned long long* __restrict__ vout, int* __restrict__ nout, int* __restrict__ flag) {
@@ -621,19 +655,32 @@ void build_chains(Ctx& c) {
                                               c.ch_tmp2, c.ch_val, c.ch_nxt);
   c.count_launch();
   unsigned long long *va = c.ch_val, *vb = c.ch_val2;
-  int *na = c.ch_nxt, *nb = c.ch_nxt2;
-  // pointer jumping; the flag read back every 4 rounds says whether any
-  // pointer moved in them (rounds after convergence change nothing)
-  for (int round = 0; round < 20; ++round) {
-    cudaMemsetAsync(c.d_cnt + 16, 0, sizeof(int), st);
-    for (int r = 0; r < 4; ++r) {
-      k_path_jump<<<grid1d(nn), kBlock, 0, st>>>(nn, va, na, vb, nb, c.d_cnt + 16);
-      std::swap(va, vb);
-      std::swap(na, nb);
+  if ((size_t)nn < ((size_t)1 << kPathOffBits)) {
+    // a scan over the DFS preorder of the current forest (pos, size)
+    unsigned* marks = reinterpret_cast<unsigned*>(c.ch_tmp);
+    unsigned* scan = reinterpret_cast<unsigned*>(c.ch_tmp2);
+    cudaMemsetAsync(marks, 0, sizeof(unsigned) * (nn + 1), st);
+    k_path_marks<<<grid1d(nn), kBlock, 0, st>>>(nn, va, c.pos, c.size, marks, c.d_err);
+    c.count_launch();
+    exclusive_scan_u32(c, marks, scan, nn + 1);
+    k_path_take<<<grid1d(nn), kBlock, 0, st>>>(nn, c.pos, scan, vb);
+    c.count_launch();
+    std::swap(va, vb);
+  } else {
+    int *na = c.ch_nxt, *nb = c.ch_nxt2;
+    // pointer jumping; the flag read back every 4 rounds says whether any
+    // pointer moved in them (rounds after convergence change nothing)
+    for (int round = 0; round < 20; ++round) {
+      cudaMemsetAsync(c.d_cnt + 16, 0, sizeof(int), st);
+      for (int r = 0; r < 4; ++r) {
+        k_path_jump<<<grid1d(nn), kBlock, 0, st>>>(nn, va, na, vb, nb, c.d_cnt + 16);
+        std::swap(va, vb);
+        std::swap(na, nb);
+      }
+      c.count_launch(4);
+      fetch_counters(c, 20);
+      if (!c.h_cnt[16]) break;
     }
-    c.count_launch(4);
-    fetch_counters(c, 20);
-    if (!c.h_cnt[16]) break;
   }
   k_hf_order<<<grid1d(nn), kBlock, 0, st>>>(nn, va, c.rec, c.ch_heavy, c.ch_ord, c.ch_pos, c.ch_ldep, c.d_err);
   k_chain_flags<<<grid1d(nn + 1), kBlock, 0, st>>>(nn, c.ch_ord, c.rec, c.ch_heavy, c.ch_tmp);

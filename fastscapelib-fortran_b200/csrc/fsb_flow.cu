@@ -573,6 +573,14 @@ struct SplMfdOp {
 // MIXED: the receivers (FP64 comparisons of the filled surface) are the
 // same; the slopes, their powers and the normalisation run in FP32 (the
 // height differences are taken in FP64 and rounded once).
+// a[n] = v for a register array (n in 0..7; no local-memory indexing)
+template <class T>
+__device__ inline void put8(T (&a)[8], int n, T v) {
+#pragma unroll
+  for (int t = 0; t < 8; ++t)
+    if (t == n) a[t] = v;
+}
+
 template <bool MIXED>
 __global__ void k_mfd_receivers(Bounds bd, double p, const double* __restrict__ h0, const double* __restrict__ ltab,
                                 int* __restrict__ mrec, int* __restrict__ mnrec, double* __restrict__ mwrec,
@@ -581,19 +589,29 @@ __global__ void k_mfd_receivers(Bounds bd, double p, const double* __restrict__ 
   for (int ij = blockIdx.x * blockDim.x + threadIdx.x; ij < nn; ij += gridDim.x * blockDim.x) {
     const int i = ij % nx, j = ij / nx;
     int nr = 0;
-    double w[8];
+    int rr[8];
+    double w[8], ll[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      rr[t] = -1;
+      w[t] = 0.0;
+      ll[t] = 0.0;
+    }
     if (i >= bd.i1 && i <= bd.i2 && j >= bd.j1 && j <= bd.j2) {
       const double hij = h0[ij];
+#pragma unroll
       for (int jj = -1; jj <= 1; ++jj) {
         const int jjj = wrap_clamp(j + jj, ny, bd.ycyc);
+#pragma unroll
         for (int ii = -1; ii <= 1; ++ii) {
           const int iii = wrap_clamp(i + ii, nx, bd.xcyc);
           const int ijk = iii + jjj * nx;
-          if (hij > h0[ijk]) {
-            const double l = ltab[(jj + 1) * 3 + (ii + 1)];
-            mrec[(size_t)ij * 8 + nr] = ijk;
-            mlrec[(size_t)ij * 8 + nr] = l;
-            w[nr] = (hij - h0[ijk]) / l;
+          const double hk = h0[ijk];
+          if (hij > hk) {
+            const double l = __ldg(&ltab[(jj + 1) * 3 + (ii + 1)]);
+            put8(rr, nr, ijk);
+            put8(ll, nr, l);
+            put8(w, nr, (hij - hk) / l);
             ++nr;
           }
         }
@@ -604,25 +622,44 @@ __global__ void k_mfd_receivers(Bounds bd, double p, const double* __restrict__ 
       double slope = 0.0;
       if (nr != 0) {
         double s = 0.0;
-        for (int t = 0; t < nr; ++t) s = s + w[t];
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+          if (t < nr) s = s + w[t];
         slope = (double)(float)(s / nr);
       }
       pe = (double)0.5f + (double)0.6f * slope;
     }
+    double mw[8];
     if constexpr (MIXED) {
       float wf[8], sumf = 0.0f;
-      for (int t = 0; t < nr; ++t) {
-        wf[t] = powf((float)w[t], (float)pe);
-        sumf = sumf + wf[t];
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        wf[t] = t < nr ? powf((float)w[t], (float)pe) : 0.0f;
+        if (t < nr) sumf = sumf + wf[t];
       }
-      for (int t = 0; t < nr; ++t) mwrec[(size_t)ij * 8 + t] = (double)(wf[t] / sumf);
+#pragma unroll
+      for (int t = 0; t < 8; ++t) mw[t] = t < nr ? (double)(wf[t] / sumf) : 0.0;
     } else {
-      for (int t = 0; t < nr; ++t) w[t] = pow(w[t], pe);
       double sumw = 0.0;
-      for (int t = 0; t < nr; ++t) sumw = sumw + w[t];
-      for (int t = 0; t < nr; ++t) mwrec[(size_t)ij * 8 + t] = w[t] / sumw;
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        if (t < nr) w[t] = pow(w[t], pe);
+        if (t < nr) sumw = sumw + w[t];
+      }
+#pragma unroll
+      for (int t = 0; t < 8; ++t) mw[t] = t < nr ? w[t] / sumw : 0.0;
     }
-    for (int t = nr; t < 8; ++t) { mrec[(size_t)ij * 8 + t] = -1; mwrec[(size_t)ij * 8 + t] = 0.0; mlrec[(size_t)ij * 8 + t] = 0.0; }
+    // the three rows, padded past nr (-1 / 0), with 16-byte stores
+    int4* r4 = reinterpret_cast<int4*>(mrec + (size_t)ij * 8);
+    r4[0] = make_int4(rr[0], rr[1], rr[2], rr[3]);
+    r4[1] = make_int4(rr[4], rr[5], rr[6], rr[7]);
+    double2* w2 = reinterpret_cast<double2*>(mwrec + (size_t)ij * 8);
+    double2* l2 = reinterpret_cast<double2*>(mlrec + (size_t)ij * 8);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      w2[t] = make_double2(mw[2 * t], mw[2 * t + 1]);
+      l2[t] = make_double2(ll[2 * t], ll[2 * t + 1]);
+    }
     mnrec[ij] = nr;
   }
 }
@@ -1022,10 +1059,13 @@ __global__ void k_diff_ycoef(Bounds bd, double dt2, double dx2, double dy2, cons
 
 // tridag (Diffusion.f90:164-202) for independent systems s in [s0, s1):
 // element t of system s at [t*L + s]; the solution overwrites F.  A block
-// of 32 threads solves 32 systems; coefficients are staged through shared
-// memory in chunks of kTC steps so that the sequential recurrence only waits
-// on arithmetic, not on DRAM latency.
-constexpr int kTC = 32;
+// of 32 threads solves 32 systems, one each (the recurrence is sequential,
+// and its arithmetic is the reference's).  Coefficients move through shared
+// memory in chunks of kTC steps, double-buffered: the next chunk's copies
+// are in flight while the recurrence runs through the current one, so it
+// waits on its divisions, not on DRAM.  Every lane touches only its own
+// column of the buffers.
+constexpr int kTC = 16;
 __device__ inline void cp_async_elem(double* smem, const double* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
@@ -1036,84 +1076,105 @@ __device__ inline void cp_async_elem(float* smem, const float* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem));
 }
 __device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ inline void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+template <int N>
+__device__ inline void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 template <class T>
 __global__ void __launch_bounds__(32) k_thomas(int N, int L, int s0, int s1, const T* __restrict__ A,
                                                const T* __restrict__ B, const T* __restrict__ C,
                                                T* __restrict__ F, T* __restrict__ G,
                                                int* __restrict__ err) {
-  __shared__ T sa[kTC][33], sb[kTC][33], sc[kTC][33], sf[kTC][33];
+  __shared__ T sa[2][kTC][33], sb[2][kTC][33], sc[2][kTC][33], sf[2][kTC][33];
   const int lane = threadIdx.x;
   const int s = s0 + blockIdx.x * 32 + lane;
   const bool act = s < s1;
-  T bet = 0, up = 0;
-  bool bad = false;
-  for (int t0 = 0; t0 < N; t0 += kTC) {
+  // forward elimination
+  auto load_fwd = [&](int buf, int t0) {
     const int tn = min(kTC, N - t0);
-    if (act) {  // all loads of the chunk in flight at once
+    if (act)
       for (int r = 0; r < tn; ++r) {
         const size_t o = (size_t)(t0 + r) * L + s;
-        cp_async_elem(&sa[r][lane], &A[o]);
-        cp_async_elem(&sb[r][lane], &B[o]);
-        cp_async_elem(&sf[r][lane], &F[o]);
-        if (t0 + r > 0) cp_async_elem(&sc[r][lane], &C[o - L]);
+        cp_async_elem(&sa[buf][r][lane], &A[o]);
+        cp_async_elem(&sb[buf][r][lane], &B[o]);
+        cp_async_elem(&sf[buf][r][lane], &F[o]);
+        if (t0 + r > 0) cp_async_elem(&sc[buf][r][lane], &C[o - L]);
       }
-    }
     cp_async_commit();
-    cp_async_wait_all();
+  };
+  T bet = 0, up = 0;
+  bool bad = false;
+  load_fwd(0, 0);
+  for (int t0 = 0, k = 0; t0 < N; t0 += kTC, ++k) {
+    const int buf = k & 1;
+    const int tn = min(kTC, N - t0);
+    if (t0 + kTC < N) {
+      load_fwd(buf ^ 1, t0 + kTC);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
     __syncwarp();
     if (act && !bad) {
       for (int r = 0; r < tn; ++r) {
         const int t = t0 + r;
         if (t == 0) {
-          bet = sb[0][lane];
+          bet = sb[buf][0][lane];
           if (bet == 0.0) { bad = true; break; }
-          up = sf[0][lane] / bet;
-          sf[0][lane] = up;
-          sc[0][lane] = 0.0;
+          up = sf[buf][0][lane] / bet;
+          sf[buf][0][lane] = up;
+          sc[buf][0][lane] = 0.0;
         } else {
-          const T g = sc[r][lane] / bet;
-          sc[r][lane] = g;
-          bet = sb[r][lane] - sa[r][lane] * g;
+          const T g = sc[buf][r][lane] / bet;
+          sc[buf][r][lane] = g;
+          bet = sb[buf][r][lane] - sa[buf][r][lane] * g;
           if (bet == 0.0) { bad = true; break; }
-          up = (sf[r][lane] - sa[r][lane] * up) / bet;
-          sf[r][lane] = up;
+          up = (sf[buf][r][lane] - sa[buf][r][lane] * up) / bet;
+          sf[buf][r][lane] = up;
         }
       }
     }
-    __syncwarp();
     if (act)
       for (int r = 0; r < tn; ++r) {
         const size_t o = (size_t)(t0 + r) * L + s;
-        F[o] = sf[r][lane];
-        G[o] = sc[r][lane];
+        F[o] = sf[buf][r][lane];
+        G[o] = sc[buf][r][lane];
       }
     __syncwarp();
   }
   if (bad) { atomicExch(err, DEV_TRIDAG_ZERO); return; }
-  // back substitution u(t) = u(t) - gam(t+1)*u(t+1), chunked from the end
-  if (act) up = F[(size_t)(N - 1) * L + s];
-  for (int t1 = N - 1; t1 > 0; t1 -= kTC) {
+  // back substitution u(t) = u(t) - gam(t+1)*u(t+1), chunked from the end;
+  // this lane's forward stores are visible to its own later loads
+  auto load_bwd = [&](int buf, int t1) {
     const int tlo = max(0, t1 - kTC);
-    const int tn = t1 - tlo;
     if (act)
-      for (int r = 0; r < tn; ++r) {
+      for (int r = 0; r < t1 - tlo; ++r) {
         const size_t o = (size_t)(tlo + r) * L + s;
-        cp_async_elem(&sf[r][lane], &F[o]);
-        cp_async_elem(&sc[r][lane], &G[o + L]);
+        cp_async_elem(&sf[buf][r][lane], &F[o]);
+        cp_async_elem(&sc[buf][r][lane], &G[o + L]);
       }
     cp_async_commit();
-    cp_async_wait_all();
+  };
+  if (act) up = F[(size_t)(N - 1) * L + s];
+  if (N > 1) load_bwd(0, N - 1);
+  for (int t1 = N - 1, k = 0; t1 > 0; t1 -= kTC, ++k) {
+    const int buf = k & 1;
+    const int tlo = max(0, t1 - kTC);
+    const int tn = t1 - tlo;
+    if (tlo > 0) {
+      load_bwd(buf ^ 1, tlo);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
     __syncwarp();
     if (act)
       for (int r = tn - 1; r >= 0; --r) {
-        up = sf[r][lane] - sc[r][lane] * up;
-        sf[r][lane] = up;
+        up = sf[buf][r][lane] - sc[buf][r][lane] * up;
+        sf[buf][r][lane] = up;
       }
-    __syncwarp();
     if (act)
-      for (int r = 0; r < tn; ++r) F[(size_t)(tlo + r) * L + s] = sf[r][lane];
+      for (int r = 0; r < tn; ++r) F[(size_t)(tlo + r) * L + s] = sf[buf][r][lane];
     __syncwarp();
   }
 }

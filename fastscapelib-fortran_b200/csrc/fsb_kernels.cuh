@@ -90,6 +90,11 @@ struct Ctx {
   // ---- scratch ----
   int *s_flag = nullptr, *s_scan = nullptr, *s_roots = nullptr, *s_root_rank = nullptr;
   unsigned long long *s_list_a = nullptr, *s_list_b = nullptr;  // 2*nn each
+  // list ranking by sublist walks: predecessor flags (2*nn bytes), the
+  // splitter lists (ping-pong) and the count of list heads
+  unsigned char* s_rank_pred = nullptr;
+  unsigned long long *s_rank_sa = nullptr, *s_rank_sb = nullptr;
+  unsigned* s_rank_nheads = nullptr;
   // LocalMinima
   size_t conn_cap = 0;       // capacity of edge arrays
   size_t hash_cap = 0;       // capacity (power of two) of the basin-pair hash
@@ -194,9 +199,15 @@ void launch_find_receiver(Ctx& c, const double* h, int* rec, double* length);
 void launch_find_donors(Ctx& c, const int* rec, int* ndon, int* don);
 void build_stack(Ctx& c, const int* rec, int* ndon, int* don, int* stack, int* pos, int* size);
 unsigned long long* list_rank(Ctx& c, size_t n, unsigned long long* a, unsigned long long* b);
+// list ranking by sublist walks: a splitter every kRankStride entries plus each
+// list head (at most kRankMaxHeads heads)
+constexpr int kRankStride = 16;
+constexpr int kRankMaxHeads = 64;
+inline size_t rank_splitter_cap(size_t n) { return (n + kRankStride - 1) / kRankStride + kRankMaxHeads; }
 
 // primitives (fsb_prims.cu)
 void exclusive_scan_int(Ctx& c, const int* in, int* out, size_t n);
+void exclusive_scan_u32(Ctx& c, const unsigned* in, unsigned* out, size_t n);
 void inclusive_scan_int(Ctx& c, const int* in, int* out, size_t n);
 void sort_pairs_u32(Ctx& c, const unsigned* kin, unsigned* kout, const int* vin, int* vout, size_t n, int end_bit);
 void sort_pairs_u64(Ctx& c, const unsigned long long* kin, unsigned long long* kout, const int* vin,

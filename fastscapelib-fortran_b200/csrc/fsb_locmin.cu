@@ -34,7 +34,8 @@ namespace {
 enum {
   C_NBASINS = 0, C_NLOCMIN = 1, C_BASIN0 = 2, C_NEDGE = 3, C_NSEG = 4, C_NSMALL = 5,
   C_CHANGED = 6, C_NTREE = 7, C_NLOCMIN_AFTER = 8, C_OVERFLOW = 9, C_NOTFLAT = 10, C_NSEG2 = 11,
-  C_NRIDX = 12, C_NRLEVELS = 13, C_NMED = 14
+  C_NRIDX = 12, C_NRLEVELS = 13, C_NMED = 14,
+  C_MST_CHANGED = 24, C_MST_FLAT = 25  // 25..27: the cooperative MST's rotating flags
 };
 constexpr int kNrCounters = 15;  // counters the NR sort reads back
 
@@ -80,7 +81,10 @@ __global__ void k_basins(int nn, const int* __restrict__ stack, const int* __res
 }
 
 // active roots (local minima) and basin0 = first basin whose root is on a fixed boundary
-__global__ void k_roots_scan(Bounds bd, int nroots, const int* __restrict__ roots, int* __restrict__ cnt) {
+// the root count comes from cnt[C_NBASINS] (set on the device), so that one
+// read-back brings the basins, the pits and basin0 together
+__global__ void k_roots_scan(Bounds bd, const int* __restrict__ roots, int* cnt) {
+  const int nroots = cnt[C_NBASINS];
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nroots; r += gridDim.x * blockDim.x) {
     const int k = roots[r];
     if (is_bc_node(bd, k % bd.nx, k / bd.nx)) atomicMin(&cnt[C_BASIN0], r + 1);
@@ -735,6 +739,83 @@ __global__ void k_mst_jump(int nb, const int* __restrict__ in, int* __restrict__
   }
 }
 
+// All Borůvka rounds in one cooperative launch (the kernels above, as phases
+// separated by grid-wide barriers), so that no round waits for the host.
+// Flattening jumps in place: comp[c] <- comp[comp[c]] only ever moves a
+// pointer towards its root, so concurrent updates leave the same roots.  A
+// pass's "not flat" flag is one of three slots used in turn: the slot a pass
+// sets was cleared two barriers earlier, after every thread had read it.
+// Rounds and passes are bounded (64 each, as the host loop); a flatten that
+// does not end sets the overflow counter.
+struct MstCoop {
+  int nb, ne;
+  const int *idx1, *b1, *b2, *rank;
+  int *comp, *mn, *next, *inmst, *cnt;
+};
+
+__global__ void __launch_bounds__(kCoopThreads) k_mst_coop(MstCoop A) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nthreads = gridDim.x * blockDim.x;
+  volatile int* comp = A.comp;
+  for (int c = tid; c < A.nb; c += nthreads) comp[c] = c;
+  for (int round = 0; round < 64; ++round) {
+    for (int c = tid; c < A.nb; c += nthreads) A.mn[c] = INT_MAX;
+    if (tid == 0) {
+      A.cnt[C_MST_CHANGED] = 0;
+      A.cnt[C_MST_FLAT] = 0;
+    }
+    grid.sync();
+    for (int e = tid; e < A.ne; e += nthreads) {
+      const int cu = comp[A.b1[e] - 1], cv = comp[A.b2[e] - 1];
+      if (cu == cv) continue;
+      atomicMin(&A.mn[cu], A.rank[e]);
+      atomicMin(&A.mn[cv], A.rank[e]);
+    }
+    grid.sync();
+    for (int c = tid; c < A.nb; c += nthreads) {
+      A.next[c] = comp[c];
+      if (comp[c] != c) continue;
+      const int r = __ldcg(&A.mn[c]);
+      if (r == INT_MAX) continue;
+      const int e = A.idx1[r + 1] - 1;
+      const int cu = comp[A.b1[e] - 1], cv = comp[A.b2[e] - 1];
+      const int other = cu == c ? cv : cu;
+      A.inmst[e] = 1;
+      if (__ldcg(&A.mn[other]) == r && c < other) continue;  // mutual choice: the smaller id stays a root
+      A.next[c] = other;
+      A.cnt[C_MST_CHANGED] = 1;
+    }
+    grid.sync();
+    if (__ldcg(&A.cnt[C_MST_CHANGED]) == 0) break;  // read by every thread after the barrier
+    for (int c = tid; c < A.nb; c += nthreads) comp[c] = __ldcg(&A.next[c]);
+    grid.sync();
+    bool flat = false;
+    for (int pass = 0; pass < 64; ++pass) {
+      volatile int* fl = A.cnt + C_MST_FLAT + pass % 3;
+      if (tid == 0) A.cnt[C_MST_FLAT + (pass + 1) % 3] = 0;
+      for (int c = tid; c < A.nb; c += nthreads) {
+        const int r = comp[c];
+        const int rr = comp[r];
+        if (rr != r) {
+          comp[c] = rr;
+          *fl = 1;
+        }
+      }
+      grid.sync();
+      if (*fl == 0) {
+        flat = true;
+        break;
+      }
+    }
+    if (!flat) {
+      if (tid == 0) A.cnt[C_OVERFLOW] = 1;
+      break;
+    }
+  }
+}
+
 // tree = accepted edges in rank order (Kruskal acceptance order)
 __global__ void k_tree_flags(int ne, const int* __restrict__ idx1, const int* __restrict__ inmst,
                              int* __restrict__ flag) {
@@ -898,8 +979,11 @@ static bool nr_indexx(Ctx& c, int n, const double* w) {
   const int small_cap = (int)(c.conn_cap / 2 + 8);
   k_nr_init<<<grid1d(n + 2), kBlock, 0, c.stream>>>(n, idx, c.nr_segof, seg, c.nr_small, c.nr_med, c.d_cnt);
   c.count_launch();
-  fetch_counters(c, kNrCounters);
-  int nseg = c.h_cnt[C_NSEG];
+  int nseg = 1;  // k_nr_init makes one segment of the whole array when n > kNrMedium
+  if (n <= kNrMedium) {
+    fetch_counters(c, kNrCounters);
+    nseg = c.h_cnt[C_NSEG];
+  }
   if (nseg > 0 && nr_levels_coop(c, n, arr, small_cap)) {
     if (c.h_cnt[C_OVERFLOW]) { c.err = "NR sort emulation: small-segment buffer overflow"; return false; }
     if (c.h_cnt[C_NRLEVELS] >= nr_max_levels(n)) { c.err = "NR sort emulation: too many levels"; return false; }
@@ -958,6 +1042,39 @@ static bool nr_indexx(Ctx& c, int n, const double* w) {
   return true;
 }
 
+// Borůvka in one cooperative launch; false when the device refuses it or the
+// graph is large (the host-driven rounds run instead).  Measured on B200: the
+// cooperative form saves the rounds' read-backs (1025^2 grid, 3.7e5 edges:
+// LocalMinima 3.12 -> 2.71 ms), but its grid-wide barriers over many blocks
+// cost more than they save on large graphs (2049^2, 1.5e6 edges: 5.08 ->
+// 5.74 ms), hence the size limit.
+constexpr int kMstCoopMax = 1 << 20;
+
+static bool mst_coop(Ctx& c, int nroots, int ne) {
+  if (std::max(ne, nroots) > kMstCoopMax) return false;
+  int dev = 0, coop = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mst_coop, kCoopThreads, 0) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    return false;
+  }
+  // about 2048 edges per block, at most what is resident at once
+  const int want = (std::max(ne, nroots) + 2047) / 2048;
+  const int blocks = std::max(1, std::min(want, sms * per_sm));
+  MstCoop A{nroots, ne, c.nr_idx, c.e_b1, c.e_b2, c.e_rank, c.mst_comp, c.mst_min, c.mst_next, c.e_inmst, c.d_cnt};
+  void* args[] = {&A};
+  if (cudaLaunchCooperativeKernel((const void*)k_mst_coop, dim3(blocks), dim3(kCoopThreads), args, 0, c.stream) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  c.count_launch();
+  return true;
+}
+
 bool local_minima(Ctx& c) {
   const int nn = c.nn;
   cudaStream_t st = c.stream;
@@ -974,11 +1091,10 @@ bool local_minima(Ctx& c) {
   k_basins<<<grid1d(nn), kBlock, 0, st>>>(nn, c.stack, c.s_scan2, c.basins);
   c.count_launch();
   catchment(c);  // find_stack's catch: labels of the forest before re-routing
-  fetch_counters(c, 10);
-  const int nroots = c.h_cnt[C_NBASINS];
-  k_roots_scan<<<grid1d(nroots), kBlock, 0, st>>>(c.bd, nroots, c.s_roots, c.d_cnt);
+  k_roots_scan<<<grid1d(nn), kBlock, 0, st>>>(c.bd, c.s_roots, c.d_cnt);
   c.count_launch();
   fetch_counters(c, 10);
+  const int nroots = c.h_cnt[C_NBASINS];
   c.nbasins = nroots;
   c.nlocmin_before = c.h_cnt[C_NLOCMIN];
   c.basin0 = c.h_cnt[C_BASIN0] == INT_MAX ? -1 : c.h_cnt[C_BASIN0];
@@ -1029,6 +1145,7 @@ bool local_minima(Ctx& c) {
   cudaMemsetAsync(c.e_inmst, 0, sizeof(int) * ne, st);
   k_mst_init<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_comp);
   c.count_launch(2);
+  if (!mst_coop(c, nroots, ne))
   for (int round = 0; round < 64; ++round) {
     k_mst_reset<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_min);
     k_mst_minedge<<<grid1d(ne), kBlock, 0, st>>>(ne, c.e_b1, c.e_b2, c.e_rank, c.mst_comp, c.mst_min);
@@ -1063,6 +1180,10 @@ bool local_minima(Ctx& c) {
   fetch_counters(c, 10);
   const int ntree = c.h_cnt[C_NTREE];
   c.tree_size = ntree;
+  if (c.h_cnt[C_OVERFLOW]) {
+    c.err = "LocalMinima: the spanning tree's components did not flatten";
+    return false;
+  }
   if (ntree != nroots - 1) {
     c.err = "LocalMinima: the basin graph is not connected";
     return false;

@@ -15,6 +15,13 @@ void exclusive_scan_int(Ctx& c, const int* in, int* out, size_t n) {
   c.count_launch(2);
 }
 
+// modulo 2^32 (for sums whose terms cancel in pairs)
+void exclusive_scan_u32(Ctx& c, const unsigned* in, unsigned* out, size_t n) {
+  size_t bytes = c.cub_tmp_bytes;
+  cub::DeviceScan::ExclusiveSum(c.cub_tmp, bytes, in, out, (int)n, c.stream);
+  c.count_launch(2);
+}
+
 void inclusive_scan_int(Ctx& c, const int* in, int* out, size_t n) {
   size_t bytes = c.cub_tmp_bytes;
   cub::DeviceScan::InclusiveSum(c.cub_tmp, bytes, in, out, (int)n, c.stream);
@@ -41,6 +48,8 @@ size_t cub_temp_bytes_needed(size_t nn, size_t nconn) {
   cub::DeviceScan::ExclusiveSum(nullptr, b, (const int*)nullptr, (int*)nullptr, (int)ns);
   mx = std::max(mx, b);
   cub::DeviceScan::InclusiveSum(nullptr, b, (const int*)nullptr, (int*)nullptr, (int)ns);
+  mx = std::max(mx, b);
+  cub::DeviceScan::ExclusiveSum(nullptr, b, (const unsigned*)nullptr, (unsigned*)nullptr, (int)ns);
   mx = std::max(mx, b);
   cub::DeviceRadixSort::SortPairs(nullptr, b, (const unsigned*)nullptr, (unsigned*)nullptr,
                                   (const int*)nullptr, (int*)nullptr, (int)std::max(nconn, nn), 0, 32);

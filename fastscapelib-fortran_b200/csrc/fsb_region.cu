@@ -136,6 +136,15 @@ __device__ inline bool is_neighbour(int i, int j, int q, int nx, int ny) {
   return di >= -1 && di <= 1 && dj >= -1 && dj <= 1 && (di != 0 || dj != 0);
 }
 
+// The slots of d's receiver row that hold k, as bits (rows are padded with -1
+// past mnrec, so all eight slots are compared: two 16-byte loads)
+__device__ inline unsigned row_hits(const int* __restrict__ mrec, int d, int k) {
+  const int4* r = reinterpret_cast<const int4*>(mrec + (size_t)d * 8);
+  const int4 a = __ldg(r), b = __ldg(r + 1);
+  return (unsigned)(a.x == k) | (unsigned)(a.y == k) << 1 | (unsigned)(a.z == k) << 2 | (unsigned)(a.w == k) << 3 |
+         (unsigned)(b.x == k) << 4 | (unsigned)(b.y == k) << 5 | (unsigned)(b.z == k) << 6 | (unsigned)(b.w == k) << 7;
+}
+
 // One record line per node, tile-major: the inputs a node gathers, their
 // coefficients, and its dependents (tile-major indices, -1 past the last;
 // dependents largest priority first).
@@ -206,9 +215,13 @@ __global__ void k_acc_lines_t(Bounds bd, TileMap tm, double dxdy, const int* __r
     const int nr = mnrec[k];
     int mr[8], dep[8];
     unsigned pr[8];
+    {  // the row past mnrec holds -1
+      const int4 ra = __ldg(reinterpret_cast<const int4*>(mrec + o)), rb = __ldg(reinterpret_cast<const int4*>(mrec + o) + 1);
+      mr[0] = ra.x; mr[1] = ra.y; mr[2] = ra.z; mr[3] = ra.w;
+      mr[4] = rb.x; mr[5] = rb.y; mr[6] = rb.z; mr[7] = rb.w;
+    }
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
-      mr[t] = t < nr ? mrec[o + t] : -1;
       dep[t] = -1;
       pr[t] = 0u;
     }
@@ -242,12 +255,12 @@ __global__ void k_acc_lines_t(Bounds bd, TileMap tm, double dxdy, const int* __r
         const int d = x + y * nx;
         if (d == k || contains(seen, ns, d)) continue;
         set_at(seen, ns++, d);
-        const int nd = mnrec[d];
+        const unsigned hm = row_hits(mrec, d, k);
         double wsum = 0.0;
         int hits = 0;
 #pragma unroll
         for (int t = 0; t < 8; ++t)
-          if (t < nd && mrec[(size_t)d * 8 + t] == k) {
+          if (hm >> t & 1u) {
             const double w = mwrec[(size_t)d * 8 + t];
             wsum = hits ? wsum + w : w;
             ++hits;
@@ -365,10 +378,7 @@ __global__ void k_spl_lines_t(Bounds bd, TileMap tm, int n_is_one, double kfsed,
         set_at(seen, ns++, d);
         const int rd = rec[d];
         if (rd == d) continue;
-        bool hits = false;
-        const int nd = mnrec[d];
-#pragma unroll
-        for (int t = 0; t < 8; ++t) hits |= t < nd && mrec[(size_t)d * 8 + t] == k;
+        const bool hits = row_hits(mrec, d, k) != 0u;
         const bool gated = hits && (n_is_one ? (h[d] >= htk) : (h[d] > htk));
         if ((gated || rd == k) && dn < 8) insert_by_priority(dep, pr, dn++, tm.g(x, y), prio16(prio[d]));
       }
@@ -404,9 +414,11 @@ __global__ void k_length_pow(const double* __restrict__ ltab, double n, double* 
 // (coefficient, input, dependent), loads input t and forms term t; the
 // node's sums then run over the present slots in slot order -- the order of
 // the queue engine in fsb_flow.cu -- with every lane of the segment doing the
-// same scalar arithmetic on shuffled terms (all eight shuffles issued
-// unconditionally, absent slots masked in the adds: an early exit from the
-// loop serialised the shuffles and measured slower).  All segments of a warp execute
+// same scalar arithmetic on shuffled terms.  The area sums issue all eight
+// shuffles and mask absent slots in the adds (an early exit serialised the
+// shuffles and measured slower); the one-node Newton loop of the stream power
+// law stops at the last present slot (measured faster: it runs once per
+// iteration).  All segments of a warp execute
 // the same instruction stream: a segment without a node, or whose node needs
 // fewer Newton iterations, runs along without effect, so warp-collective
 // shuffles and ballots stay convergent.  Lane 0 of a segment stores the
@@ -567,6 +579,34 @@ struct SplRegionOpN {
         }
       }
       if (solve) hk = f / df;
+    } else if constexpr (HALF3 && NPW == 1) {
+      // one node per warp: solve and npres are warp-uniform, so the loop is
+      // the reference's and the sums stop at the last present slot
+      if (solve) {
+        const double tolp = 1.0e-3;
+        double errp = 2.0 * tolp;
+        int guard = 0;
+        while (errp > tolp) {
+          if (++guard > kNewtonLimit) {
+            if (sg.sl == 0) atomicExch(err, DEV_NEWTON_LIMIT);
+            break;
+          }
+          const double x = fmax(0.0, hk - hq);
+          const double r = sqrt(x);
+          const double tf = sl.c * (x * r), tdf = sl.c * np.n * r;
+          double f = hk - elev, df = 1.0;
+#pragma unroll
+          for (int s = 0; s < 8; ++s) {
+            if (s >= npres) break;
+            const double a = sg.shfl(tf, s), b = sg.shfl(tdf, s);
+            f = f + a;
+            df = df + b;
+          }
+          const double hn = hk - f / df;
+          errp = fabs(hn - hk);
+          hk = hk * (1.0 - omega) + hn * omega;
+        }
+      }
     } else if constexpr (HALF3) {
       const double tolp = 1.0e-3;
       bool go = solve;
@@ -695,6 +735,32 @@ struct SplRegionOpMN {
         }
       }
       d = -num / den;
+    } else if constexpr (HALF3 && NPW == 1) {  // warp-uniform, as in SplRegionOpN
+      if (solve) {
+        const float tolp = 1.0e-3f;
+        float errp = 2.0f * tolp;
+        int guard = 0;
+        while (errp > tolp) {
+          if (++guard > kNewtonLimit) {
+            if (sg.sl == 0) atomicExch(err, DEV_NEWTON_LIMIT);
+            break;
+          }
+          const float x = fmaxf(0.0f, dist + d);
+          const float r = sqrtf(x);
+          const float tf = sl.c * (x * r), tdf = sl.c * n * r;
+          float f = d, df = 1.0f;
+#pragma unroll
+          for (int s = 0; s < 8; ++s) {
+            if (s >= npres) break;
+            const float a = sg.shfl(tf, s), b = sg.shfl(tdf, s);
+            f = f + a;
+            df = df + b;
+          }
+          const float dn = d - f / df;
+          errp = fabsf(dn - d);
+          d = d * (1.0f - omega) + dn * omega;
+        }
+      }
     } else if constexpr (HALF3) {
       const float tolp = 1.0e-3f;
       bool go = solve;
@@ -879,33 +945,36 @@ __global__ void __launch_bounds__(Op::kThreads, kRegionCtasPerSm)
   const unsigned segmask = (W == 32 ? 0xffffffffu : ((1u << W) - 1u)) << sg.base;
   int cur = -1, slot = -1, ticks = 0, back = 32;
   for (;;) {
-    // segments without a node try their queue slot (the segment's lane 0)
-    int got = -1;
-    if (cur < 0 && sg.sl == 0) {
-      if (slot < 0) slot = atomicAdd(&qhead, 1);
-      if (slot < R) {
-        const unsigned short v = *(volatile unsigned short*)&q[slot];
-        if (v != kQEmpty) {
-          got = v;
-          slot = -1;
+    // segments without a node try their queue slot (the segment's lane 0);
+    // a one-segment warp that continues with a dependent skips the poll
+    if (W < 32 || cur < 0) {
+      int got = -1;
+      if (cur < 0 && sg.sl == 0) {
+        if (slot < 0) slot = atomicAdd(&qhead, 1);
+        if (slot < R) {
+          const unsigned short v = *(volatile unsigned short*)&q[slot];
+          if (v != kQEmpty) {
+            got = v;
+            slot = -1;
+          }
         }
       }
+      got = __shfl_sync(FULL, got, sg.base);
+      if (cur < 0) cur = got;
+      if (!__any_sync(FULL, cur >= 0)) {
+        int quit = 0;
+        if (lane == 0) quit = *(volatile int*)&ndone >= count || should_stop(ticks);
+        if (__shfl_sync(FULL, quit, 0)) return;
+        // idle warps back off (32 ns doubling to 512 ns): polling warps take
+        // issue slots from the busy ones (stream-power sweep at 2049^2:
+        // 15.9 -> 15.3 ms against a constant 32 ns)
+        __nanosleep(back);
+        if (back < 512) back <<= 1;
+        continue;
+      }
+      back = 32;
+      __threadfence_block();  // acquire: the producers' values
     }
-    got = __shfl_sync(FULL, got, sg.base);
-    if (cur < 0) cur = got;
-    if (!__any_sync(FULL, cur >= 0)) {
-      int quit = 0;
-      if (lane == 0) quit = *(volatile int*)&ndone >= count || should_stop(ticks);
-      if (__shfl_sync(FULL, quit, 0)) return;
-      // idle warps back off (32 ns doubling to 512 ns): polling warps take
-      // issue slots from the busy ones (stream-power sweep at 2049^2:
-      // 15.9 -> 15.3 ms against a constant 32 ns)
-      __nanosleep(back);
-      if (back < 512) back <<= 1;
-      continue;
-    }
-    back = 32;
-    __threadfence_block();  // acquire: the producers' values
     const int d = op.run(cur >= 0 ? gbase + cur : -1, sg, vc);
     __syncwarp();
     __threadfence_block();  // release: the node's value before its dependents' counters

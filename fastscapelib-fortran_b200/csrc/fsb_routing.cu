@@ -179,6 +179,88 @@ __global__ void k_list_rank_round(size_t n, const unsigned long long* __restrict
   }
 }
 
+// ---- list ranking by sublist walks (long lists) --------------------------------
+// Entry e's result is the suffix sum of the weights from e to its list's end.
+// Splitters: every kRankStride-th entry and every head (an entry that is no
+// entry's successor).  Each splitter walks its sublist up to the next
+// splitter, writing for every entry (splitter id << 32 | prefix), the prefix
+// being the weights before the entry within the sublist, and records
+// (next splitter id << 32 | sublist total).  Pointer jumping over the
+// splitters then gives each its suffix sum V, and entry e's result is
+// V(its splitter) - its prefix.  O(n) work against Wyllie's O(n log n).
+
+// flags every entry that is some entry's successor; leaves the unused head
+// slots of the splitter list inert (no successor, weight 0)
+__global__ void k_rank_pred(size_t n, const unsigned long long* __restrict__ lst, unsigned char* __restrict__ pred,
+                            unsigned long long* __restrict__ spl, size_t s0) {
+  const unsigned END = 0xffffffffu;
+  const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  for (size_t e = tid; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const unsigned nx = (unsigned)(lst[e] >> 32);
+    if (nx != END && nx < n) pred[nx] = 1;
+  }
+  if (tid < (size_t)kRankMaxHeads) spl[s0 + tid] = (unsigned long long)END << 32;
+}
+
+// one sublist walk from splitter entry e with splitter id `id`; every step is
+// one dependent load, and the walk ends within n steps
+__device__ void rank_walk(size_t n, const unsigned long long* __restrict__ lst, unsigned long long* __restrict__ sub,
+                          unsigned long long* __restrict__ spl, size_t e, unsigned id, int* err) {
+  const unsigned END = 0xffffffffu;
+  unsigned pre = 0, nid = END;
+  size_t x = e;
+  for (size_t steps = 0;; ++steps) {
+    const unsigned long long cur = lst[x];
+    sub[x] = ((unsigned long long)id << 32) | pre;
+    pre += (unsigned)cur;
+    const unsigned nx = (unsigned)(cur >> 32);
+    if (nx == END) break;
+    if (nx >= n || steps >= n) {  // not a list
+      atomicExch(err, DEV_STACK_ERROR);
+      break;
+    }
+    if (nx % kRankStride == 0) {
+      nid = nx / kRankStride;
+      break;
+    }
+    x = nx;
+  }
+  spl[id] = ((unsigned long long)nid << 32) | pre;
+}
+
+// thread t: the splitter at t*kRankStride, then any head among the next
+// kRankStride - 1 entries (one 16-byte load of their flags)
+__global__ void k_rank_walk(size_t n, size_t s0, const unsigned long long* __restrict__ lst,
+                            const unsigned char* __restrict__ pred, unsigned long long* __restrict__ sub,
+                            unsigned long long* __restrict__ spl, unsigned* nheads, int* err) {
+  static_assert(kRankStride == 16, "one uint4 of flags per splitter");
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < s0; t += (size_t)gridDim.x * blockDim.x) {
+    const size_t base = t * kRankStride;
+    rank_walk(n, lst, sub, spl, base, (unsigned)t, err);
+    const uint4 f4 = *reinterpret_cast<const uint4*>(pred + base);
+    const unsigned f[4] = {f4.x, f4.y, f4.z, f4.w};
+#pragma unroll
+    for (int j = 1; j < kRankStride; ++j) {
+      const size_t e = base + j;
+      if (e >= n || ((f[j >> 2] >> (8 * (j & 3))) & 0xffu) != 0u) continue;
+      const unsigned h = atomicAdd(nheads, 1u);
+      if (h >= (unsigned)kRankMaxHeads) {
+        atomicExch(err, DEV_OVERFLOW);
+        continue;
+      }
+      rank_walk(n, lst, sub, spl, e, (unsigned)(s0 + h), err);
+    }
+  }
+}
+
+__global__ void k_rank_final(size_t n, const unsigned long long* __restrict__ sub,
+                             const unsigned long long* __restrict__ vs, unsigned long long* __restrict__ out) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const unsigned long long s = sub[e];
+    out[e] = (unsigned long long)((unsigned)vs[s >> 32] - (unsigned)s);
+  }
+}
+
 // preorder position and subtree size from the ranks of the enter/exit events
 __global__ void k_stack_from_ranks(int nn, const unsigned long long* __restrict__ lst,
                                    int* __restrict__ pos, int* __restrict__ size, int* __restrict__ stack,
@@ -216,7 +298,7 @@ void launch_find_donors(Ctx& c, const int* rec, int* ndon, int* don) {
 
 // Wyllie list ranking over `n` packed entries, ping-ponging between a and b.
 // Returns the buffer that holds the result.
-unsigned long long* list_rank(Ctx& c, size_t n, unsigned long long* a, unsigned long long* b) {
+static unsigned long long* wyllie(Ctx& c, size_t n, unsigned long long* a, unsigned long long* b) {
   int rounds = 1;
   while (((size_t)1 << rounds) < n) ++rounds;
   for (int r = 0; r < rounds; ++r) {
@@ -224,6 +306,25 @@ unsigned long long* list_rank(Ctx& c, size_t n, unsigned long long* a, unsigned 
     c.count_launch();
     std::swap(a, b);
   }
+  return a;
+}
+
+// Suffix sums of `n` packed entries (succ << 32 | weight) in the low words of
+// the returned buffer (a or b).  Lists of 2^16 entries or more are ranked by
+// sublist walks (n <= 2*nn: the scratch is sized for that), shorter ones by
+// Wyllie alone.
+unsigned long long* list_rank(Ctx& c, size_t n, unsigned long long* a, unsigned long long* b) {
+  if (n < ((size_t)1 << 16) || n > 2 * (size_t)c.nn) return wyllie(c, n, a, b);
+  const size_t s0 = (n + kRankStride - 1) / kRankStride;
+  cudaMemsetAsync(c.s_rank_pred, 0, s0 * kRankStride, c.stream);  // whole flag words past n too
+  cudaMemsetAsync(c.s_rank_nheads, 0, sizeof(unsigned), c.stream);
+  k_rank_pred<<<grid1d(n), kBlock, 0, c.stream>>>(n, a, c.s_rank_pred, c.s_rank_sa, s0);
+  k_rank_walk<<<(unsigned)((s0 + 127) / 128), 128, 0, c.stream>>>(n, s0, a, c.s_rank_pred, b, c.s_rank_sa,
+                                                                    c.s_rank_nheads, c.d_err);
+  c.count_launch(2);
+  const unsigned long long* v = wyllie(c, s0 + kRankMaxHeads, c.s_rank_sa, c.s_rank_sb);
+  k_rank_final<<<grid1d(n), kBlock, 0, c.stream>>>(n, b, v, a);
+  c.count_launch();
   return a;
 }
 
