@@ -144,6 +144,7 @@ size_t layout(fsb::Ctx& c, char* base) {
   c.nr_seg = L.take<int>(E + 8); c.nr_seg2 = L.take<int>(E + 8); c.nr_small = L.take<int>(E + 16);
   c.nr_med = L.take<int>(2 * (E / 8 + 8));
   c.nr_piv = L.take<double>(E / 2 + 8); c.nr_segmeta = L.take<int>(2 * E + 32);
+  c.nr_child = L.take<int>(4 * ((E + 2) / 512 + 16));  // level segments hold > 512 keys
   c.nr_bsum_cap = 2 * 4096; c.nr_bsum = L.take<int>(c.nr_bsum_cap);
   c.e_rank = L.take<int>(E); c.e_inmst = L.take<int>(E); c.tree = L.take<int>(N);
   c.mst_comp = L.take<int>(N); c.mst_min = L.take<int>(N); c.mst_next = L.take<int>(N);

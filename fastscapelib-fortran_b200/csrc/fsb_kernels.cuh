@@ -116,6 +116,7 @@ struct Ctx {
   int *nr_med = nullptr;                      // segments of 8..512 elements (l, ir), finished in shared memory
   double* nr_piv = nullptr;
   int* nr_segmeta = nullptr;  // per segment: pv, i, j, T
+  int* nr_child = nullptr;    // per level segment: i, left id, right id, j (cooperative levels)
   int *e_rank = nullptr, *e_inmst = nullptr, *tree = nullptr;
   int *mst_comp = nullptr, *mst_min = nullptr, *mst_next = nullptr;
   int *arc_deg = nullptr, *arc_start = nullptr, *arc_slot = nullptr, *arc_adj = nullptr;

@@ -33,9 +33,10 @@ namespace {
 
 enum {
   C_NBASINS = 0, C_NLOCMIN = 1, C_BASIN0 = 2, C_NEDGE = 3, C_NSEG = 4, C_NSMALL = 5,
-  C_CHANGED = 6, C_NTREE = 7, C_NLOCMIN_AFTER = 8, C_OVERFLOW = 9, C_NOTFLAT = 10, C_NSEG2 = 11,
+  C_CHANGED = 6, C_NTREE = 7, C_NLOCMIN_AFTER = 8, C_OVERFLOW = 9, C_NSEG2 = 11,
   C_NRIDX = 12, C_NRLEVELS = 13, C_NMED = 14,
-  C_MST_CHANGED = 24, C_MST_FLAT = 25  // 25..27: the cooperative MST's rotating flags
+  C_MST_CHANGED = 24, C_MST_FLAT = 25,  // 25..27: the cooperative MST's rotating flags
+  C_MST_DONE = 28                        // host-driven MST: a round changed nothing
 };
 constexpr int kNrCounters = 15;  // counters the NR sort reads back
 
@@ -338,7 +339,9 @@ __device__ inline int nr_apply_one(int q, const int* segof, const int* seg,
 // they hold more than kNrMedium elements (counted in cnt[out_slot]), finished
 // in shared memory when they hold 8..kNrMedium (cnt[C_NMED]), insertion-sorted
 // when fewer (M = 7)
-__device__ inline void nr_newsegs_one(int s, int out_slot, const int* seg, int* meta,
+// The children's ids go to child[4s..4s+3] (i, left id, right id, j); child
+// may be meta itself (i and j are read before anything is written).
+__device__ inline void nr_newsegs_one(int s, int out_slot, const int* seg, const int* meta, int* child,
                                       int* seg2, int* small, int* med, int* cnt,
                                       int small_cap, int med_cap) {
   const int l = seg[2 * s], ir = seg[2 * s + 1];
@@ -361,22 +364,21 @@ __device__ inline void nr_newsegs_one(int s, int out_slot, const int* seg, int* 
       else atomicExch(&cnt[C_OVERFLOW], 1);
     }
   }
-  // reuse meta slots for the children ids (i, j no longer needed after this)
-  meta[4 * s + 1] = ids[0];
-  meta[4 * s + 2] = ids[1];
-  meta[4 * s + 3] = j;  // boundary of the left child
-  meta[4 * s] = i;      // start of the right child
+  child[4 * s + 1] = ids[0];
+  child[4 * s + 2] = ids[1];
+  child[4 * s + 3] = j;  // boundary of the left child
+  child[4 * s] = i;      // start of the right child
 }
 
-__device__ inline void nr_segof_one(int q, const int* seg, const int* meta,
+__device__ inline void nr_segof_one(int q, const int* seg, const int* child,
                                     int* segof) {
   const int s = segof[q];
   if (s < 0) return;
   const int l = seg[2 * s], ir = seg[2 * s + 1];
-  const int i = meta[4 * s], j = meta[4 * s + 3];
+  const int i = child[4 * s], j = child[4 * s + 3];
   int ns = -1;
-  if (q >= l && q <= j - 1) ns = meta[4 * s + 1];
-  else if (q >= i && q <= ir) ns = meta[4 * s + 2];
+  if (q >= l && q <= j - 1) ns = child[4 * s + 1];
+  else if (q >= i && q <= ir) ns = child[4 * s + 2];
   segof[q] = ns;
 }
 
@@ -431,7 +433,7 @@ __global__ void k_nr_newsegs(int in_slot, int out_slot, const int* __restrict__ 
                              int* __restrict__ cnt, int small_cap, int med_cap) {
   const int nseg = cnt[in_slot];
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x)
-    nr_newsegs_one(s, out_slot, seg, meta, seg2, small, med, cnt, small_cap, med_cap);
+    nr_newsegs_one(s, out_slot, seg, meta, meta, seg2, small, med, cnt, small_cap, med_cap);
 }
 
 __global__ void k_nr_segof(int n, const int* __restrict__ seg, const int* __restrict__ meta,
@@ -441,17 +443,18 @@ __global__ void k_nr_segof(int n, const int* __restrict__ seg, const int* __rest
 }
 
 // ---- all levels in one cooperative kernel ----------------------------------
-// The phases of a level (medians; stopper flags and their prefix sums with
-// the stopper positions; crossings; the partitioned permutation; the next
-// level's segments; segment ids) are separated by grid-wide barriers, so the
-// whole sort is one launch instead of about eleven per level.  The prefix
+// The phases of a level (stopper flags and their prefix sums with the stopper
+// positions; crossings; the partitioned permutation with the next level's
+// segments; segment ids with the next level's medians) are separated by
+// grid-wide barriers, five per level, so the whole sort is one launch
+// instead of about eleven per level.  The prefix
 // sums run over contiguous chunks of positions, one chunk per block: block
 // totals, then each block's offset, then a tiled scan of the chunk (the two
 // flags packed into one int, 16 bits each, per 256-position tile).
 struct NrCoop {
   int n;
   const double* arr;
-  int *idx, *idx2, *seg, *seg2, *segof, *lf, *rf, *ls, *rs, *lpos, *rpos, *meta, *small, *med, *cnt, *bsum;
+  int *idx, *idx2, *seg, *seg2, *segof, *lf, *rf, *ls, *rs, *lpos, *rpos, *meta, *child, *small, *med, *cnt, *bsum;
   double* piv;
   int small_cap, med_cap;
   int max_levels;
@@ -491,12 +494,15 @@ __global__ void __launch_bounds__(kCoopThreads) k_nr_levels(NrCoop A) {
   int *idx = A.idx, *idx2 = A.idx2, *seg = A.seg, *seg2 = A.seg2;
   int in = C_NSEG, out = C_NSEG2;
   int level = 0;
+  {  // the first level's medians; later levels' run with the previous level's segment ids
+    const int nseg0 = __ldcg(&A.cnt[in]);
+    for (int s = tid; s < nseg0; s += nthreads) nr_median_one(s, seg, A.arr, idx, A.piv, A.meta);
+  }
+  grid.sync();
   for (; level < A.max_levels; ++level) {
     const int nseg = __ldcg(&A.cnt[in]);
     if (nseg == 0) break;
     if (tid == 0) A.cnt[out] = 0;
-    for (int s = tid; s < nseg; s += nthreads) nr_median_one(s, seg, A.arr, idx, A.piv, A.meta);
-    grid.sync();
     // stopper flags and the block's totals
     int tl = 0, tr = 0;
     for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
@@ -555,13 +561,20 @@ __global__ void __launch_bounds__(kCoopThreads) k_nr_levels(NrCoop A) {
     grid.sync();
     for (int s = tid; s < nseg; s += nthreads) nr_cross_one(s, seg, A.ls, A.rs, A.lpos, A.rpos, A.meta);
     grid.sync();
+    // the partitioned permutation and the children (apply reads meta, the
+    // children go to child: one phase)
     for (int q = tid + 1; q <= n; q += nthreads)
       idx2[q] = nr_apply_one(q, A.segof, seg, A.meta, idx, A.lf, A.rf, A.ls, A.rs, A.lpos, A.rpos);
-    grid.sync();
     for (int s = tid; s < nseg; s += nthreads)
-      nr_newsegs_one(s, out, seg, A.meta, seg2, A.small, A.med, A.cnt, A.small_cap, A.med_cap);
+      nr_newsegs_one(s, out, seg, A.meta, A.child, seg2, A.small, A.med, A.cnt, A.small_cap, A.med_cap);
     grid.sync();
-    for (int q = tid; q <= n + 1; q += nthreads) nr_segof_one(q, seg, A.meta, A.segof);
+    // segment ids from the children, and the next level's medians on the
+    // partitioned permutation (they touch neither segof nor child: one phase)
+    for (int q = tid; q <= n + 1; q += nthreads) nr_segof_one(q, seg, A.child, A.segof);
+    {
+      const int nnext = __ldcg(&A.cnt[out]);
+      for (int s = tid; s < nnext; s += nthreads) nr_median_one(s, seg2, A.arr, idx2, A.piv, A.meta);
+    }
     grid.sync();
     int* t = idx; idx = idx2; idx2 = t;
     t = seg; seg = seg2; seg2 = t;
@@ -693,12 +706,19 @@ __global__ void k_mst_init(int nb, int* __restrict__ comp) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) comp[b] = b;
 }
 
-__global__ void k_mst_reset(int nb, int* __restrict__ mn) {
+// Host-driven Borůvka rounds (graphs above kMstCoopMax edges).  Rounds are
+// launched in batches without a read-back in between: once a round's hooking
+// changes nothing, k_mst_check sets C_MST_DONE and every later kernel of the
+// batch returns at once.
+__global__ void k_mst_reset(int nb, int* __restrict__ mn, const int* __restrict__ done) {
+  if (*done) return;
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) mn[b] = INT_MAX;
 }
 
 __global__ void k_mst_minedge(int ne, const int* __restrict__ b1, const int* __restrict__ b2,
-                              const int* __restrict__ rank, const int* __restrict__ comp, int* __restrict__ mn) {
+                              const int* __restrict__ rank, const int* __restrict__ comp, int* __restrict__ mn,
+                              const int* __restrict__ done) {
+  if (*done) return;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
     const int cu = comp[b1[e] - 1], cv = comp[b2[e] - 1];
     if (cu == cv) continue;
@@ -710,6 +730,7 @@ __global__ void k_mst_minedge(int ne, const int* __restrict__ b1, const int* __r
 __global__ void k_mst_hook(int nb, const int* __restrict__ idx1, const int* __restrict__ b1,
                            const int* __restrict__ b2, const int* __restrict__ comp, const int* __restrict__ mn,
                            int* __restrict__ next, int* __restrict__ inmst, int* __restrict__ cnt) {
+  if (cnt[C_MST_DONE]) return;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nb; c += gridDim.x * blockDim.x) {
     next[c] = comp[c];
     if (comp[c] != c) continue;
@@ -725,17 +746,38 @@ __global__ void k_mst_hook(int nb, const int* __restrict__ idx1, const int* __re
   }
 }
 
-__global__ void k_mst_apply(int nb, const int* __restrict__ next, int* __restrict__ comp) {
+// one thread: a round whose hooking changed nothing ends the MST
+__global__ void k_mst_check(int* cnt) {
+  if (cnt[C_MST_DONE]) return;
+  if (!cnt[C_CHANGED]) cnt[C_MST_DONE] = 1;
+  cnt[C_CHANGED] = 0;
+}
+
+__global__ void k_mst_apply(int nb, const int* __restrict__ next, int* __restrict__ comp,
+                            const int* __restrict__ done) {
+  if (*done) return;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nb; c += gridDim.x * blockDim.x) comp[c] = next[c];
 }
 
-// one synchronous pointer-jumping round: out[c] = in[in[c]]
-__global__ void k_mst_jump(int nb, const int* __restrict__ in, int* __restrict__ out, int* __restrict__ cnt) {
+// Flattens the hook forest in one launch: each thread moves its pointer to
+// its grandparent until it reaches a root.  Other threads' updates only move
+// pointers towards the roots (which never change here), so every thread ends
+// at its root; the loop is bounded by the number of components.
+__global__ void k_mst_flatten(int nb, int* comp, int* cnt) {
+  if (*(volatile int*)&cnt[C_MST_DONE]) return;
+  volatile int* vc = comp;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nb; c += gridDim.x * blockDim.x) {
-    const int r = in[c];
-    const int rr = in[r];
-    out[c] = rr;
-    if (rr != r) cnt[C_NOTFLAT] = 1;
+    int it = 0;
+    for (;; ++it) {
+      const int r = vc[c];
+      const int rr = vc[r];
+      if (rr == r) break;
+      if (it > nb) {  // not a forest
+        atomicExch(&cnt[C_OVERFLOW], 1);
+        break;
+      }
+      vc[c] = rr;
+    }
   }
 }
 
@@ -956,7 +998,7 @@ static bool nr_levels_coop(Ctx& c, int n, const double* arr, int small_cap) {
   const int want = (n + 2 + 2047) / 2048;
   const int blocks = std::max(1, std::min(want, std::min(sms * per_sm, c.nr_bsum_cap / 2)));
   NrCoop A{n,         arr,       c.nr_idx,  c.nr_idx2, c.nr_seg,     c.nr_seg2,  c.nr_segof,
-           c.nr_lf,   c.nr_rf,   c.nr_ls,   c.nr_rs,   c.nr_lpos,    c.nr_rpos,  c.nr_segmeta,
+           c.nr_lf,   c.nr_rf,   c.nr_ls,   c.nr_rs,   c.nr_lpos,    c.nr_rpos,  c.nr_segmeta, c.nr_child,
            c.nr_small, c.nr_med, c.d_cnt,   c.nr_bsum, c.nr_piv,     small_cap,  nr_med_cap(c),
            nr_max_levels(n)};
   void* args[] = {&A};
@@ -1145,31 +1187,27 @@ bool local_minima(Ctx& c) {
   cudaMemsetAsync(c.e_inmst, 0, sizeof(int) * ne, st);
   k_mst_init<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_comp);
   c.count_launch(2);
-  if (!mst_coop(c, nroots, ne))
-  for (int round = 0; round < 64; ++round) {
-    k_mst_reset<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_min);
-    k_mst_minedge<<<grid1d(ne), kBlock, 0, st>>>(ne, c.e_b1, c.e_b2, c.e_rank, c.mst_comp, c.mst_min);
+  if (!mst_coop(c, nroots, ne)) {
+    // rounds in batches of four, one read-back per batch (Borůvka at least
+    // halves the components per round, so the bound of 64 is never reached)
+    constexpr int kMstBatch = 4;
     cudaMemsetAsync(c.d_cnt + C_CHANGED, 0, sizeof(int), st);
-    k_mst_hook<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.nr_idx, c.e_b1, c.e_b2, c.mst_comp, c.mst_min,
-                                                   c.mst_next, c.e_inmst, c.d_cnt);
-    k_mst_apply<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_next, c.mst_comp);
-    c.count_launch(4);
-    // flatten the hook forest: comp[c] <- root of c, four jumps per read-back
-    // (jumps on a flat forest change nothing); the first read-back also
-    // brings the round's "changed" flag
-    bool changed = true;
-    for (int jr = 0; jr < 20; ++jr) {
-      cudaMemsetAsync(c.d_cnt + C_NOTFLAT, 0, sizeof(int), st);
-      for (int r = 0; r < 2; ++r) {
-        k_mst_jump<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_comp, c.mst_next, c.d_cnt);
-        k_mst_jump<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_next, c.mst_comp, c.d_cnt);
+    cudaMemsetAsync(c.d_cnt + C_MST_DONE, 0, sizeof(int), st);
+    const int* done = c.d_cnt + C_MST_DONE;
+    for (int round = 0; round < 64; round += kMstBatch) {
+      for (int r = 0; r < kMstBatch; ++r) {
+        k_mst_reset<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_min, done);
+        k_mst_minedge<<<grid1d(ne), kBlock, 0, st>>>(ne, c.e_b1, c.e_b2, c.e_rank, c.mst_comp, c.mst_min, done);
+        k_mst_hook<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.nr_idx, c.e_b1, c.e_b2, c.mst_comp, c.mst_min,
+                                                       c.mst_next, c.e_inmst, c.d_cnt);
+        k_mst_check<<<1, 1, 0, st>>>(c.d_cnt);
+        k_mst_apply<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_next, c.mst_comp, done);
+        k_mst_flatten<<<grid1d(nroots), kBlock, 0, st>>>(nroots, c.mst_comp, c.d_cnt);
+        c.count_launch(6);
       }
-      c.count_launch(4);
-      fetch_counters(c, 12);
-      if (jr == 0 && !c.h_cnt[C_CHANGED]) { changed = false; break; }
-      if (!c.h_cnt[C_NOTFLAT]) break;
+      fetch_counters(c, C_MST_DONE + 1);
+      if (c.h_cnt[C_MST_DONE]) break;
     }
-    if (!changed) break;
   }
   k_tree_flags<<<grid1d(ne + 1), kBlock, 0, st>>>(ne, c.nr_idx, c.e_inmst, c.nr_lf);
   c.count_launch();

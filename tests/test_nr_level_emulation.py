@@ -78,7 +78,7 @@ extern "C" int nr_emulate(int n, const double* w, int* perm, int* levels_out) {
     std::swap(idx, idx2);
     cnt[out] = 0;
     for (int s = 0; s < nseg; ++s)
-      nr_newsegs_one(s, out, seg.data(), meta.data(), seg2.data(), small.data(), med.data(), cnt, cap, cap);
+      nr_newsegs_one(s, out, seg.data(), meta.data(), meta.data(), seg2.data(), small.data(), med.data(), cnt, cap, cap);
     for (int q = 0; q <= n + 1; ++q) nr_segof_one(q, seg.data(), meta.data(), segof.data());
     std::swap(seg, seg2);
     std::swap(in, out);
