@@ -129,11 +129,39 @@ __device__ inline bool contains(const T (&a)[8], int n, T v) {
   for (int t = 0; t < 8; ++t) f |= t < n && a[t] == v;
   return f;
 }
-__device__ inline bool is_neighbour(int i, int j, int q, int nx, int ny) {
-  int di = q % nx - i, dj = q / nx - j;
+
+// Coordinates of q if it is one of the 3x3 neighbours of (i, j), rows and
+// columns wrapping across the grid's edges; the row is found by range compares
+// (q lies in row j-1, j or j+1, or in a wrapped edge row), so the common
+// case needs no integer division.  False if q is not a neighbour.
+__device__ inline bool nbr_of(int i, int j, int q, int nx, int ny, int& qi, int& qj) {
+  const int r0 = j * nx;
+  int y;
+  if (q >= r0 && q < r0 + nx) y = j;
+  else if (q < r0 && q >= r0 - nx) y = j - 1;
+  else if (q >= r0 + nx && q < r0 + 2 * nx) y = j + 1;
+  else if (q >= 0 && q < nx) y = 0;
+  else if (q >= (ny - 1) * nx && q < ny * nx) y = ny - 1;
+  else return false;
+  const int x = q - y * nx;
+  int di = x - i, dj = y - j;
   if (di > 1) di -= nx; else if (di < -1) di += nx;
   if (dj > 1) dj -= ny; else if (dj < -1) dj += ny;
-  return di >= -1 && di <= 1 && dj >= -1 && dj <= 1 && (di != 0 || dj != 0);
+  if (di < -1 || di > 1 || dj < -1 || dj > 1 || (di == 0 && dj == 0)) return false;
+  qi = x;
+  qj = y;
+  return true;
+}
+
+// tile-major index of receiver q of (i, j), reporting a non-neighbour
+__device__ inline int nbr_g(const TileMap& tm, int i, int j, int q, int nx, int ny, int* err) {
+  int qi, qj;
+  if (!nbr_of(i, j, q, nx, ny, qi, qj)) {
+    atomicExch(err, DEV_NOT_ADJACENT);
+    qi = q % nx;
+    qj = q / nx;
+  }
+  return tm.g(qi, qj);
 }
 
 // The slots of d's receiver row that hold k, as bits (rows are padded with -1
@@ -231,8 +259,7 @@ __global__ void k_acc_lines_t(Bounds bd, TileMap tm, double dxdy, const int* __r
       if (t >= nr) break;
       const int q = mr[t];
       if (contains(mr, t, q)) continue;
-      if (!is_neighbour(i, j, q, nx, ny)) atomicExch(err, DEV_NOT_ADJACENT);
-      insert_by_priority(dep, pr, rn++, tm.g(q % nx, q / nx), prio16(prio[q]));
+      insert_by_priority(dep, pr, rn++, nbr_g(tm, i, j, q, nx, ny, err), prio16(prio[q]));
     }
     int inp[8], seen[8];
     double aw[8];
@@ -304,6 +331,8 @@ __global__ void k_spl_lines_t(Bounds bd, TileMap tm, int n_is_one, double kfsed,
                               RegionLineT<T>* __restrict__ line, double2* __restrict__ hw,
                               unsigned char* __restrict__ cnt0, int* __restrict__ xcnt, int* err) {
   const int nx = bd.nx, ny = bd.ny, nn = nx * ny;
+  const double l_diag = __ldg(&ltab[0]), l_dy = __ldg(&ltab[1]);
+  const T lp_diag = __ldg(&lpow[0]), lp_dy = __ldg(&lpow[1]), lp_dx = __ldg(&lpow[3]);
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
     const int i = k % nx, j = k / nx;
     const int gk = tm.g(i, j);
@@ -332,33 +361,30 @@ __global__ void k_spl_lines_t(Bounds bd, TileMap tm, int n_is_one, double kfsed,
       const int q = mrec[o + t];
       if (n_is_one ? (htk >= h[q]) : (htk > h[q])) {
         const double w = mwrec[o + t], l = mlrec[o + t];
-        if (!is_neighbour(i, j, q, nx, ny)) atomicExch(err, DEV_NOT_ADJACENT);
-        // l^n from the table of the nine neighbour lengths (l is one of them)
-        T ln = 0;
-#pragma unroll
-        for (int e = 0; e < 9; ++e)
-          if (__ldg(&ltab[e]) == l) ln = __ldg(&lpow[e]);
+        // l^n from the table of the neighbour lengths: l is one of its three
+        // values (diagonal at 0, dy at 1, dx at 3; equal values have equal powers)
+        const T ln = l == l_diag ? lp_diag : l == l_dy ? lp_dy : lp_dx;
         if constexpr (sizeof(T) == sizeof(double)) {
           set_at(fact, nq, n_is_one ? kk * pow(ak * w, m) / l : kk * pow(ak * w, m) / ln);
         } else {  // mixed precision: the erosion factor in FP32
           const float kf32 = (float)kk, aw32 = (float)(ak * w), l32 = (float)l;
           set_at(fact, nq, n_is_one ? kf32 * powf(aw32, (float)m) / l32 : kf32 * powf(aw32, (float)m) / ln);
         }
-        set_at(inp, nq, tm.g(q % nx, q / nx));
+        set_at(inp, nq, nbr_g(tm, i, j, q, nx, ny, err));
         set_at(qv, nq++, q);
       }
     }
     // distinct inputs: gated receivers and rec(k), split by tile
     int nin = 0, nx_in = 0;
+    const int rg = r != k ? nbr_g(tm, i, j, r, nx, ny, err) : -1;
     if (r != k) {
-      if (!is_neighbour(i, j, r, nx, ny)) atomicExch(err, DEV_NOT_ADJACENT);
 #pragma unroll
       for (int t = 0; t < 8; ++t)
         if (t < nq && !contains(qv, t, qv[t])) {
-          if ((tm.g(qv[t] % nx, qv[t] / nx) >> tm.lr()) == tile) ++nin; else ++nx_in;
+          if ((inp[t] >> tm.lr()) == tile) ++nin; else ++nx_in;
         }
       if (!contains(qv, nq, r)) {
-        if ((tm.g(r % nx, r / nx) >> tm.lr()) == tile) ++nin; else ++nx_in;
+        if ((rg >> tm.lr()) == tile) ++nin; else ++nx_in;
       }
     }
     int dn = 0, ns = 0;
@@ -391,7 +417,7 @@ __global__ void k_spl_lines_t(Bounds bd, TileMap tm, int n_is_one, double kfsed,
       L.inp[t] = inp[t];
     }
     line[gk] = L;
-    hw[gk] = make_double2(htk, pack_meta(r != k ? tm.g(r % nx, r / nx) : -1, nr > 0));
+    hw[gk] = make_double2(htk, pack_meta(rg, nr > 0));
     cnt0[gk] = (unsigned char)(nin + (nx_in > 0 ? 1 : 0));
     xcnt[gk] = nx_in;
   }
