@@ -43,7 +43,7 @@ typedef std::vector<int> ivec;
 // reference's result is kept and the differences are counted.
 struct Pow15Diag {
   bool on = false;
-  long long solves = 0, iters = 0, iter_diff = 0, h_diff = 0;
+  long long solves = 0, iters = 0, iter_diff = 0, h_diff = 0, max_iters = 0, long_solves = 0;
   double max_rel = 0.0;
 } g_pow15;
 
@@ -748,6 +748,8 @@ void stream_power_law(Ctx& c) {
                   }
                   g_pow15.solves += 1;
                   g_pow15.iters += it;
+                  if (it > g_pow15.max_iters) g_pow15.max_iters = it;
+                  g_pow15.long_solves += it > 20;
                   g_pow15.iter_diff += itb != it;
                   g_pow15.h_diff += hb != c.h[ijk];
                   const double rel = std::fabs(hb - c.h[ijk]) / std::max(std::fabs(c.h[ijk]), 1.0);
@@ -985,9 +987,12 @@ const char* fso_last_error() { return C->err.c_str(); }
 // FastScape_Init -- FastScape_api.f90:146 -> FastScape_ctx.f90:40-53
 // on != 0: start the n = 1.5 power diagnostic (counters reset); out (may be
 // null) receives solves, total iterations, solves whose iteration count
-// differs, solves whose result differs, and the largest relative difference
+// differs, solves whose result differs, the largest relative difference,
+// the most iterations of one solve and the solves of more than 20 iterations
 int fso_pow15_diag(int on, double* out) {
   if (out) {
+    out[5] = (double)g_pow15.max_iters;
+    out[6] = (double)g_pow15.long_solves;
     out[0] = (double)g_pow15.solves;
     out[1] = (double)g_pow15.iters;
     out[2] = (double)g_pow15.iter_diff;

@@ -195,10 +195,11 @@ def pow15_diag(on=None) -> dict:
     """Counters of the n = 1.5 power diagnostic (every multiple-flow Newton
     solve repeated with x*sqrt(x) and sqrt(x) for x**1.5 and x**0.5).
     on=True/False starts/stops it (and resets the counters); None reads."""
-    out = np.zeros(5, dtype=np.float64)
+    out = np.zeros(7, dtype=np.float64)
     lib().fso_pow15_diag(-1 if on is None else int(bool(on)), out.ctypes.data)
     return {"solves": int(out[0]), "iterations": int(out[1]), "iteration_count_differs": int(out[2]),
-            "result_differs": int(out[3]), "max_rel_diff": float(out[4])}
+            "result_differs": int(out[3]), "max_rel_diff": float(out[4]), "max_iterations": int(out[5]),
+            "solves_over_20_iterations": int(out[6])}
 
 
 def locmin_debug() -> dict:
