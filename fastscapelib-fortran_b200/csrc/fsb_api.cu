@@ -529,6 +529,13 @@ int fsb_set_precision(fsb_ctx* h, int precision) {
   return 0;
 }
 
+int fsb_set_concurrency(fsb_ctx* h, int instances) {
+  if (!h) return fail("null fsb_ctx");
+  if (instances < 1) return fail("set_concurrency: instances must be at least 1");
+  h->c.launch_share = instances > 1 ? 4 : 1;
+  return 0;
+}
+
 int fsb_get_precision(fsb_ctx* h, int* precision) {
   if (!h || !precision) return fail("null argument");
   *precision = h->c.mixed ? FSB_PREC_MIXED : FSB_PREC_FP64;

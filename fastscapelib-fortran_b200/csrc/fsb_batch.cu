@@ -56,6 +56,7 @@ struct fsb_batch {
   size_t in_use = 0;
   int running = 0;
   bool stop = false;
+  int nworkers = 0;  // set before the workers start
   long long next_id = 1;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -67,7 +68,7 @@ struct fsb_batch {
 namespace {
 
 // Runs one job on `stream`; returns 0 or an error code with `msg` set.
-int run_job(Job& j, cudaStream_t stream, std::string& msg) {
+int run_job(Job& j, cudaStream_t stream, int instances, std::string& msg) {
   const fsb_job& s = j.spec;
   fsb_ctx* h = nullptr;
   void* arena = nullptr;
@@ -83,6 +84,7 @@ int run_job(Job& j, cudaStream_t stream, std::string& msg) {
   };
   step([&] { return fsb_set_nx_ny(h, s.nx, s.ny); });
   step([&] { return fsb_set_stream(h, stream); });
+  step([&] { return fsb_set_concurrency(h, instances); });
   size_t bytes = 0;
   step([&] { return fsb_workspace_bytes(h, &bytes); });
   if (rc == 0) {
@@ -134,7 +136,7 @@ void worker_main(fsb_batch* b) {
     std::string msg;
     int rc = 0;
     if (se != cudaSuccess) { rc = 1; msg = std::string("worker stream: ") + cudaGetErrorString(se); }
-    else rc = run_job(*j, stream, msg);
+    else rc = run_job(*j, stream, b->nworkers, msg);
     {
       std::lock_guard<std::mutex> lk(b->mu);
       j->t_end = now_s();
@@ -177,6 +179,7 @@ int fsb_batch_create(fsb_batch** out, int device, int workers, size_t mem_budget
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
   }
+  b->nworkers = workers;
   for (int w = 0; w < workers; ++w) b->workers.emplace_back(worker_main, b);
   *out = b;
   return 0;

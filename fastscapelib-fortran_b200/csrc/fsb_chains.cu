@@ -745,14 +745,20 @@ static void next_epoch(Ctx& c) {
 #ifndef FSB_CHAIN_TICKETS_PER_BLOCK
 #define FSB_CHAIN_TICKETS_PER_BLOCK 4096
 #endif
-// bottom-up sweeps take one chain per warp: one block per 512 tickets
-static int chain_blocks_bu(int ntickets) {
-  const int want = (ntickets + 511) / 512;
+// bottom-up sweeps take one chain per warp: one block per 512 tickets.  An
+// instance that shares the device with others (fsb_set_concurrency) takes a
+// quarter of the blocks: the persistent blocks of each instance hold SMs
+// while they wait, and fewer of them let more instances run at once (256
+// uneven single-flow grids on 32 workers: 3.22e8 -> 3.8e8 node-steps/s).
+static int chain_blocks_bu(const Ctx& c, int ntickets) {
+  const int per = 512 * c.launch_share;
+  const int want = (ntickets + per - 1) / per;
   return want < 1 ? 1 : (want > 148 * 8 ? 148 * 8 : want);
 }
 
-static int chain_blocks(int ntickets) {
-  const int want = (ntickets + FSB_CHAIN_TICKETS_PER_BLOCK - 1) / FSB_CHAIN_TICKETS_PER_BLOCK;
+static int chain_blocks(const Ctx& c, int ntickets) {
+  const int per = FSB_CHAIN_TICKETS_PER_BLOCK * c.launch_share;
+  const int want = (ntickets + per - 1) / per;
   return want < 1 ? 1 : (want > 148 * 8 ? 148 * 8 : want);
 }
 
@@ -760,7 +766,7 @@ void fill_chains(Ctx& c) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_td, c.nchains, c.ntickets_td, c.nn};
   stage_begin(c, KT_FILL);
-  k_fill_chains<<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.h, c.hwater, c.lake_depth, c.ticket,
+  k_fill_chains<<<chain_blocks(c, cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.h, c.hwater, c.lake_depth, c.ticket,
                                                     c.done, c.epoch, c.d_err);
   stage_end(c, KT_FILL);
   c.count_launch();
@@ -769,7 +775,7 @@ void fill_chains(Ctx& c) {
 void area_chains(Ctx& c) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_bu, c.nchains, c.ntickets_bu, c.nn};
-  k_area_chains<<<chain_blocks_bu(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don,
+  k_area_chains<<<chain_blocks_bu(c, cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don,
                                                                  AreaFin{c.precip, c.dx * c.dy}, c.a, c.ticket,
                                                                  c.done, c.epoch, c.d_err);
   c.count_launch();
@@ -778,7 +784,7 @@ void area_chains(Ctx& c) {
 void flux_chains(Ctx& c, double* flux) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_bu, c.nchains, c.ntickets_bu, c.nn};
-  k_area_chains<<<chain_blocks_bu(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, FluxFin{c.erate}, flux,
+  k_area_chains<<<chain_blocks_bu(c, cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, FluxFin{c.erate}, flux,
                                                                  c.ticket, c.done, c.epoch, c.d_err);
   c.count_launch();
 }
@@ -786,7 +792,7 @@ void flux_chains(Ctx& c, double* flux) {
 void chi_chains(Ctx& c, double a0, double mn, double* chi) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_td, c.nchains, c.ntickets_td, c.nn};
-  k_chi_chains<<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.a, c.length, a0, mn, chi, c.ticket,
+  k_chi_chains<<<chain_blocks(c, cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.a, c.length, a0, mn, chi, c.ticket,
                                                                 c.done, c.epoch, c.d_err);
   c.count_launch();
 }
@@ -795,7 +801,7 @@ void spl_chains(Ctx& c, double* hnew) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_td, c.nchains, c.ntickets_td, c.nn};
   const int n1 = fabs(c.n - 1.0) < 2.2250738585072014e-308;
-  k_spl_chains<false><<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(
+  k_spl_chains<false><<<chain_blocks(c, cv.ntickets), 128, 0, c.stream>>>(
       cv, c.rec, c.ndon, c.h, c.b, c.kf, c.a, c.length, c.kfsed, c.dt, c.m, c.n, 0.875 / c.n, n1, hnew, c.water,
       GsIo{nullptr, nullptr, nullptr, nullptr}, c.ticket, c.done, c.epoch, c.d_err);
   c.count_launch();
@@ -805,7 +811,7 @@ void spl_chains_gs(Ctx& c, const double* elev, const double* hstart, double* hne
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_td, c.nchains, c.ntickets_td, c.nn};
   const int n1 = fabs(c.n - 1.0) < 2.2250738585072014e-308;
-  k_spl_chains<true><<<chain_blocks(cv.ntickets), 128, 0, c.stream>>>(
+  k_spl_chains<true><<<chain_blocks(c, cv.ntickets), 128, 0, c.stream>>>(
       cv, c.rec, c.ndon, c.h, c.b, c.kf, c.a, c.length, c.kfsed, c.dt, c.m, c.n, 0.875 / c.n, n1, hnew, c.water,
       GsIo{elev, hstart, sill, contrib}, c.ticket, c.done, c.epoch, c.d_err);
   c.count_launch();
@@ -814,7 +820,7 @@ void spl_chains_gs(Ctx& c, const double* elev, const double* hstart, double* hne
 void gs_erosion_chains(Ctx& c, const double* hp, const int* sill, double* lsed, double* dh) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_bu, c.nchains, c.ntickets_bu, c.nn};
-  k_area_chains<<<chain_blocks_bu(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, GsFin{c.h, hp, sill, lsed},
+  k_area_chains<<<chain_blocks_bu(c, cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, GsFin{c.h, hp, sill, lsed},
                                                                  dh, c.ticket, c.done, c.epoch, c.d_err);
   c.count_launch();
 }
@@ -822,7 +828,7 @@ void gs_erosion_chains(Ctx& c, const double* hp, const int* sill, double* lsed, 
 void lake_volume_chains(Ctx& c, const int* sill, const double* contrib, double* vol, double* up) {
   next_epoch(c);
   ChainView cv{c.ch_ord, c.ch_start, c.ch_tk_bu, c.nchains, c.ntickets_bu, c.nn};
-  k_area_chains<<<chain_blocks_bu(cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, VolFin{sill, contrib, vol},
+  k_area_chains<<<chain_blocks_bu(c, cv.ntickets), 128, 0, c.stream>>>(cv, c.rec, c.ndon, c.don, VolFin{sill, contrib, vol},
                                                                  up, c.ticket, c.done, c.epoch, c.d_err);
   c.count_launch();
 }

@@ -52,6 +52,7 @@ struct Ctx {
   // mixed precision (fsb_set_precision): FP32 weights, area, Newton iterations
   // and tridiagonal solves; FP64 state, h update and residuals
   bool mixed = false;
+  int launch_share = 1;  // 1: alone on the device; 4: beside other instances (persistent sweeps take 1/4 the blocks)
   bool capture = false;  // keep LocalMinima intermediates of the last step
   bool routed = false;   // a step has built receivers, stack, chains and area
   bool precip_uniform = true;  // every node has precipitation precip_value (SetUp: 1)

@@ -83,6 +83,7 @@ _sig("fsb_set_dt", _vp, _d)
 _sig("fsb_set_erosional_parameters", _vp, _vp, _d, _d, _d, _vp, _d, _d, _d, _d, _i)
 _sig("fsb_set_bc", _vp, _i)
 _sig("fsb_set_precision", _vp, _i)
+_sig("fsb_set_concurrency", _vp, _i)
 _sig("fsb_get_precision", _vp, ctypes.POINTER(_i))
 _sig("fsb_set_v", _vp, _vp, _vp, _i)
 for _n in ("fsb_set_u", "fsb_init_h", "fsb_set_h", "fsb_set_basement", "fsb_set_precip"):
@@ -240,6 +241,12 @@ class FastScape:
     def set_precision(self, precision: str) -> None:
         """"fp64" (default, the reference's arithmetic) or "mixed"."""
         _check(_lib.fsb_set_precision(self._h, PRECISIONS[precision]))
+
+    def set_concurrency(self, instances: int) -> None:
+        """How many instances share the GPU with this one (1: alone).  Above 1,
+        the persistent tree sweeps take a quarter of their blocks, leaving SMs
+        to the others; results are unchanged.  Batch jobs set this themselves."""
+        _check(_lib.fsb_set_concurrency(self._h, int(instances)))
 
     def get_precision(self) -> str:
         v = _i()

@@ -108,6 +108,13 @@ int fsb_set_v(fsb_ctx* c, const double* vx, const double* vy, int where);
 enum { FSB_PREC_FP64 = 0, FSB_PREC_MIXED = 1 };
 int fsb_set_precision(fsb_ctx* c, int precision);
 int fsb_get_precision(fsb_ctx* c, int* precision);
+/* How many instances share the device with this one (no counterpart in the
+   reference, which runs one grid at a time).  1 (default): the persistent
+   tree sweeps take as many blocks as keep one grid's critical path busy;
+   more than 1: a quarter of those, leaving the SMs to the other instances
+   (the batch runtime sets its number of workers).  The results do not
+   depend on it. */
+int fsb_set_concurrency(fsb_ctx* c, int instances);
 /* FastScape_Init_H (api:267 -> ctx:339-350): h and basement b */
 int fsb_init_h(fsb_ctx* c, const double* h, int where);
 /* FastScape_Set_H (api:664 -> ctx:636-644) */
