@@ -56,3 +56,21 @@ def test_handle_errors_without_setup():
     assert fs._lib.fsb_workspace_bytes(h, ctypes.byref(size)) != 0  # nx, ny >= 3 required
     assert fs._lib.fsb_destroy(h) == 0
     del inst
+
+
+def test_instance_settings_without_gpu():
+    """Precision and concurrency are host-side settings of a handle: valid values
+    are taken, invalid ones refused with a message."""
+    import fastscapelib_fortran as fs
+    h = ctypes.c_void_p()
+    assert fs._lib.fsb_create(ctypes.byref(h)) == 0
+    prec = ctypes.c_int(-1)
+    assert fs._lib.fsb_set_precision(h, 1) == 0
+    assert fs._lib.fsb_get_precision(h, ctypes.byref(prec)) == 0 and prec.value == 1
+    assert fs._lib.fsb_set_precision(h, 7) != 0
+    assert b"precision" in fs._lib.fsb_last_error()
+    assert fs._lib.fsb_set_concurrency(h, 32) == 0
+    assert fs._lib.fsb_set_concurrency(h, 1) == 0
+    assert fs._lib.fsb_set_concurrency(h, 0) != 0
+    assert b"instances" in fs._lib.fsb_last_error()
+    assert fs._lib.fsb_destroy(h) == 0
